@@ -1,0 +1,286 @@
+"""CPU oracle for the paratt tensor-train hot path -- TEST INFRASTRUCTURE ONLY.
+
+A numpy restatement of the reference algorithms, used by ``tests/`` and by
+``bench.py``'s CPU-baseline leg as the checker.  The product (``paratt_b200``,
+``libparatt_b200.so``) never imports this module.  It is pinned against the
+reference itself: ``oracle/_ref/libparatt_ref.so`` is the reference's own C
+compiled by ``oracle/Makefile``, and ``tests/test_oracle_vs_ref.py`` plus the
+golden fixtures under ``tests/golden/`` check every function here against it.
+
+Layout (source/paratt.h:36-42): core k is a numpy array of shape
+(r_k, n_k, r_{k+1}); its Fortran-order ravel is the reference buffer, element
+(i, j, l) at ``i + r_k*(j + n_k*l)``.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+EPS = np.finfo(np.float64).eps / 2  # LAPACK DLAMCH('E'): unit roundoff
+
+
+# --------------------------------------------------------------------------
+# helpers
+# --------------------------------------------------------------------------
+def ranks_of(cores):
+    return [cores[0].shape[0]] + [c.shape[2] for c in cores]
+
+
+def dims_of(cores):
+    return [c.shape[1] for c in cores]
+
+
+def left_unfold(c):
+    r, n, r1 = c.shape
+    return c.reshape(r * n, r1, order="F")
+
+
+def right_unfold(c):
+    r, n, r1 = c.shape
+    return c.reshape(r, n * r1, order="F")
+
+
+def full(cores):
+    """Dense tensor (tiny cases only), index order (i_0, ..., i_{d-1})."""
+    t = cores[0].reshape(cores[0].shape[1], cores[0].shape[2], order="F")
+    for c in cores[1:]:
+        r, n, r1 = c.shape
+        t = np.tensordot(t, c, axes=([t.ndim - 1], [0]))
+    return t.reshape(t.shape[:-1])
+
+
+# --------------------------------------------------------------------------
+# rank rule and numerical rank
+# --------------------------------------------------------------------------
+def svdq_numrank(L):
+    """Numerical rank that LAPACK dgesvdq with JOBA='A' keeps (called from
+    pattac.c:431-452): column-pivoted QR of L, then the leading diagonal run
+    with |R_pp| >= sqrt(N)*eps*|R_11| (N = number of columns)."""
+    import scipy.linalg as sl
+
+    m, n = L.shape
+    if n == 0:
+        return 0
+    R = sl.qr(L, mode="r", pivoting=True)[0]
+    dg = np.abs(np.diag(R))
+    thr = math.sqrt(n) * EPS * dg[0]
+    nr = 1
+    for p in range(1, min(m, n)):
+        if dg[p] < thr:
+            break
+        nr += 1
+    return nr
+
+
+def rank_rule(sig, nsv, q, maxr, delta):
+    """Tail-sum truncation rule, pattac.c:468-481: walk singular values from
+    the smallest, drop while sqrt(tail sum of squares) < delta, then cap by q
+    and maxr and floor at 1."""
+    s = 0.0
+    rank = nsv
+    for j in range(nsv - 1, -1, -1):
+        s += sig[j] * sig[j]
+        if math.sqrt(s) < delta:
+            rank = j
+        else:
+            break
+    rank = min(rank, q)
+    rank = min(rank, maxr)
+    return max(rank, 1)
+
+
+# --------------------------------------------------------------------------
+# TT rounding (paratt_truncate -> pattacTruncate, ortho 'R', one rank)
+# --------------------------------------------------------------------------
+def left_orthogonalize(cores):
+    """pattacLOrthogonalization (pattac.c:244-294) with one rank: QR of each
+    left unfolding (tsqr_factorize, tsqr.c:541-714), R pushed into the next
+    core (trapezoid_mult, utilities.c:233-308), Q kept (tsqr_make_q).
+    Ranks become r_{i+1} <- min(r_i n_i, r_{i+1})."""
+    x = [c.copy() for c in cores]
+    d = len(x)
+    for i in range(d - 1):
+        r, n, r1 = x[i].shape
+        Q, R = np.linalg.qr(left_unfold(x[i]), mode="reduced")
+        q = Q.shape[1]
+        x[i] = Q.reshape(r, n, q, order="F")
+        nr1, n2, r2 = x[i + 1].shape
+        x[i + 1] = (R @ right_unfold(x[i + 1])).reshape(q, n2, r2, order="F")
+    return x
+
+
+def truncate_sweep(x, delta, maxr, info=None):
+    """pattacLTruncate (pattac.c:297-522) with one rank: for i = d-1..1, LQ of
+    the right unfolding (wflq_factorize), SVD of L (dgesvdq), rank rule,
+    x_i <- V_r^T Q, x_{i-1} <- x_{i-1} U_r S_r."""
+    d = len(x)
+    for i in range(d - 1, 0, -1):
+        r, n, r1 = x[i].shape
+        Cm = right_unfold(x[i])
+        Qt, Rt = np.linalg.qr(Cm.T, mode="reduced")  # Cm = Rt^T Qt^T
+        L = Rt.T  # r x q
+        q = L.shape[1]
+        U, s, Vt = np.linalg.svd(L, full_matrices=False)
+        nsv = min(svdq_numrank(L), len(s))
+        rank = rank_rule(s, nsv, q, maxr[i], delta)
+        if info is not None:
+            info.append({"bond": i, "sigma": s.copy(), "rank": rank, "nsv": nsv})
+        x[i] = (Vt[:rank] @ Qt.T).reshape(rank, n, r1, order="F")
+        rp, npv, _ = x[i - 1].shape
+        x[i - 1] = (left_unfold(x[i - 1]) @ (U[:, :rank] * s[:rank])).reshape(
+            rp, npv, rank, order="F")
+    return x
+
+
+def round_tt(cores, tol, maxrank, info=None):
+    """paratt_truncate(x, tol, maxRank) (paratt.c:316-342 -> pattac.c:590-675).
+
+    ``tol`` is ABSOLUTE on the grid-normalised (RMS) norm: every core is divided
+    by sqrt(n_k) first (pattac.c:608-616) and the per-bond threshold is
+    tol/sqrt(d-1) (pattac.c:315); cores are multiplied back afterwards
+    (pattac.c:665-673).  ``maxrank`` is an int or a per-bond list of d+1."""
+    d = len(cores)
+    if not hasattr(maxrank, "__len__"):
+        maxrank = [maxrank] * (d + 1)
+    x = [c / math.sqrt(c.shape[1]) for c in cores]
+    x = left_orthogonalize(x)
+    delta = tol / math.sqrt(d - 1.0) if d > 1 else math.inf
+    x = truncate_sweep(x, delta, maxrank, info)
+    return [c * math.sqrt(c.shape[1]) for c in x]
+
+
+# --------------------------------------------------------------------------
+# formal arithmetic
+# --------------------------------------------------------------------------
+def axpby(a, x, b, y):
+    """attac_tt_axpby (paratt.c:237-268) -> attacFormalAXPBY (attac.c:81-112):
+    ranks add; a and b scale core 0 only; interior cores block-diagonal; the
+    last core stacks x over y.  Requires d >= 2."""
+    d = len(x)
+    z = []
+    for k in range(d):
+        rx, n, rx1 = x[k].shape
+        ry, _, ry1 = y[k].shape
+        if k == 0:
+            c = np.concatenate([a * x[0], b * y[0]], axis=2)
+        elif k == d - 1:
+            c = np.concatenate([x[k], y[k]], axis=0)
+        else:
+            c = np.zeros((rx + ry, n, rx1 + ry1))
+            c[:rx, :, :rx1] = x[k]
+            c[rx:, :, rx1:] = y[k]
+        z.append(c)
+    return z
+
+
+def hadamard(x, y):
+    """attacHadamard (attac.c:128-136) with attacKron (utilities.c:112-129):
+    z_k[:, j, :] = kron(x_k[:, j, :], y_k[:, j, :]), row index k_y + r_y*i_x."""
+    z = []
+    for xc, yc in zip(x, y):
+        rx, n, rx1 = xc.shape
+        ry, _, ry1 = yc.shape
+        c = np.einsum("ajb,cjd->acjbd", xc, yc).reshape(rx, ry, n, rx1, ry1)
+        # row (a, c) -> c + ry*a ; col (b, d) -> d + ry1*b
+        c = c.transpose(1, 0, 2, 4, 3).reshape(ry * rx, n, ry1 * rx1, order="F")
+        z.append(c)
+    return z
+
+
+def scale(a, x):
+    """attac_tt_scale (paratt.c:271-281): core 0 times a."""
+    return [a * x[0]] + [c.copy() for c in x[1:]]
+
+
+def mult_diag(x, mode, vec):
+    """attac_mult_diag_mat (paratt.c:571-581): core[mode][:, j, :] *= vec[j]."""
+    out = [c.copy() for c in x]
+    out[mode] = out[mode] * np.asarray(vec)[None, :, None]
+    return out
+
+
+def periodic_stencil_core(core, sten):
+    """Centred periodic stencil along the mode index of one core:
+    out[i, a, l] = sum_t s_t f[i, (a + t - h) mod n, l], h = (s-1)/2, with an
+    even length decremented first (paratt.c:586, 680).  This is what
+    attac_apply_periodic_stencil (paratt.c:584-661) computes for every length
+    and what pattac_apply_periodic_stencil (paratt.c:665-770) computes for
+    3-point stencils; for h >= 2 the latter reads the wrong wrap-around ghost
+    row at 0 < a < h (its ghost counter starts at the first negative index)."""
+    s = len(sten)
+    if s % 2 == 0:
+        s -= 1
+    h = (s - 1) // 2
+    out = np.zeros_like(core)
+    for t in range(s):
+        out += sten[t] * np.roll(core, h - t, axis=1)
+    return out
+
+
+def periodic_stencil(x, mode, sten):
+    out = [c.copy() for c in x]
+    out[mode] = periodic_stencil_core(x[mode], sten)
+    return out
+
+
+# --------------------------------------------------------------------------
+# contractions
+# --------------------------------------------------------------------------
+def inner_raw(x, y):
+    """Unnormalised <X, Y> by transfer matrices (pattacInnerProduct logic,
+    pattac.c:693-741)."""
+    a = np.ones((1, 1))
+    for xc, yc in zip(x, y):
+        # a: rx x ry ; new a[b, d] = sum a[i, k] x[i, j, b] y[k, j, d]
+        t = np.einsum("ik,kjd->ijd", a, yc)
+        a = np.einsum("ijb,ijd->bd", xc, t)
+    return float(a[0, 0])
+
+
+def dot(x, y):
+    """paratt_dotprod (paratt.c:412-469): <X, Y> / prod(n)."""
+    p = 1.0
+    for c in x:
+        p *= c.shape[1]
+    return inner_raw(x, y) / p
+
+
+def norm(x):
+    """paratt_norm (paratt.c:369-409): ||X||_F / sqrt(prod n)."""
+    return math.sqrt(max(dot(x, x), 0.0))
+
+
+def entry(x, idx):
+    """paratt_entry (paratt.c:471-499 -> pattacValue, pattac.c:82-121)."""
+    v = np.ones((1,))
+    for c, j in zip(x, idx):
+        v = v @ c[:, j, :]
+    return float(v[0])
+
+
+def rel_diff(x, y):
+    """Gauge-free ||X - Y|| / ||Y|| through inner products."""
+    xx = inner_raw(x, x)
+    yy = inner_raw(y, y)
+    xy = inner_raw(x, y)
+    num = max(xx + yy - 2.0 * xy, 0.0)
+    return math.sqrt(num) / math.sqrt(yy) if yy > 0 else math.sqrt(num)
+
+
+def rel_diff_exact(x, y):
+    """Same as rel_diff but with the difference formed as a TT (x - y) and
+    left-orthogonalised, so it does not lose digits to cancellation."""
+    dz = axpby(1.0, x, -1.0, y) if len(x) > 1 else [x[0] - y[0]]
+    dz = left_orthogonalize(dz)
+    yy = left_orthogonalize(y)
+    return float(np.linalg.norm(dz[-1]) / max(np.linalg.norm(yy[-1]), 1e-300))
+
+
+# --------------------------------------------------------------------------
+# seeded synthetic inputs
+# --------------------------------------------------------------------------
+def random_tt(dims, ranks, seed, std=1.0):
+    rng = np.random.default_rng(seed)
+    return [rng.standard_normal((ranks[k], dims[k], ranks[k + 1])) * std
+            for k in range(len(dims))]
