@@ -1,0 +1,102 @@
+/*
+ * paratt_b200 -- device-resident tensor-train hot path for NVIDIA B200 (sm_100a).
+ *
+ * This is the native C ABI underneath the reference-compatible API in
+ * paratt.h / paratt_ode.h.  A ptt_tt is one tensor train whose cores live in
+ * HBM at a fixed rank capacity; its actual ranks live in device memory too,
+ * so every operation below is a fixed sequence of kernel launches on the
+ * context's stream (no host synchronisation, CUDA-graph capturable) unless
+ * its comment says it reads results back.
+ *
+ * Core layout is the reference's (source/paratt.h:36-42): core k is
+ * r_k x n_k x r_{k+1}, column-major, element (i, j, l) at
+ * i + r_k*(j + n_k*l).
+ *
+ * All functions return PTT_OK (0) or a PTT_ERR_* code; ptt_last_error()
+ * and ptt_last_error_message() describe the most recent failure.
+ */
+#ifndef PARATT_B200_H
+#define PARATT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PTT_MAX_DIM 128
+
+#if defined(__GNUC__)
+#define PTT_API __attribute__((visibility("default")))
+#else
+#define PTT_API
+#endif
+
+enum {
+    PTT_OK = 0,
+    PTT_ERR_ARG = 1,       /* invalid argument / shape mismatch            */
+    PTT_ERR_CUDA = 2,      /* CUDA runtime error (message has the details) */
+    PTT_ERR_CAPACITY = 3,  /* ranks exceed the allocated rank capacity      */
+    PTT_ERR_NUMERIC = 4,   /* non-finite values or a solver did not converge */
+    PTT_ERR_NOGPU = 5,     /* no CUDA device: this library has no CPU path  */
+    PTT_ERR_TIMEOUT = 6    /* a bounded device-side wait expired            */
+};
+
+typedef struct ptt_ctx ptt_ctx; /* device, stream, workspace, status word */
+typedef struct ptt_tt ptt_tt;   /* one device-resident tensor train      */
+
+PTT_API int ptt_last_error(void);
+PTT_API const char* ptt_last_error_message(void);
+
+/* ---- context ---------------------------------------------------------- */
+PTT_API ptt_ctx* ptt_ctx_create(int device);
+PTT_API void ptt_ctx_destroy(ptt_ctx* ctx);
+/* Blocks until the stream drains; returns the first device-side status
+ * (PTT_ERR_NUMERIC / PTT_ERR_TIMEOUT) raised since the last call, or a CUDA
+ * error.  The status word is cleared. */
+PTT_API int ptt_ctx_synchronize(ptt_ctx* ctx);
+PTT_API void* ptt_ctx_stream(ptt_ctx* ctx); /* the cudaStream_t, as void* */
+/* Launch counter: number of kernels this context has launched. */
+PTT_API long long ptt_ctx_launch_count(const ptt_ctx* ctx);
+
+/* ---- tensor trains ----------------------------------------------------- */
+/* rank_cap has d+1 entries (rank_cap[0] = rank_cap[d] = 1). */
+PTT_API ptt_tt* ptt_tt_create(ptt_ctx* ctx, int d, const int* n, const int* rank_cap);
+PTT_API void ptt_tt_destroy(ptt_tt* t);
+PTT_API int ptt_tt_shape(const ptt_tt* t, int* d, int* n, int* rank_cap);
+/* Grow the rank capacity (never shrinks); contents are kept. Allocates. */
+PTT_API int ptt_tt_reserve(ptt_tt* t, const int* rank_cap);
+/* Copy host cores in (ranks has d+1 entries; cores[k] holds
+ * ranks[k]*n[k]*ranks[k+1] doubles).  Synchronous w.r.t. the host buffers. */
+PTT_API int ptt_tt_set(ptt_tt* t, const int* ranks, const double* const* cores);
+/* Read ranks (d+1 ints) and, if cores != NULL, the cores (each cores[k]
+ * must hold ranks[k]*n[k]*ranks[k+1] doubles).  Synchronises the stream. */
+PTT_API int ptt_tt_get(ptt_tt* t, int* ranks, double* const* cores);
+PTT_API int ptt_tt_get_ranks(ptt_tt* t, int* ranks);
+/* dst <- src (shapes must agree, capacity of dst must cover src). */
+PTT_API int ptt_tt_copy(ptt_tt* dst, const ptt_tt* src);
+/* Raw device addresses of the current core buffers (valid until the next
+ * operation on t) and of the device rank array. */
+PTT_API int ptt_tt_device_cores(const ptt_tt* t, double** cores, int** ranks);
+
+/* ---- hot path ---------------------------------------------------------- */
+/* paratt_truncate semantics (paratt.c:316-342, pattac.c:590-675): tol is
+ * absolute on the grid-normalised norm ||X||_F / sqrt(prod n_k); per-bond
+ * threshold tol/sqrt(d-1); maxrank has d+1 entries (NULL = capacity). */
+PTT_API int ptt_round(ptt_tt* x, double tol, const int* maxrank);
+/* z = a*x + b*y in formal form (attacFormalAXPBY, attac.c:81-112). */
+PTT_API int ptt_axpby(double a, const ptt_tt* x, double b, const ptt_tt* y, ptt_tt* z);
+/* z = x (.) y in formal form (attacHadamard, attac.c:128-136). */
+PTT_API int ptt_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z);
+PTT_API int ptt_scale(double a, ptt_tt* x);                          /* paratt.c:271 */
+PTT_API int ptt_mult_diag(ptt_tt* x, int mode, const double* vec);   /* paratt.c:571 */
+/* Centred periodic stencil along one mode (paratt.c:584-661); an even slen
+ * is decremented.  slen <= 15. */
+PTT_API int ptt_stencil(ptt_tt* x, int mode, const double* sten, int slen);
+/* Reductions (these read a scalar back, so they synchronise). */
+PTT_API int ptt_dot(const ptt_tt* x, const ptt_tt* y, double* out);  /* <X,Y>/prod n */
+PTT_API int ptt_norm(const ptt_tt* x, double* out);                  /* RMS norm     */
+PTT_API int ptt_entry(const ptt_tt* x, const int* idx, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,215 @@
+"""paratt_b200 -- B200 tensor-train hot path (rounding, axpby, Hadamard,
+stencils, step-truncation RK2) behind the reference paratt C API.
+
+The product is the C ABI library ``libparatt_b200.so`` built in this folder
+(``make -C paratt_b200``); this module is a thin ctypes binding used by the
+tests and the benchmark.  There is no CPU implementation: importing works
+without a GPU, but every operation raises ``PttError`` (PTT_ERR_NOGPU) when no
+CUDA device is present, and ``lib()`` raises if the library was not built.
+
+Cores are numpy arrays of shape (r_k, n_k, r_{k+1}); their Fortran-order
+ravel is the reference layout ``i + r_k*(j + n_k*l)`` (source/paratt.h:36-42).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libparatt_b200.so")
+
+PTT_OK, PTT_ERR_ARG, PTT_ERR_CUDA, PTT_ERR_CAPACITY, PTT_ERR_NUMERIC, PTT_ERR_NOGPU, PTT_ERR_TIMEOUT = range(7)
+
+
+class PttError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"paratt_b200 error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+_i = C.c_int
+_d = C.c_double
+_p = C.c_void_p
+_ip = C.POINTER(C.c_int)
+_dp = C.POINTER(C.c_double)
+_dpp = C.POINTER(_dp)
+
+# name -> (restype, argtypes) for the device ABI (include/paratt_b200.h)
+_SIGS = {
+    "ptt_last_error": (_i, []),
+    "ptt_last_error_message": (C.c_char_p, []),
+    "ptt_ctx_create": (_p, [_i]),
+    "ptt_ctx_destroy": (None, [_p]),
+    "ptt_ctx_synchronize": (_i, [_p]),
+    "ptt_ctx_stream": (_p, [_p]),
+    "ptt_ctx_launch_count": (C.c_longlong, [_p]),
+    "ptt_tt_create": (_p, [_p, _i, _ip, _ip]),
+    "ptt_tt_destroy": (None, [_p]),
+    "ptt_tt_shape": (_i, [_p, _ip, _ip, _ip]),
+    "ptt_tt_reserve": (_i, [_p, _ip]),
+    "ptt_tt_set": (_i, [_p, _ip, _dpp]),
+    "ptt_tt_get": (_i, [_p, _ip, _dpp]),
+    "ptt_tt_get_ranks": (_i, [_p, _ip]),
+    "ptt_tt_copy": (_i, [_p, _p]),
+    "ptt_tt_device_cores": (_i, [_p, _dpp, C.POINTER(_ip)]),
+    "ptt_round": (_i, [_p, _d, _ip]),
+    "ptt_axpby": (_i, [_d, _p, _d, _p, _p]),
+    "ptt_hadamard": (_i, [_p, _p, _p]),
+    "ptt_scale": (_i, [_d, _p]),
+    "ptt_mult_diag": (_i, [_p, _i, _dp]),
+    "ptt_stencil": (_i, [_p, _i, _dp, _i]),
+    "ptt_dot": (_i, [_p, _p, _dp]),
+    "ptt_norm": (_i, [_p, _dp]),
+    "ptt_entry": (_i, [_p, _ip, _dp]),
+}
+
+
+def lib():
+    """Load libparatt_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} not built: run `make -C paratt_b200`")
+        L = C.CDLL(LIB_PATH, mode=os.RTLD_LOCAL)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != PTT_OK:
+        msg = lib().ptt_last_error_message()
+        raise PttError(rc, msg.decode() if msg else "")
+
+
+def _iarr(v):
+    return (C.c_int * len(v))(*[int(t) for t in v])
+
+
+class Context:
+    """One device + stream + workspace (ptt_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self.h = lib().ptt_ctx_create(device)
+        if not self.h:
+            _check(lib().ptt_last_error() or PTT_ERR_CUDA)
+
+    def sync(self):
+        _check(lib().ptt_ctx_synchronize(self.h))
+
+    @property
+    def stream(self):
+        return lib().ptt_ctx_stream(self.h)
+
+    @property
+    def launches(self) -> int:
+        return int(lib().ptt_ctx_launch_count(self.h))
+
+    def close(self):
+        if self.h:
+            lib().ptt_ctx_destroy(self.h)
+            self.h = None
+
+
+class TT:
+    """A device-resident tensor train (ptt_tt)."""
+
+    def __init__(self, ctx: Context, dims, rank_cap, cores=None):
+        self.ctx = ctx
+        self.dims = [int(n) for n in dims]
+        self.d = len(self.dims)
+        rc = list(rank_cap)
+        self.h = lib().ptt_tt_create(ctx.h, self.d, _iarr(self.dims), _iarr(rc))
+        if not self.h:
+            _check(lib().ptt_last_error() or PTT_ERR_ARG)
+        if cores is not None:
+            self.set(cores)
+
+    @classmethod
+    def from_cores(cls, ctx, cores, rank_cap=None):
+        dims = [c.shape[1] for c in cores]
+        ranks = [cores[0].shape[0]] + [c.shape[2] for c in cores]
+        return cls(ctx, dims, rank_cap or ranks, cores)
+
+    def set(self, cores):
+        ranks = [cores[0].shape[0]] + [c.shape[2] for c in cores]
+        bufs = [np.ascontiguousarray(c.ravel(order="F"), dtype=np.float64) for c in cores]
+        ptrs = (_dp * self.d)(*[b.ctypes.data_as(_dp) for b in bufs])
+        _check(lib().ptt_tt_set(self.h, _iarr(ranks), ptrs))
+
+    def ranks(self):
+        r = (C.c_int * (self.d + 1))()
+        _check(lib().ptt_tt_get_ranks(self.h, r))
+        return list(r)
+
+    def get(self):
+        r = self.ranks()
+        bufs = [np.empty(r[k] * self.dims[k] * r[k + 1]) for k in range(self.d)]
+        ptrs = (_dp * self.d)(*[b.ctypes.data_as(_dp) for b in bufs])
+        _check(lib().ptt_tt_get(self.h, _iarr(r), ptrs))
+        return [b.reshape((r[k], self.dims[k], r[k + 1]), order="F") for k, b in enumerate(bufs)]
+
+    def reserve(self, rank_cap):
+        _check(lib().ptt_tt_reserve(self.h, _iarr(rank_cap)))
+
+    def round(self, tol, maxrank=None):
+        mr = None
+        if maxrank is not None:
+            mr = _iarr(maxrank if hasattr(maxrank, "__len__") else [maxrank] * (self.d + 1))
+        _check(lib().ptt_round(self.h, float(tol), mr))
+        return self
+
+    def scale(self, a):
+        _check(lib().ptt_scale(float(a), self.h))
+        return self
+
+    def mult_diag(self, mode, vec):
+        v = np.ascontiguousarray(vec, dtype=np.float64)
+        _check(lib().ptt_mult_diag(self.h, int(mode), v.ctypes.data_as(_dp)))
+        return self
+
+    def stencil(self, mode, sten):
+        s = np.ascontiguousarray(sten, dtype=np.float64)
+        _check(lib().ptt_stencil(self.h, int(mode), s.ctypes.data_as(_dp), len(s)))
+        return self
+
+    def dot(self, other):
+        v = C.c_double()
+        _check(lib().ptt_dot(self.h, other.h, C.byref(v)))
+        return v.value
+
+    def norm(self):
+        v = C.c_double()
+        _check(lib().ptt_norm(self.h, C.byref(v)))
+        return v.value
+
+    def entry(self, idx):
+        v = C.c_double()
+        _check(lib().ptt_entry(self.h, _iarr(idx), C.byref(v)))
+        return v.value
+
+    def copy_from(self, other):
+        _check(lib().ptt_tt_copy(self.h, other.h))
+        return self
+
+    def close(self):
+        if self.h:
+            lib().ptt_tt_destroy(self.h)
+            self.h = None
+
+
+def axpby(a, x: TT, b, y: TT, z: TT):
+    _check(lib().ptt_axpby(float(a), x.h, float(b), y.h, z.h))
+    return z
+
+
+def hadamard(x: TT, y: TT, z: TT):
+    _check(lib().ptt_hadamard(x.h, y.h, z.h))
+    return z

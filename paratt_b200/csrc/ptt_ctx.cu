@@ -1,0 +1,370 @@
+// Context, device-resident tensor-train container, host<->device transfer.
+//
+// The reference allocates every core with malloc and grows it with realloc
+// (paratt.c:73-162); here the cores of a tensor train live in one HBM
+// allocation sized for a rank capacity, with a second buffer per core for
+// out-of-place kernels.  Actual ranks are kept on the device (DevDesc).
+#include "ptt_common.cuh"
+
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static __thread int g_last_error = 0;
+static __thread char g_last_msg[512];
+
+int ptt_set_error(int code, const char* fmt, ...) {
+    g_last_error = code;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_msg, sizeof(g_last_msg), fmt, ap);
+    va_end(ap);
+    if (code != PTT_OK && getenv("PTT_VERBOSE")) fprintf(stderr, "paratt_b200: %s\n", g_last_msg);
+    return code;
+}
+
+int ptt_cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return PTT_OK;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+        return ptt_set_error(PTT_ERR_NOGPU, "%s: %s (this library has no CPU path)", what,
+                             cudaGetErrorString(e));
+    return ptt_set_error(PTT_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+extern "C" int ptt_last_error(void) { return g_last_error; }
+extern "C" const char* ptt_last_error_message(void) { return g_last_msg; }
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+extern "C" ptt_ctx* ptt_ctx_create(int device) {
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        ptt_set_error(PTT_ERR_NOGPU, "no CUDA device (%s): paratt_b200 has no CPU fallback",
+                      e == cudaSuccess ? "count 0" : cudaGetErrorString(e));
+        return NULL;
+    }
+    if (device < 0 || device >= ndev) {
+        ptt_set_error(PTT_ERR_ARG, "device %d out of range (%d devices)", device, ndev);
+        return NULL;
+    }
+    if (ptt_cuda_check(cudaSetDevice(device), "cudaSetDevice")) return NULL;
+    ptt_ctx* c = (ptt_ctx*)calloc(1, sizeof(ptt_ctx));
+    c->device = device;
+    if (ptt_cuda_check(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream") ||
+        ptt_cuda_check(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking), "stream") ||
+        ptt_cuda_check(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming), "event") ||
+        ptt_cuda_check(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming), "event") ||
+        ptt_cuda_check(cudaMalloc(&c->d_status, sizeof(int)), "cudaMalloc status") ||
+        ptt_cuda_check(cudaMemset(c->d_status, 0, sizeof(int)), "memset") ||
+        ptt_cuda_check(cudaMalloc(&c->d_scalars, 512 * sizeof(double)), "cudaMalloc scalars") ||
+        ptt_cuda_check(cudaMallocHost(&c->h_scalars, 512 * sizeof(double)), "cudaMallocHost")) {
+        free(c);
+        return NULL;
+    }
+    return c;
+}
+
+extern "C" void ptt_ctx_destroy(ptt_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    cudaStreamSynchronize(c->side);
+    cudaFree(c->ws);
+    cudaFree(c->d_counters);
+    cudaFree(c->d_status);
+    cudaFree(c->d_scalars);
+    cudaFreeHost(c->h_scalars);
+    cudaEventDestroy(c->ev_fork);
+    cudaEventDestroy(c->ev_join);
+    cudaStreamDestroy(c->stream);
+    cudaStreamDestroy(c->side);
+    free(c);
+}
+
+extern "C" void* ptt_ctx_stream(ptt_ctx* c) { return c ? (void*)c->stream : NULL; }
+extern "C" long long ptt_ctx_launch_count(const ptt_ctx* c) { return c ? c->launches : 0; }
+
+extern "C" int ptt_ctx_synchronize(ptt_ctx* c) {
+    if (!c) return ptt_set_error(PTT_ERR_ARG, "null context");
+    PTT_CUDA(cudaStreamSynchronize(c->side));
+    PTT_CUDA(cudaStreamSynchronize(c->stream));
+    int st = 0;
+    PTT_CUDA(cudaMemcpy(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st) {
+        PTT_CUDA(cudaMemset(c->d_status, 0, sizeof(int)));
+        const char* what = st == PTT_ERR_CAPACITY ? "rank exceeds capacity"
+                         : st == PTT_ERR_TIMEOUT  ? "device wait timed out"
+                         : st == PTT_ERR_NUMERIC  ? "non-finite value or solver did not converge"
+                                                  : "device error";
+        return ptt_set_error(st, "device status %d: %s", st, what);
+    }
+    return PTT_OK;
+}
+
+int ptt_ws_reserve(ptt_ctx* c, size_t bytes) {
+    if (bytes <= c->ws_bytes) return PTT_OK;
+    PTT_CUDA(cudaStreamSynchronize(c->stream));
+    PTT_CUDA(cudaStreamSynchronize(c->side));
+    if (c->ws) PTT_CUDA(cudaFree(c->ws));
+    c->ws = NULL;
+    c->ws_bytes = 0;
+    size_t b = ptt_align(bytes + bytes / 4);
+    PTT_CUDA(cudaMalloc(&c->ws, b));
+    c->ws_bytes = b;
+    return PTT_OK;
+}
+
+int ptt_counters_reserve(ptt_ctx* c, size_t n) {
+    if (n <= c->counters_n) return PTT_OK;
+    PTT_CUDA(cudaStreamSynchronize(c->stream));
+    PTT_CUDA(cudaStreamSynchronize(c->side));
+    if (c->d_counters) PTT_CUDA(cudaFree(c->d_counters));
+    size_t m = n < 4096 ? 4096 : 2 * n;
+    PTT_CUDA(cudaMalloc(&c->d_counters, m * sizeof(int)));
+    PTT_CUDA(cudaMemset(c->d_counters, 0, m * sizeof(int)));
+    c->counters_n = m;
+    return PTT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// tensor trains
+// ---------------------------------------------------------------------------
+static int alloc_cores(ptt_tt* t) {
+    for (int k = 0; k < t->d; k++) {
+        long long cap = (long long)t->rcap[k] * t->n[k] * t->rcap[k + 1];
+        t->cap[k] = cap;
+        t->hd.cap[k] = cap;
+        PTT_CUDA(cudaMalloc(&t->hd.core[k], ptt_align(cap * sizeof(double))));
+        PTT_CUDA(cudaMalloc(&t->hd.alt[k], ptt_align(cap * sizeof(double))));
+    }
+    return PTT_OK;
+}
+
+extern "C" ptt_tt* ptt_tt_create(ptt_ctx* ctx, int d, const int* n, const int* rank_cap) {
+    if (!ctx || d < 1 || d > PTT_MAX_DIM || !n || !rank_cap) {
+        ptt_set_error(PTT_ERR_ARG, "ptt_tt_create: bad arguments (d=%d)", d);
+        return NULL;
+    }
+    if (rank_cap[0] != 1 || rank_cap[d] != 1) {
+        ptt_set_error(PTT_ERR_ARG, "ptt_tt_create: boundary ranks must be 1");
+        return NULL;
+    }
+    for (int k = 0; k < d; k++)
+        if (n[k] < 1 || rank_cap[k] < 1 || rank_cap[k + 1] < 1) {
+            ptt_set_error(PTT_ERR_ARG, "ptt_tt_create: bad size at mode %d", k);
+            return NULL;
+        }
+    if (ptt_cuda_check(cudaSetDevice(ctx->device), "cudaSetDevice")) return NULL;
+    ptt_tt* t = (ptt_tt*)calloc(1, sizeof(ptt_tt));
+    t->ctx = ctx;
+    t->d = d;
+    t->hd.d = d;
+    for (int k = 0; k < d; k++) t->n[k] = t->hd.n[k] = n[k];
+    for (int k = 0; k <= d; k++) {
+        t->rcap[k] = t->hd.rcap[k] = rank_cap[k];
+        t->hd.r[k] = 1;
+    }
+    if (alloc_cores(t) || ptt_cuda_check(cudaMalloc(&t->dd, sizeof(DevDesc)), "cudaMalloc desc") ||
+        ptt_cuda_check(cudaMemcpyAsync(t->dd, &t->hd, sizeof(DevDesc), cudaMemcpyHostToDevice, ctx->stream),
+                       "desc upload") ||
+        ptt_cuda_check(cudaStreamSynchronize(ctx->stream), "sync")) {
+        ptt_tt_destroy(t);
+        return NULL;
+    }
+    return t;
+}
+
+extern "C" void ptt_tt_destroy(ptt_tt* t) {
+    if (!t) return;
+    cudaStreamSynchronize(t->ctx->stream);
+    cudaStreamSynchronize(t->ctx->side);
+    for (int k = 0; k < t->d; k++) {
+        cudaFree(t->hd.core[k]);
+        cudaFree(t->hd.alt[k]);
+    }
+    cudaFree(t->dd);
+    free(t);
+}
+
+extern "C" int ptt_tt_shape(const ptt_tt* t, int* d, int* n, int* rank_cap) {
+    if (!t) return ptt_set_error(PTT_ERR_ARG, "null tt");
+    if (d) *d = t->d;
+    if (n) memcpy(n, t->n, sizeof(int) * t->d);
+    if (rank_cap) memcpy(rank_cap, t->rcap, sizeof(int) * (t->d + 1));
+    return PTT_OK;
+}
+
+// Pull the device descriptor (current buffer order and ranks) to the host.
+static int pull_desc(ptt_tt* t) {
+    PTT_CUDA(cudaStreamSynchronize(t->ctx->side));
+    PTT_CUDA(cudaMemcpyAsync(&t->hd, t->dd, sizeof(DevDesc), cudaMemcpyDeviceToHost, t->ctx->stream));
+    PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
+    return PTT_OK;
+}
+
+static int push_desc(ptt_tt* t) {
+    PTT_CUDA(cudaMemcpyAsync(t->dd, &t->hd, sizeof(DevDesc), cudaMemcpyHostToDevice, t->ctx->stream));
+    return PTT_OK;
+}
+
+extern "C" int ptt_tt_reserve(ptt_tt* t, const int* rank_cap) {
+    if (!t || !rank_cap) return ptt_set_error(PTT_ERR_ARG, "ptt_tt_reserve: bad arguments");
+    int grow = 0;
+    for (int k = 0; k <= t->d; k++) grow |= rank_cap[k] > t->rcap[k];
+    if (!grow) return PTT_OK;
+    if (rank_cap[0] != 1 || rank_cap[t->d] != 1)
+        return ptt_set_error(PTT_ERR_ARG, "ptt_tt_reserve: boundary ranks must be 1");
+    int rc = pull_desc(t);
+    if (rc) return rc;
+    for (int k = 0; k <= t->d; k++)
+        if (rank_cap[k] > t->rcap[k]) t->rcap[k] = t->hd.rcap[k] = rank_cap[k];
+    for (int k = 0; k < t->d; k++) {
+        long long cap = (long long)t->rcap[k] * t->n[k] * t->rcap[k + 1];
+        if (cap <= t->cap[k]) continue;
+        double *nc = NULL, *na = NULL;
+        PTT_CUDA(cudaMalloc(&nc, ptt_align(cap * sizeof(double))));
+        PTT_CUDA(cudaMalloc(&na, ptt_align(cap * sizeof(double))));
+        PTT_CUDA(cudaMemcpyAsync(nc, t->hd.core[k], t->cap[k] * sizeof(double), cudaMemcpyDeviceToDevice,
+                                 t->ctx->stream));
+        PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
+        cudaFree(t->hd.core[k]);
+        cudaFree(t->hd.alt[k]);
+        t->hd.core[k] = nc;
+        t->hd.alt[k] = na;
+        t->cap[k] = t->hd.cap[k] = cap;
+    }
+    rc = push_desc(t);
+    if (rc) return rc;
+    PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
+    return PTT_OK;
+}
+
+extern "C" int ptt_tt_set(ptt_tt* t, const int* ranks, const double* const* cores) {
+    if (!t || !ranks || !cores) return ptt_set_error(PTT_ERR_ARG, "ptt_tt_set: bad arguments");
+    if (ranks[0] != 1 || ranks[t->d] != 1) return ptt_set_error(PTT_ERR_ARG, "ptt_tt_set: boundary ranks must be 1");
+    int need = 0;
+    for (int k = 0; k <= t->d; k++) {
+        if (ranks[k] < 1) return ptt_set_error(PTT_ERR_ARG, "ptt_tt_set: rank %d < 1", k);
+        need |= ranks[k] > t->rcap[k];
+    }
+    if (need) {
+        int rc[PTT_MAX_DIM + 1];
+        for (int k = 0; k <= t->d; k++) rc[k] = ranks[k] > t->rcap[k] ? ranks[k] : t->rcap[k];
+        int e = ptt_tt_reserve(t, rc);
+        if (e) return e;
+    }
+    int rc = pull_desc(t);
+    if (rc) return rc;
+    for (int k = 0; k < t->d; k++) {
+        size_t cnt = (size_t)ranks[k] * t->n[k] * ranks[k + 1];
+        PTT_CUDA(cudaMemcpyAsync(t->hd.core[k], cores[k], cnt * sizeof(double), cudaMemcpyHostToDevice,
+                                 t->ctx->stream));
+    }
+    for (int k = 0; k <= t->d; k++) t->hd.r[k] = ranks[k];
+    rc = push_desc(t);
+    if (rc) return rc;
+    PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
+    return PTT_OK;
+}
+
+extern "C" int ptt_tt_get_ranks(ptt_tt* t, int* ranks) {
+    if (!t || !ranks) return ptt_set_error(PTT_ERR_ARG, "ptt_tt_get_ranks: bad arguments");
+    PTT_CUDA(cudaStreamSynchronize(t->ctx->side));
+    PTT_CUDA(cudaMemcpyAsync(t->ctx->h_scalars, t->dd->r, sizeof(int) * (t->d + 1), cudaMemcpyDeviceToHost,
+                             t->ctx->stream));
+    PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
+    memcpy(ranks, t->ctx->h_scalars, sizeof(int) * (t->d + 1));
+    return PTT_OK;
+}
+
+extern "C" int ptt_tt_get(ptt_tt* t, int* ranks, double* const* cores) {
+    if (!t) return ptt_set_error(PTT_ERR_ARG, "ptt_tt_get: null tt");
+    int rc = pull_desc(t);
+    if (rc) return rc;
+    if (ranks) memcpy(ranks, t->hd.r, sizeof(int) * (t->d + 1));
+    if (cores) {
+        for (int k = 0; k < t->d; k++) {
+            size_t cnt = (size_t)t->hd.r[k] * t->n[k] * t->hd.r[k + 1];
+            PTT_CUDA(cudaMemcpyAsync(cores[k], t->hd.core[k], cnt * sizeof(double), cudaMemcpyDeviceToHost,
+                                     t->ctx->stream));
+        }
+        PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
+    }
+    return PTT_OK;
+}
+
+extern "C" int ptt_tt_device_cores(const ptt_tt* t, double** cores, int** ranks) {
+    if (!t) return ptt_set_error(PTT_ERR_ARG, "null tt");
+    int rc = pull_desc((ptt_tt*)t);
+    if (rc) return rc;
+    if (cores)
+        for (int k = 0; k < t->d; k++) cores[k] = t->hd.core[k];
+    if (ranks) *ranks = t->dd->r;
+    return PTT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// copy and swap kernels
+// ---------------------------------------------------------------------------
+__global__ void k_swap(DevDesc* D, int k0, int k1) {
+    int k = k0 + threadIdx.x;
+    if (k < k1) {
+        double* a = D->core[k];
+        D->core[k] = D->alt[k];
+        D->alt[k] = a;
+    }
+}
+
+int ptt_swap(ptt_tt* t, int k0, int k1) {
+    if (k1 <= k0) return PTT_OK;
+    k_swap<<<1, 128, 0, t->ctx->stream>>>(t->dd, k0, k1);
+    PTT_LAUNCHED(t->ctx);
+    return PTT_OK;
+}
+
+__global__ void k_copy_tt(DevDesc* S, DevDesc* Dst, int* status) {
+    int k = blockIdx.y;
+    int d = S->d;
+    if (k >= d) return;
+    long long cnt = (long long)S->r[k] * S->n[k] * S->r[k + 1];
+    if (S->r[k] > Dst->rcap[k] || S->r[k + 1] > Dst->rcap[k + 1] || cnt > Dst->cap[k]) {
+        if (threadIdx.x == 0 && blockIdx.x == 0) PTT_STATUS_SET(status, PTT_ERR_CAPACITY);
+        return;
+    }
+    const double* s = S->core[k];
+    double* o = Dst->core[k];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
+         i += (long long)gridDim.x * blockDim.x)
+        o[i] = s[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        Dst->r[k] = S->r[k];
+        if (k == d - 1) Dst->r[d] = S->r[d];
+    }
+}
+
+extern "C" int ptt_tt_copy(ptt_tt* dst, const ptt_tt* src) {
+    if (!dst || !src || dst->d != src->d) return ptt_set_error(PTT_ERR_ARG, "ptt_tt_copy: shape mismatch");
+    for (int k = 0; k < src->d; k++)
+        if (dst->n[k] != src->n[k]) return ptt_set_error(PTT_ERR_ARG, "ptt_tt_copy: mode %d differs", k);
+    if (dst == src) return PTT_OK;
+    int rc = ptt_tt_reserve(dst, src->rcap);
+    if (rc) return rc;
+    ptt_ctx* c = dst->ctx;
+    long long mx = 0;
+    for (int k = 0; k < src->d; k++) mx = src->cap[k] > mx ? src->cap[k] : mx;
+    int bx = (int)((mx + 255) / 256);
+    if (bx > 1184) bx = 1184;
+    if (src->ctx != c) {
+        PTT_CUDA(cudaEventRecord(src->ctx->ev_fork, src->ctx->stream));
+        PTT_CUDA(cudaStreamWaitEvent(c->stream, src->ctx->ev_fork, 0));
+    }
+    k_copy_tt<<<dim3(bx, src->d), 256, 0, c->stream>>>(src->dd, dst->dd, c->d_status);
+    PTT_LAUNCHED(c);
+    return PTT_OK;
+}

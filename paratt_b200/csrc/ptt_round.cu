@@ -1,0 +1,991 @@
+// TT rounding on the device, FP64: paratt_truncate (paratt.c:316-342) ->
+// pattacTruncate (pattac.c:590-675) with ortho 'R':
+//
+//   left-to-right:  for i = 0..d-2   QR of the left unfolding of core i
+//                   (pattacLOrthogonalization, pattac.c:244-294), R pushed into
+//                   core i+1 (trapezoid_mult, utilities.c:233-308), Q kept.
+//   right-to-left:  for i = d-1..1   LQ of the right unfolding (as QR of its
+//                   transpose), SVD of L, tail-sum rank rule, core i <- V_r^T Q,
+//                   core i-1 <- core i-1 * U_r S_r (pattacLTruncate,
+//                   pattac.c:297-522).
+//
+// The grid normalisation of pattac.c:608-616/665-673 (divide every core by
+// sqrt(n_k), multiply back afterwards) scales every bond's singular values by
+// 1/sqrt(prod n_k); it is folded into the threshold instead of two passes
+// over the cores: drop while sqrt(tail) < tol/sqrt(d-1) * sqrt(prod n_k).
+//
+// Every stage reads sizes from device memory (descriptor + Info record), so
+// a rounding is a fixed launch sequence with no host synchronisation.
+#include "ptt_tsqr.cuh"
+
+#include <stdio.h>
+#include <string.h>
+
+using namespace tsqr;
+
+namespace {
+
+constexpr int MAXSW = 40;  // Jacobi sweep limit
+
+__device__ __forceinline__ unsigned group_mask8(int tid) { return 0xFFu << ((tid & 31) & ~7); }
+
+__device__ __forceinline__ double gsum8(double v, unsigned mask) {
+    v += __shfl_xor_sync(mask, v, 4);
+    v += __shfl_xor_sync(mask, v, 2);
+    v += __shfl_xor_sync(mask, v, 1);
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// Householder kernels on shared-memory tiles (row stride S = CT + 1).
+// Thread tid: column slot cs = tid/8 (columns cs + 32u), row part tid%8
+// (rows part + 8v).  One block barrier per reflector.
+// ---------------------------------------------------------------------------
+template <int CT>
+__device__ void geqrt_smem(double* Rb, double* tau_s, int c, int tid) {
+    constexpr int S = CT + 1;
+    constexpr int NU = (CT + 31) / 32;
+    constexpr int NV = CT / 8;
+    const int cs = tid >> 3, part = tid & 7;
+    const unsigned gm = group_mask8(tid);
+    for (int j = 0; j < c; j++) {
+        if ((j & 31) == cs) {
+            const double alpha = Rb[j * S + j];
+            double s2 = 0.0;
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                const int t = part + 8 * v;
+                if (t > j) {
+                    const double x = Rb[t * S + j];
+                    s2 += x * x;
+                }
+            }
+            s2 = gsum8(s2, gm);
+            double tau = 0.0, beta = alpha;
+            if (s2 > 0.0) {
+                beta = -copysign(sqrt(alpha * alpha + s2), alpha);
+                tau = (beta - alpha) / beta;
+                const double sc = 1.0 / (alpha - beta);
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    const int t = part + 8 * v;
+                    if (t > j) Rb[t * S + j] *= sc;
+                }
+            }
+            if (part == (j & 7)) Rb[j * S + j] = beta;
+            if (part == 0) tau_s[j] = tau;
+        }
+        __syncthreads();
+        const double tau = tau_s[j];
+        if (tau != 0.0) {
+#pragma unroll
+            for (int u = 0; u < NU; u++) {
+                const int l = cs + 32 * u;
+                const bool act = (l > j) && (l < c);
+                double pr = 0.0;
+                if (act) {
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        const int t = part + 8 * v;
+                        if (t >= j) pr += (t == j ? 1.0 : Rb[t * S + j]) * Rb[t * S + l];
+                    }
+                }
+                pr = gsum8(pr, 0xffffffffu);
+                if (act) {
+                    const double tw = tau * pr;
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        const int t = part + 8 * v;
+                        if (t >= j) Rb[t * S + l] -= tw * (t == j ? 1.0 : Rb[t * S + j]);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Eliminate an H-row chunk Ch into the upper triangle Rb (TSQRT): reflector j
+// has pivot Rb[j][j] and vector Ch[:, j]; on exit Ch holds the vectors.
+template <int CT>
+__device__ void tsqrt_smem(double* Rb, double* Ch, double* tau_s, int c, int tid) {
+    constexpr int S = CT + 1;
+    constexpr int NU = (CT + 31) / 32;
+    constexpr int NV = H / 8;
+    const int cs = tid >> 3, part = tid & 7;
+    const unsigned gm = group_mask8(tid);
+    for (int j = 0; j < c; j++) {
+        if ((j & 31) == cs) {
+            const double alpha = Rb[j * S + j];
+            double s2 = 0.0;
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                const double x = Ch[(part + 8 * v) * S + j];
+                s2 += x * x;
+            }
+            s2 = gsum8(s2, gm);
+            double tau = 0.0, beta = alpha;
+            if (s2 > 0.0) {
+                beta = -copysign(sqrt(alpha * alpha + s2), alpha);
+                tau = (beta - alpha) / beta;
+                const double sc = 1.0 / (alpha - beta);
+#pragma unroll
+                for (int v = 0; v < NV; v++) Ch[(part + 8 * v) * S + j] *= sc;
+            }
+            if (part == 0) {
+                Rb[j * S + j] = beta;
+                tau_s[j] = tau;
+            }
+        }
+        __syncthreads();
+        const double tau = tau_s[j];
+        if (tau != 0.0) {
+#pragma unroll
+            for (int u = 0; u < NU; u++) {
+                const int l = cs + 32 * u;
+                const bool act = (l > j) && (l < c);
+                double pr = 0.0, rjl = 0.0;
+                if (act) {
+                    rjl = Rb[j * S + l];
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        const int t = part + 8 * v;
+                        pr += Ch[t * S + j] * Ch[t * S + l];
+                    }
+                }
+                pr = gsum8(pr, 0xffffffffu);
+                if (act) {
+                    const double tw = tau * (rjl + pr);
+                    if (part == 0) Rb[j * S + l] = rjl - tw;
+#pragma unroll
+                    for (int v = 0; v < NV; v++) {
+                        const int t = part + 8 * v;
+                        Ch[t * S + l] -= tw * Ch[t * S + j];
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// factor kernel: leaves + last-arriver tree
+// ---------------------------------------------------------------------------
+template <int CT>
+__global__ void __launch_bounds__(NT) k_tsqr_factor(const DevDesc* D, int kcore, int mode, Plan pl, double* ws,
+                                                    int* status) {
+    extern __shared__ double sm[];
+    constexpr int S = CT + 1;
+    double* Rb = sm;
+    double* Ch = Rb + CT * S;
+    double* tau_s = Ch + H * S;
+    __shared__ int s_flag;
+    const int tid = threadIdx.x;
+    const View A = make_view(D, kcore, mode, false);
+    const int m = A.m, c = A.c;
+    const int P = pl.P, p = blockIdx.x;
+    double* Rn = ws + pl.o_Rn;
+    const bool bad = (c > CT || c < 1 || m < 1);
+    if (p == 0 && tid == 0) {
+        pl.info->m = m;
+        pl.info->c = c;
+        pl.info->q = m < c ? m : c;
+        pl.info->rank = 0;
+        pl.info->status = bad ? 1 : 0;
+        if (bad) PTT_STATUS_SET(status, PTT_ERR_CAPACITY);
+    }
+    if (bad) return;
+    int r0, r1;
+    leaf_range(m, pl.L, P, p, &r0, &r1);
+    const int rows = r1 - r0;
+    const int slot = P - 1 + p;
+    double* tau_leaf = ws + pl.o_tau_leaf + (long long)p * pl.KL * CT;
+    if (rows > 0) {
+        const int rb = rows < c ? rows : c;
+        for (int e = tid; e < CT * CT; e += NT) {
+            const int t = e / CT, l = e - (e / CT) * CT;
+            Rb[t * S + l] = (t < rb && l < c) ? A.p[(long long)(r0 + t) * A.rs + (long long)l * A.cs] : 0.0;
+        }
+        __syncthreads();
+        geqrt_smem<CT>(Rb, tau_s, c, tid);
+        __syncthreads();
+        for (int e = tid; e < CT * CT; e += NT) {
+            const int t = e / CT, l = e - (e / CT) * CT;
+            if (t > l) {
+                if (t < rb && l < c) A.p[(long long)(r0 + t) * A.rs + (long long)l * A.cs] = Rb[t * S + l];
+                Rb[t * S + l] = 0.0;
+            }
+        }
+        for (int j = tid; j < CT; j += NT) tau_leaf[j] = j < c ? tau_s[j] : 0.0;
+        __syncthreads();
+        int s = 0;
+        for (int t0 = r0 + rb; t0 < r1; t0 += H, s++) {
+            const int h = (r1 - t0) < H ? (r1 - t0) : H;
+            for (int e = tid; e < H * CT; e += NT) {
+                const int t = e / CT, l = e - (e / CT) * CT;
+                Ch[t * S + l] = (t < h && l < c) ? A.p[(long long)(t0 + t) * A.rs + (long long)l * A.cs] : 0.0;
+            }
+            __syncthreads();
+            tsqrt_smem<CT>(Rb, Ch, tau_s, c, tid);
+            __syncthreads();
+            for (int e = tid; e < H * CT; e += NT) {
+                const int t = e / CT, l = e - (e / CT) * CT;
+                if (t < h && l < c) A.p[(long long)(t0 + t) * A.rs + (long long)l * A.cs] = Ch[t * S + l];
+            }
+            for (int j = tid; j < CT; j += NT) tau_leaf[(long long)(1 + s) * CT + j] = j < c ? tau_s[j] : 0.0;
+            __syncthreads();
+        }
+        double* Ro = Rn + (long long)slot * CT * CT;
+        for (int e = tid; e < CT * CT; e += NT) {
+            const int t = e / CT, l = e - (e / CT) * CT;
+            Ro[e] = (t <= l) ? Rb[t * S + l] : 0.0;
+        }
+    }
+    if (tid == 0) pl.qn[slot] = rows > 0 ? (rows < c ? rows : c) : 0;
+
+    int node = slot;
+    while (node > 0) {
+        const int par = (node - 1) >> 1;
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) s_flag = atomicAdd(&pl.cnt[par], 1);
+        __syncthreads();
+        if (s_flag == 0) return;
+        __threadfence();
+        if (tid == 0) pl.cnt[par] = 0;
+        const int cl = 2 * par + 1, cr = 2 * par + 2;
+        const int qL = ldcg(&pl.qn[cl]), qR = ldcg(&pl.qn[cr]);
+        double* Rp = Rn + (long long)par * CT * CT;
+        if (qL > 0 && qR > 0) {
+            if ((qL != c || qR != c) && tid == 0) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
+            const double* RL = Rn + (long long)cl * CT * CT;
+            double* RR = Rn + (long long)cr * CT * CT;
+            for (int e = tid; e < CT * CT; e += NT) {
+                const int t = e / CT, l = e - (e / CT) * CT;
+                Rb[t * S + l] = ldcg(RL + e);
+            }
+            for (int half = 0; half < pl.NH; half++) {
+                const int h0 = half * H;
+                __syncthreads();
+                for (int e = tid; e < H * CT; e += NT) {
+                    const int t = e / CT, l = e - (e / CT) * CT;
+                    Ch[t * S + l] = (h0 + t < c) ? ldcg(RR + (long long)(h0 + t) * CT + l) : 0.0;
+                }
+                __syncthreads();
+                if (h0 < c) tsqrt_smem<CT>(Rb, Ch, tau_s, c, tid);
+                __syncthreads();
+                for (int e = tid; e < H * CT; e += NT) {
+                    const int t = e / CT, l = e - (e / CT) * CT;
+                    if (h0 + t < CT) RR[(long long)(h0 + t) * CT + l] = Ch[t * S + l];
+                }
+                double* tn = ws + pl.o_tau_node + ((long long)par * pl.NH + half) * CT;
+                for (int j = tid; j < CT; j += NT) tn[j] = (h0 < c && j < c) ? tau_s[j] : 0.0;
+            }
+            __syncthreads();
+            for (int e = tid; e < CT * CT; e += NT) {
+                const int t = e / CT, l = e - (e / CT) * CT;
+                Rp[e] = (t <= l) ? Rb[t * S + l] : 0.0;
+            }
+            if (tid == 0) {
+                pl.qn[par] = c;
+                pl.pass[par] = 0;
+            }
+        } else {
+            const int which = qL > 0 ? 1 : (qR > 0 ? 2 : 3);
+            if (which != 3) {
+                const double* src = Rn + (long long)(which == 1 ? cl : cr) * CT * CT;
+                for (int e = tid; e < CT * CT; e += NT) Rp[e] = ldcg(src + e);
+            }
+            if (tid == 0) {
+                pl.qn[par] = which == 1 ? qL : (which == 2 ? qR : 0);
+                pl.pass[par] = which;
+            }
+        }
+        node = par;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Q application: out = Q * B, B = Bn[root] (q x k), k read from device.
+// ---------------------------------------------------------------------------
+template <int CT>
+__device__ void replay_tsqrt(double* Rp, const double* Vs, const double* taus, int c, double* out, int col, int part) {
+    constexpr int S = CT + 1;
+    constexpr int NV = H / 8;
+    const unsigned gm = 0xffffffffu;
+    for (int j = c - 1; j >= 0; j--) {
+        const double tau = taus[j];
+        if (tau == 0.0) continue;
+        double pr = 0.0;
+#pragma unroll
+        for (int v = 0; v < NV; v++) pr += Vs[(part + 8 * v) * S + j] * out[v];
+        const double rj = Rp[j * KG + col];
+        pr = gsum8(pr, gm);
+        const double tw = tau * (rj + pr);
+        if (part == 0) Rp[j * KG + col] = rj - tw;
+#pragma unroll
+        for (int v = 0; v < NV; v++) out[v] -= tw * Vs[(part + 8 * v) * S + j];
+        __syncwarp();
+    }
+}
+
+template <int CT>
+__device__ void replay_geqrt(double* Rp, const double* Vb, const double* taus, int c, int col, int part) {
+    constexpr int S = CT + 1;
+    constexpr int NV = CT / 8;
+    for (int j = c - 1; j >= 0; j--) {
+        const double tau = taus[j];
+        if (tau == 0.0) continue;
+        double pr = 0.0;
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            const int t = part + 8 * v;
+            if (t >= j) pr += (t == j ? 1.0 : Vb[t * S + j]) * Rp[t * KG + col];
+        }
+        pr = gsum8(pr, 0xffffffffu);
+        const double tw = tau * pr;
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            const int t = part + 8 * v;
+            if (t >= j) Rp[t * KG + col] -= tw * (t == j ? 1.0 : Vb[t * S + j]);
+        }
+        __syncwarp();
+    }
+}
+
+template <int CT>
+__global__ void __launch_bounds__(NT) k_apply_node(Plan pl, double* ws, int first, const int* kptr) {
+    extern __shared__ double sm[];
+    constexpr int S = CT + 1;
+    double* Rp = sm;             // CT x KG
+    double* Vs = Rp + CT * KG;   // H x S
+    const int node = first + blockIdx.x;
+    const int kg0 = blockIdx.y * KG;
+    const int kk = *kptr;
+    if (pl.info->status || kg0 >= kk) return;
+    const int q = pl.qn[node];
+    if (q == 0) return;
+    const int tid = threadIdx.x, col = tid >> 3, part = tid & 7;
+    const int c = pl.info->c;
+    const int KC = pl.KC;
+    double* Bn = ws + pl.o_Bn;
+    const double* Bi = Bn + (long long)node * CT * KC;
+    const int cl = 2 * node + 1, cr = 2 * node + 2;
+    const int ps = pl.pass[node];
+    if (ps == 1 || ps == 2) {
+        double* Bo = Bn + (long long)(ps == 1 ? cl : cr) * CT * KC;
+        for (int e = tid; e < CT * KG; e += NT) {
+            const int a = e / KG, b = e - (e / KG) * KG;
+            Bo[(long long)a * KC + kg0 + b] = Bi[(long long)a * KC + kg0 + b];
+        }
+        return;
+    }
+    if (ps != 0) return;
+    for (int e = tid; e < CT * KG; e += NT) {
+        const int a = e / KG, b = e - (e / KG) * KG;
+        Rp[e] = Bi[(long long)a * KC + kg0 + b];
+    }
+    const double* RR = ws + pl.o_Rn + (long long)cr * CT * CT;
+    double* Bcr = Bn + (long long)cr * CT * KC;
+    for (int half = pl.NH - 1; half >= 0; half--) {
+        const int h0 = half * H;
+        if (h0 >= c) continue;
+        __syncthreads();
+        for (int e = tid; e < H * CT; e += NT) {
+            const int t = e / CT, l = e - (e / CT) * CT;
+            Vs[t * S + l] = (h0 + t < c) ? RR[(long long)(h0 + t) * CT + l] : 0.0;
+        }
+        __syncthreads();
+        double out[H / 8];
+#pragma unroll
+        for (int v = 0; v < H / 8; v++) out[v] = 0.0;
+        const double* taus = ws + pl.o_tau_node + ((long long)node * pl.NH + half) * CT;
+        replay_tsqrt<CT>(Rp, Vs, taus, c, out, col, part);
+#pragma unroll
+        for (int v = 0; v < H / 8; v++) {
+            const int t = h0 + part + 8 * v;
+            if (t < CT) Bcr[(long long)t * KC + kg0 + col] = out[v];
+        }
+    }
+    __syncthreads();
+    double* Bcl = Bn + (long long)cl * CT * KC;
+    for (int e = tid; e < CT * KG; e += NT) {
+        const int a = e / KG, b = e - (e / KG) * KG;
+        Bcl[(long long)a * KC + kg0 + b] = Rp[e];
+    }
+}
+
+// out_mode LEFT: out(row, col) at alt[row + m*col];  RIGHT_T: alt[row*k + col]
+template <int CT>
+__global__ void __launch_bounds__(NT) k_apply_leaf(const DevDesc* D, int kcore, int mode, Plan pl, double* ws,
+                                                   const int* kptr) {
+    extern __shared__ double sm[];
+    constexpr int S = CT + 1;
+    constexpr int VR = CT > H ? CT : H;
+    double* Rp = sm;             // CT x KG
+    double* Vs = Rp + CT * KG;   // VR x S
+    const int p = blockIdx.x;
+    const int kg0 = blockIdx.y * KG;
+    const int kk = *kptr;
+    if (pl.info->status || kg0 >= kk) return;
+    const int tid = threadIdx.x, col = tid >> 3, part = tid & 7;
+    const int m = pl.info->m, c = pl.info->c;
+    const View A = make_view(D, kcore, mode, false);
+    double* outp = D->alt[kcore];
+    const long long ors = (mode == LEFT) ? 1 : kk;
+    const long long ocs = (mode == LEFT) ? m : 1;
+    int r0, r1;
+    leaf_range(m, pl.L, pl.P, p, &r0, &r1);
+    const int rows = r1 - r0;
+    if (rows <= 0) return;
+    const int rb = rows < c ? rows : c;
+    const int slot = pl.P - 1 + p;
+    const int KC = pl.KC;
+    const double* Bi = ws + pl.o_Bn + (long long)slot * CT * KC;
+    const double* tau_leaf = ws + pl.o_tau_leaf + (long long)p * pl.KL * CT;
+    for (int e = tid; e < CT * KG; e += NT) {
+        const int a = e / KG, b = e - (e / KG) * KG;
+        Rp[e] = Bi[(long long)a * KC + kg0 + b];
+    }
+    const int ocol = kg0 + col;
+    const bool colok = ocol < kk;
+    const int nch = (rows - rb + H - 1) / H;
+    for (int s = nch - 1; s >= 0; s--) {
+        const int t0 = r0 + rb + s * H;
+        const int h = (r1 - t0) < H ? (r1 - t0) : H;
+        __syncthreads();
+        for (int e = tid; e < H * CT; e += NT) {
+            const int t = e / CT, l = e - (e / CT) * CT;
+            Vs[t * S + l] = (t < h && l < c) ? A.p[(long long)(t0 + t) * A.rs + (long long)l * A.cs] : 0.0;
+        }
+        __syncthreads();
+        double out[H / 8];
+#pragma unroll
+        for (int v = 0; v < H / 8; v++) out[v] = 0.0;
+        replay_tsqrt<CT>(Rp, Vs, tau_leaf + (long long)(1 + s) * CT, c, out, col, part);
+#pragma unroll
+        for (int v = 0; v < H / 8; v++) {
+            const int t = part + 8 * v;
+            if (t < h && colok) outp[(long long)(t0 + t) * ors + (long long)ocol * ocs] = out[v];
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < CT * CT; e += NT) {
+        const int t = e / CT, l = e - (e / CT) * CT;
+        Vs[t * S + l] = (t < rb && l < c && t > l) ? A.p[(long long)(r0 + t) * A.rs + (long long)l * A.cs] : 0.0;
+    }
+    __syncthreads();
+    replay_geqrt<CT>(Rp, Vs, tau_leaf, c, col, part);
+    __syncthreads();
+    for (int e = tid; e < CT * KG; e += NT) {
+        const int t = e / KG, b = e - (e / KG) * KG;
+        if (t < rb && kg0 + b < kk) outp[(long long)(r0 + t) * ors + (long long)(kg0 + b) * ocs] = Rp[e];
+    }
+}
+
+// B = I_q at the root, zero-padded to CT x KC.
+__global__ void k_set_identity(Plan pl, double* ws) {
+    if (pl.info->status) return;
+    const int CT = pl.CT, KC = pl.KC;
+    const int q = pl.info->q;
+    double* B = ws + pl.o_Bn;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < CT * KC; e += gridDim.x * blockDim.x) {
+        const int a = e / KC, b = e - (e / KC) * KC;
+        B[e] = (a == b && a < q) ? 1.0 : 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// one-sided Jacobi SVD of L = R^T (c x q), R = root factor of the LQ.
+// Column pairs follow the circle (round-robin) order; rotations are recorded
+// so V can be rebuilt row-parallel by k_svd_replay.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int circle_col(int pos, int round, int qq) {
+    return pos == 0 ? 0 : 1 + (pos - 1 + round) % (qq - 1);
+}
+
+constexpr int SVD_NT = 512;
+
+template <int CT>
+__global__ void __launch_bounds__(SVD_NT) k_svd_jacobi(Plan pl, double* ws, double delta, int maxr, int* status) {
+    extern __shared__ double sm[];
+    constexpr int S = CT + 1;
+    double* Lc = sm;                   // (CT+1) columns x S
+    __shared__ double s_sig[CT + 1];
+    __shared__ int s_ord[CT + 1];
+    __shared__ int s_rot;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = SVD_NT / 32;
+    Info* info = pl.info;
+    if (info->status) return;
+    const int c = info->c, q = info->q;
+    const int qq = q + (q & 1);
+    const double* R = ws + pl.o_Rn;  // root, row-major CT x CT
+    for (int e = tid; e < qq * S; e += SVD_NT) {
+        const int j = e / S, t = e - (e / S) * S;
+        Lc[e] = (j < q && t < c) ? R[(long long)j * CT + t] : 0.0;
+    }
+    __syncthreads();
+    double2* rot = (double2*)(ws + pl.o_rot);
+    const double tol = sqrt((double)c) * 1.1102230246251565e-16;
+    int sweeps = 0;
+    if (qq >= 2) {
+        for (int sw = 0; sw < MAXSW; sw++) {
+            if (tid == 0) s_rot = 0;
+            __syncthreads();
+            int myrot = 0;
+            for (int rd = 0; rd < qq - 1; rd++) {
+                for (int i = warp; i < qq / 2; i += NW) {
+                    const int pc = circle_col(i, rd, qq), qc = circle_col(qq - 1 - i, rd, qq);
+                    double* ap = Lc + pc * S;
+                    double* aq = Lc + qc * S;
+                    double al = 0.0, be = 0.0, ga = 0.0;
+                    for (int t = lane; t < c; t += 32) {
+                        const double x = ap[t], y = aq[t];
+                        al += x * x;
+                        be += y * y;
+                        ga += x * y;
+                    }
+                    al = warp_sum(al);
+                    be = warp_sum(be);
+                    ga = warp_sum(ga);
+                    double cs = 1.0, sn = 0.0;
+                    if (ga != 0.0 && fabs(ga) > tol * sqrt(al) * sqrt(be)) {
+                        const double zeta = (be - al) / (2.0 * ga);
+                        double t;
+                        if (fabs(zeta) > 1e150)
+                            t = 0.5 / zeta;
+                        else
+                            t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                        cs = 1.0 / sqrt(1.0 + t * t);
+                        sn = cs * t;
+                        for (int tt = lane; tt < c; tt += 32) {
+                            const double x = ap[tt], y = aq[tt];
+                            ap[tt] = cs * x - sn * y;
+                            aq[tt] = sn * x + cs * y;
+                        }
+                        myrot = 1;
+                    }
+                    if (lane == 0) rot[((long long)sw * (CT + 1) + rd) * ((CT + 2) / 2) + i] = make_double2(cs, sn);
+                }
+                __syncthreads();
+            }
+            if (myrot && lane == 0) atomicOr(&s_rot, 1);
+            __syncthreads();
+            sweeps = sw + 1;
+            if (s_rot == 0) break;
+        }
+        if (s_rot != 0 && tid == 0) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
+    }
+    // singular values and descending order
+    for (int j = warp; j < qq; j += NW) {
+        double s2 = 0.0;
+        for (int t = lane; t < c; t += 32) s2 += Lc[j * S + t] * Lc[j * S + t];
+        s2 = warp_sum(s2);
+        if (lane == 0) s_sig[j] = (j < q) ? sqrt(s2) : -1.0;
+    }
+    __syncthreads();
+    for (int j = tid; j < qq; j += SVD_NT) {
+        const double sj = s_sig[j];
+        int pos = 0;
+        for (int i = 0; i < qq; i++) {
+            const double si = s_sig[i];
+            pos += (si > sj) || (si == sj && i < j);
+        }
+        s_ord[pos] = j;
+    }
+    __syncthreads();
+    double* sig_out = ws + pl.o_sig;
+    if (tid == 0) {
+        const double s0 = q > 0 ? s_sig[s_ord[0]] : 0.0;
+        // numerical rank kept by LAPACK dgesvdq(JOBA='A'): sqrt(N)*eps*s0
+        const double thr = sqrt((double)q) * 1.1102230246251565e-16 * s0;
+        int nsv = q > 0 ? 1 : 0;
+        while (nsv < q && s_sig[s_ord[nsv]] >= thr) nsv++;
+        if (!(s0 == s0)) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
+        // tail-sum rule, pattac.c:468-481
+        double ssum = 0.0;
+        int rank = nsv;
+        for (int j = nsv - 1; j >= 0; j--) {
+            const double sj = s_sig[s_ord[j]];
+            ssum += sj * sj;
+            if (sqrt(ssum) < delta)
+                rank = j;
+            else
+                break;
+        }
+        if (rank > q) rank = q;
+        if (rank > maxr) rank = maxr;
+        if (rank < 1) rank = 1;
+        info->rank = rank;
+        info->nsv = nsv;
+        info->sweeps = sweeps;
+        double tail = 0.0;
+        for (int j = rank; j < q; j++) tail += s_sig[s_ord[j]] * s_sig[s_ord[j]];
+        info->tail = tail;
+    }
+    for (int j = tid; j < CT; j += SVD_NT) {
+        sig_out[j] = j < q ? s_sig[s_ord[j]] : 0.0;
+        ((int*)(sig_out + CT))[j] = j < qq ? s_ord[j] : 0;
+    }
+    __syncthreads();
+    const int rank = info->rank;
+    double* US = ws + pl.o_US;  // c x rank, column-major ld CT
+    for (int e = tid; e < CT * CT; e += SVD_NT) {
+        const int b = e / CT, t = e - (e / CT) * CT;
+        US[e] = (b < rank && t < c) ? Lc[s_ord[b] * S + t] : 0.0;
+    }
+}
+
+// Rebuild rows of V from the recorded rotations; write V_r into Bn[root].
+__global__ void __launch_bounds__(256) k_svd_replay(Plan pl, double* ws) {
+    extern __shared__ double sm[];
+    const int CT = pl.CT, KC = pl.KC;
+    const int SR = CT + 2;
+    double* vrow = sm + (threadIdx.x >> 5) * SR;  // 8 rows
+    double2* rbuf = (double2*)(sm + 8 * SR);       // (CT+2)/2 pairs
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int row = blockIdx.x * 8 + warp;
+    const Info* info = pl.info;
+    if (info->status) return;
+    const int q = info->q, qq = q + (q & 1), sweeps = info->sweeps, rank = info->rank;
+    for (int j = lane; j < SR; j += 32) vrow[j] = (j == row) ? 1.0 : 0.0;
+    const double2* rot = (const double2*)(ws + pl.o_rot);
+    const int npair = (CT + 2) / 2;
+    for (int sw = 0; sw < sweeps; sw++) {
+        for (int rd = 0; rd < qq - 1; rd++) {
+            __syncthreads();
+            for (int i = threadIdx.x; i < qq / 2; i += blockDim.x)
+                rbuf[i] = rot[((long long)sw * (CT + 1) + rd) * npair + i];
+            __syncthreads();
+            if (row < q) {
+                for (int i = lane; i < qq / 2; i += 32) {
+                    const double2 r = rbuf[i];
+                    if (r.y != 0.0) {
+                        const int pc = circle_col(i, rd, qq), qc = circle_col(qq - 1 - i, rd, qq);
+                        const double x = vrow[pc], y = vrow[qc];
+                        vrow[pc] = r.x * x - r.y * y;
+                        vrow[qc] = r.y * x + r.x * y;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    if (row >= CT) return;
+    const int* ord = (const int*)(ws + pl.o_sig + CT);
+    double* B = ws + pl.o_Bn + (long long)row * KC;
+    for (int b = lane; b < KC; b += 32) B[b] = (row < q && b < rank) ? vrow[ord[b]] : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 GEMM tiles: C[M x N] = A[M x K] * B[K x N], views with strides.
+// ---------------------------------------------------------------------------
+struct GV {
+    const double* p;
+    long long rs, cs;
+};
+
+constexpr int GT = 64, GK = 16;
+
+__device__ void gemm_tile(GV A, GV B, double* C, long long crs, long long ccs, int M, int N, int K, int tm, int tn) {
+    __shared__ double sA[GK][GT + 1];
+    __shared__ double sB[GK][GT + 1];
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    const int m0 = tm * GT, n0 = tn * GT;
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+    for (int k0 = 0; k0 < K; k0 += GK) {
+        for (int e = tid; e < GT * GK; e += 256) {
+            const int r = e % GT, kk = e / GT;
+            const int gr = m0 + r, gk = k0 + kk;
+            sA[kk][r] = (gr < M && gk < K) ? A.p[(long long)gr * A.rs + (long long)gk * A.cs] : 0.0;
+        }
+        for (int e = tid; e < GT * GK; e += 256) {
+            const int kk = e % GK, cn = e / GK;
+            const int gk = k0 + kk, gc = n0 + cn;
+            sB[kk][cn] = (gk < K && gc < N) ? B.p[(long long)gk * B.rs + (long long)gc * B.cs] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < GK; kk++) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) a[i] = sA[kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; j++) b[j] = sB[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int gr = m0 + ty + 16 * i;
+        if (gr >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int gc = n0 + tx + 16 * j;
+            if (gc < N) C[(long long)gr * crs + (long long)gc * ccs] = acc[i][j];
+        }
+    }
+}
+
+// core[i+1] <- R * core[i+1]   (R = root factor, q x c, row-major CT)
+__global__ void __launch_bounds__(256) k_gemm_rx(const DevDesc* D, int i1, Plan pl, double* ws) {
+    if (pl.info->status) return;
+    const int q = pl.info->q, c = pl.info->c;
+    const int N = D->n[i1] * D->r[i1 + 1];
+    const int tm = blockIdx.x, tn = blockIdx.y;
+    if (tm * GT >= q) return;
+    for (int t = tn; t * GT < N; t += gridDim.y) {
+        GV A{ws + pl.o_Rn, pl.CT, 1};
+        GV B{D->core[i1], 1, c};
+        gemm_tile(A, B, D->alt[i1], 1, q, q, N, c, tm, t);
+    }
+}
+
+// core[i-1] <- core[i-1] * US   (US = c x rank, column-major ld CT)
+__global__ void __launch_bounds__(256) k_gemm_xm(const DevDesc* D, int im1, Plan pl, double* ws) {
+    if (pl.info->status) return;
+    const int c = pl.info->c, rank = pl.info->rank;
+    const int M = D->r[im1] * D->n[im1];
+    const int tn = blockIdx.y;
+    if (tn * GT >= rank) return;
+    for (int t = blockIdx.x; t * GT < M; t += gridDim.x) {
+        GV A{D->core[im1], 1, M};
+        GV B{ws + pl.o_US, 1, pl.CT};
+        gemm_tile(A, B, D->alt[im1], 1, M, M, rank, c, t, tn);
+    }
+}
+
+// publish a bond's new rank and swap the two rewritten cores
+__global__ void k_bond_finalize(DevDesc* D, int kq, int ka, int kb, const int* val, const Info* info) {
+    if (threadIdx.x == 0 && info->status == 0) {
+        D->r[kq] = *val;
+        double* t = D->core[ka];
+        D->core[ka] = D->alt[ka];
+        D->alt[ka] = t;
+        t = D->core[kb];
+        D->core[kb] = D->alt[kb];
+        D->alt[kb] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host planning
+// ---------------------------------------------------------------------------
+static int next_pow2(int v) {
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+struct Layout {
+    Plan pl;
+    long long bytes;
+};
+
+static void plan_bond(int CT, long long mcap, int KC, Plan* pl) {
+    int L = 2 * CT;
+    if (L < 128) L = 128;
+    L = (L + H - 1) / H * H;
+    long long P = (mcap + L - 1) / L;
+    while (P > 512) {
+        L *= 2;
+        P = (mcap + L - 1) / L;
+    }
+    pl->CT = CT;
+    pl->L = L;
+    pl->P = next_pow2((int)(P < 1 ? 1 : P));
+    pl->KL = 1 + (2 * L - 1 + H - 1) / H;
+    pl->NH = (CT + H - 1) / H;
+    pl->KC = KC;
+}
+
+static long long carve(Plan* pl, int PMAX, int LMAXKL) {
+    const int CT = pl->CT, KC = pl->KC;
+    long long o = 0;
+    auto take = [&](long long n) {
+        long long r = o;
+        o += (n + 31) / 32 * 32;
+        return r;
+    };
+    pl->o_tau_leaf = take((long long)PMAX * LMAXKL * CT);
+    pl->o_Rn = take((long long)(2 * PMAX - 1) * CT * CT);
+    pl->o_tau_node = take((long long)PMAX * pl->NH * CT);
+    pl->o_Bn = take((long long)(2 * PMAX - 1) * CT * KC);
+    pl->o_US = take((long long)CT * CT);
+    pl->o_rot = take((long long)MAXSW * (CT + 1) * ((CT + 2) / 2) * 2);
+    pl->o_sig = take(2LL * CT + 64);
+    pl->o_info_d = take(64);
+    pl->total = o;
+    return o;
+}
+
+template <int CT>
+static size_t factor_smem() {
+    return sizeof(double) * ((size_t)CT * (CT + 1) + (size_t)H * (CT + 1) + CT);
+}
+template <int CT>
+static size_t apply_smem() {
+    const int VR = CT > H ? CT : H;
+    return sizeof(double) * ((size_t)CT * KG + (size_t)VR * (CT + 1));
+}
+template <int CT>
+static size_t svd_smem() {
+    return sizeof(double) * (size_t)(CT + 2) * (CT + 1);
+}
+
+template <int CT>
+static int set_attrs() {
+    static bool done = false;
+    if (done) return PTT_OK;
+    PTT_CUDA(cudaFuncSetAttribute(k_tsqr_factor<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)factor_smem<CT>()));
+    PTT_CUDA(cudaFuncSetAttribute(k_apply_leaf<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)apply_smem<CT>()));
+    PTT_CUDA(cudaFuncSetAttribute(k_apply_node<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)apply_smem<CT>()));
+    PTT_CUDA(cudaFuncSetAttribute(k_svd_jacobi<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)svd_smem<CT>()));
+    done = true;
+    return PTT_OK;
+}
+
+// Factor the unfolding (mode) of core k; R lands at the root slot.
+template <int CT>
+static int launch_factor(ptt_ctx* c, ptt_tt* x, int k, int mode, Plan& pl, double* ws) {
+    k_tsqr_factor<CT><<<pl.P, NT, factor_smem<CT>(), c->stream>>>(x->dd, k, mode, pl, ws, c->d_status);
+    PTT_LAUNCHED(c);
+    return PTT_OK;
+}
+
+// out = Q * Bn[root]; k columns read from *kptr, at most kcap.
+template <int CT>
+static int launch_apply(ptt_ctx* c, ptt_tt* x, int k, int mode, Plan& pl, double* ws, const int* kptr, int kcap) {
+    const int kgroups = (kcap + KG - 1) / KG;
+    int first = 0, cnt = 1;
+    while (first + cnt <= pl.P - 1) {  // internal levels: nodes [first, first+cnt)
+        k_apply_node<CT><<<dim3(cnt, kgroups), NT, apply_smem<CT>(), c->stream>>>(pl, ws, first, kptr);
+        PTT_LAUNCHED(c);
+        first += cnt;
+        cnt *= 2;
+    }
+    k_apply_leaf<CT><<<dim3(pl.P, kgroups), NT, apply_smem<CT>(), c->stream>>>(x->dd, k, mode, pl, ws, kptr);
+    PTT_LAUNCHED(c);
+    return PTT_OK;
+}
+
+template <int CT>
+static int round_impl(ptt_tt* x, double delta, const int* maxr) {
+    ptt_ctx* c = x->ctx;
+    const int d = x->d;
+    int rc = set_attrs<CT>();
+    if (rc) return rc;
+    // plan: largest leaf count over all bonds decides the workspace
+    const int KC = (CT + KG - 1) / KG * KG;
+    int PMAX = 1, KLMAX = 1;
+    for (int i = 0; i < d; i++) {
+        Plan t;
+        long long ml = (long long)x->rcap[i] * x->n[i], mr = (long long)x->n[i] * x->rcap[i + 1];
+        plan_bond(CT, ml > mr ? ml : mr, KC, &t);
+        if (t.P > PMAX) PMAX = t.P;
+        if (t.KL > KLMAX) KLMAX = t.KL;
+    }
+    Plan base;
+    plan_bond(CT, 1, KC, &base);
+    base.NH = (CT + H - 1) / H;
+    long long total = carve(&base, PMAX, KLMAX);
+    size_t bytes = (size_t)total * sizeof(double) + 256;
+    if ((rc = ptt_ws_reserve(c, bytes))) return rc;
+    if ((rc = ptt_counters_reserve(c, (size_t)PMAX * 4 + 64))) return rc;
+    double* ws = (double*)c->ws;
+    // ints live after the doubles: qn [2P-1], pass [P], Info
+    int* ints = c->d_counters + PMAX;  // counters use [0, PMAX)
+    Info* info = (Info*)(ws + base.o_info_d);
+
+    auto mkplan = [&](long long mcap) {
+        Plan pl = base;
+        Plan t;
+        plan_bond(CT, mcap, KC, &t);
+        pl.L = t.L;
+        pl.P = t.P;
+        pl.KL = KLMAX;
+        pl.cnt = c->d_counters;
+        pl.qn = ints;
+        pl.pass = ints + 2 * PMAX;
+        pl.info = info;
+        return pl;
+    };
+
+    // left-to-right orthogonalisation
+    for (int i = 0; i < d - 1; i++) {
+        Plan pl = mkplan((long long)x->rcap[i] * x->n[i]);
+        if ((rc = launch_factor<CT>(c, x, i, LEFT, pl, ws))) return rc;
+        {
+            const long long ncap = (long long)x->n[i + 1] * x->rcap[i + 2];
+            int gy = (int)((ncap + GT - 1) / GT);
+            if (gy > 4096) gy = 4096;
+            k_gemm_rx<<<dim3((CT + GT - 1) / GT, gy), 256, 0, c->stream>>>(x->dd, i + 1, pl, ws);
+            PTT_LAUNCHED(c);
+        }
+        k_set_identity<<<32, 256, 0, c->stream>>>(pl, ws);
+        PTT_LAUNCHED(c);
+        if ((rc = launch_apply<CT>(c, x, i, LEFT, pl, ws, &info->q, CT))) return rc;
+        k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i, i + 1, &info->q, info);
+        PTT_LAUNCHED(c);
+    }
+    // right-to-left truncation
+    for (int i = d - 1; i >= 1; i--) {
+        Plan pl = mkplan((long long)x->n[i] * x->rcap[i + 1]);
+        if ((rc = launch_factor<CT>(c, x, i, RIGHT_T, pl, ws))) return rc;
+        const int mr = maxr ? maxr[i] : x->rcap[i];
+        k_svd_jacobi<CT><<<1, SVD_NT, svd_smem<CT>(), c->stream>>>(pl, ws, delta, mr, c->d_status);
+        PTT_LAUNCHED(c);
+        k_svd_replay<<<(CT + 7) / 8, 256, sizeof(double) * (8 * (CT + 2) + (CT + 2)), c->stream>>>(pl, ws);
+        PTT_LAUNCHED(c);
+        if ((rc = launch_apply<CT>(c, x, i, RIGHT_T, pl, ws, &info->rank, CT))) return rc;
+        {
+            const long long mcap = (long long)x->rcap[i - 1] * x->n[i - 1];
+            int gx = (int)((mcap + GT - 1) / GT);
+            if (gx > 4096) gx = 4096;
+            k_gemm_xm<<<dim3(gx, (CT + GT - 1) / GT), 256, 0, c->stream>>>(x->dd, i - 1, pl, ws);
+            PTT_LAUNCHED(c);
+        }
+        k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i, i, i - 1, &info->rank, info);
+        PTT_LAUNCHED(c);
+    }
+    return PTT_OK;
+}
+
+}  // namespace
+
+// Per-bond threshold of the reference applied to the unnormalised tensor.
+double ptt_round_threshold(const ptt_tt* x, double tol) {
+    const int d = x->d;
+    if (d < 2) return INFINITY;
+    double lg = 0.0;
+    for (int k = 0; k < d; k++) lg += log((double)x->n[k]);
+    return tol / sqrt(d - 1.0) * exp(0.5 * lg);
+}
+
+extern "C" int ptt_round(ptt_tt* x, double tol, const int* maxrank) {
+    if (!x) return ptt_set_error(PTT_ERR_ARG, "ptt_round: null tt");
+    if (x->d < 2) return PTT_OK;
+    if (!(tol >= 0.0)) return ptt_set_error(PTT_ERR_ARG, "ptt_round: tol must be >= 0");
+    int rmax = 1;
+    for (int k = 0; k <= x->d; k++) rmax = x->rcap[k] > rmax ? x->rcap[k] : rmax;
+    const double delta = ptt_round_threshold(x, tol);
+    cudaSetDevice(x->ctx->device);
+    if (rmax <= 32) return round_impl<32>(x, delta, maxrank);
+    if (rmax <= 64) return round_impl<64>(x, delta, maxrank);
+    if (rmax <= 128) return round_impl<128>(x, delta, maxrank);
+    return ptt_set_error(PTT_ERR_CAPACITY, "ptt_round: rank capacity %d > 128 not supported", rmax);
+}

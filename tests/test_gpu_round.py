@@ -1,0 +1,84 @@
+"""TT rounding (ptt_round, paratt_truncate semantics) on the GPU against the
+oracle on identical seeded inputs: ranks equal and the rounded tensors agree
+to 1e-12 of ||X|| (gauge-free comparison through inner products of the
+difference, which is formed as a TT and orthogonalised).  Inputs are built
+with a spectral gap at the cutoff so LAPACK and the GPU cannot disagree on a
+rank by round-off."""
+import numpy as np
+import pytest
+
+import paratt_b200 as P
+from oracle import tt_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def gapped_tt(dims, ranks, seed, keep, decay=1e-9):
+    """Random TT whose bond k has `keep[k]` singular values O(1) and the rest
+    ~decay: a left-orthonormal train with the first keep[k] columns scaled 1
+    and the others by decay."""
+    rng = np.random.default_rng(seed)
+    cores = []
+    for k, n in enumerate(dims):
+        r, r1 = ranks[k], ranks[k + 1]
+        a = rng.standard_normal((r * n, r1))
+        q, _ = np.linalg.qr(a)
+        s = np.ones(r1)
+        if k < len(dims) - 1:
+            s[keep[k + 1]:] = decay * (1 + rng.random(r1 - keep[k + 1]))
+        cores.append((q[:, :r1] * s).reshape(r, n, r1, order="F"))
+    return cores
+
+
+CASES = [
+    # dims, ranks, keep (per bond), rel tol, maxrank
+    ([6, 5, 7, 4, 6], [1, 6, 8, 9, 6, 1], [1, 3, 4, 5, 2, 1], 1e-6, 64),
+    ([4] * 8, [1, 4, 9, 12, 12, 12, 9, 4, 1], [1, 2, 3, 3, 4, 3, 2, 2, 1], 1e-6, 64),
+    ([32, 16, 8], [1, 20, 30, 1], [1, 5, 7, 1], 1e-6, 64),
+    ([10, 10, 10, 10], [1, 10, 40, 10, 1], [1, 6, 12, 6, 1], 1e-6, 8),   # rank cap binds
+    ([64, 64, 64], [1, 64, 64, 1], [1, 40, 50, 1], 1e-6, 64),           # CT = 64
+    ([20, 7, 20], [1, 20, 100, 1], [1, 15, 60, 1], 1e-6, 128),          # CT = 128
+]
+
+
+@pytest.mark.parametrize("dims,ranks,keep,rtol,maxr", CASES)
+def test_round_parity(ctx, dims, ranks, keep, rtol, maxr):
+    x = gapped_tt(dims, ranks, 11, keep)
+    tol = rtol * O.norm(x)
+    ref = O.round_tt(x, tol, maxr)
+    X = P.TT.from_cores(ctx, x)
+    X.round(tol, [maxr] * (len(dims) + 1))
+    got = X.get()
+    assert O.ranks_of(got) == O.ranks_of(ref)
+    assert O.rel_diff_exact(got, ref) <= 1e-12
+    # cores 1..d-1 right-orthonormal, as the reference leaves them
+    for c in got[1:]:
+        m = O.right_unfold(c)
+        np.testing.assert_allclose(m @ m.T, np.eye(m.shape[0]), atol=1e-12)
+
+
+def test_round_rank_deficient_sum(ctx):
+    """x + x has exactly rank-deficient unfoldings (the case CholeskyQR cannot
+    take); the result must be rank(x) with norm 2||x|| (round(a f + b f))."""
+    x = gapped_tt([8, 6, 8, 5], [1, 5, 7, 4, 1], 21, [1, 5, 7, 4, 1], decay=1.0)
+    z = O.axpby(1.0, x, 2.0, x)
+    tol = 1e-10 * O.norm(z)
+    ref = O.round_tt(z, tol, 64)
+    Z = P.TT.from_cores(ctx, z)
+    Z.round(tol)
+    got = Z.get()
+    assert O.ranks_of(got) == O.ranks_of(ref) == O.ranks_of(x)
+    assert abs(O.norm(got) / O.norm(x) - 3.0) < 1e-12
+    assert O.rel_diff_exact(got, ref) <= 1e-12
+
+
+def test_round_small_modes(ctx):
+    """Unfoldings with fewer rows than columns (q = m < c)."""
+    x = O.random_tt([2, 3, 2, 3, 2], [1, 2, 6, 6, 3, 1], 31)
+    tol = 1e-12 * O.norm(x)
+    ref = O.round_tt(x, tol, 64)
+    X = P.TT.from_cores(ctx, x)
+    X.round(tol)
+    got = X.get()
+    assert O.ranks_of(got) == O.ranks_of(ref)
+    assert O.rel_diff_exact(got, ref) <= 1e-12
