@@ -825,6 +825,7 @@ static long long carve(Plan* pl, int PMAX, int LMAXKL) {
     pl->o_rot = take((long long)MAXSW * (CT + 1) * ((CT + 2) / 2) * 2);
     pl->o_sig = take(2LL * CT + 64);
     pl->o_info_d = take(64);
+    pl->o_nodes = take((long long)(3 * PMAX + 64) / 2 + 1);  // qn [2P-1] and pass [P] as ints
     pl->total = o;
     return o;
 }
@@ -908,7 +909,9 @@ static int round_impl(ptt_tt* x, double delta, const int* maxr) {
     if ((rc = ptt_counters_reserve(c, (size_t)PMAX * 4 + 64))) return rc;
     double* ws = (double*)c->ws;
     // ints live after the doubles: qn [2P-1], pass [P], Info
-    int* ints = c->d_counters + PMAX;  // counters use [0, PMAX)
+    // Tree counters live alone in ctx->d_counters (zero between launches,
+    // reset by the combining block); node ranks and pass flags in ws.
+    int* ints = (int*)(ws + base.o_nodes);
     Info* info = (Info*)(ws + base.o_info_d);
 
     auto mkplan = [&](long long mcap) {

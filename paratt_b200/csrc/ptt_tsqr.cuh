@@ -74,7 +74,7 @@ struct Plan {
     int NH;          // chunks per tree node (= ceil(CT / H))
     int KC;          // column capacity of B (multiple of KG)
     // offsets (in doubles) into the workspace
-    long long o_tau_leaf, o_Rn, o_tau_node, o_Bn, o_US, o_rot, o_sig, o_info_d;
+    long long o_tau_leaf, o_Rn, o_tau_node, o_Bn, o_US, o_rot, o_sig, o_info_d, o_nodes;
     long long total;  // doubles
     int* qn;          // device ints [2P-1]
     int* pass;        // device ints [P-1]
