@@ -56,6 +56,27 @@ PTT_API int ptt_ctx_synchronize(ptt_ctx* ctx);
 PTT_API void* ptt_ctx_stream(ptt_ctx* ctx); /* the cudaStream_t, as void* */
 /* Launch counter: number of kernels this context has launched. */
 PTT_API long long ptt_ctx_launch_count(const ptt_ctx* ctx);
+/* Measurement: record event `slot` (0..63) on the context's stream; elapsed
+ * milliseconds between two recorded slots (waits for the second). */
+PTT_API int ptt_ctx_mark(ptt_ctx* ctx, int slot);
+PTT_API int ptt_ctx_elapsed(ptt_ctx* ctx, int a, int b, double* ms);
+/* Time every launch of one kernel class with an event pair (adds a few us
+ * per launch): PTT_TIME_TSQR (TSQR factor tree), PTT_TIME_SVD (bond SVD),
+ * PTT_TIME_GEMM (sketch contractions); 0 stops.  ptt_ctx_kernel_time
+ * resolves the pairs (synchronises) and returns total ms and launch count. */
+#define PTT_TIME_TSQR 1
+#define PTT_TIME_SVD 2
+#define PTT_TIME_GEMM 3
+PTT_API int ptt_ctx_time_kernels(ptt_ctx* ctx, int kind);
+PTT_API int ptt_ctx_kernel_time(ptt_ctx* ctx, double* ms, long long* count);
+/* Algorithmic work of the timed launches: bytes for PTT_TIME_TSQR (16 m c
+ * per factorisation of an m x c unfolding), flops for PTT_TIME_GEMM. */
+PTT_API int ptt_ctx_kernel_work(ptt_ctx* ctx, double* work);
+/* Overwrite a device buffer of twice the L2 size on the context's stream. */
+PTT_API int ptt_ctx_flush_l2(ptt_ctx* ctx);
+/* Page-lock / release host memory for fast transfers (cudaHostRegister). */
+PTT_API int ptt_host_pin(void* ptr, unsigned long long bytes);
+PTT_API int ptt_host_unpin(void* ptr);
 
 /* ---- tensor trains ----------------------------------------------------- */
 /* rank_cap has d+1 entries (rank_cap[0] = rank_cap[d] = 1). */
@@ -82,6 +103,13 @@ PTT_API int ptt_tt_device_cores(const ptt_tt* t, double** cores, int** ranks);
  * absolute on the grid-normalised norm ||X||_F / sqrt(prod n_k); per-bond
  * threshold tol/sqrt(d-1); maxrank has d+1 entries (NULL = capacity). */
 PTT_API int ptt_round(ptt_tt* x, double tol, const int* maxrank);
+/* Per-bond record of the context's last ptt_round (bond i = 1..d-1, record i;
+ * PTT_STAT_LEN doubles each): rank, numerical rank, Jacobi sweeps, q, r_i,
+ * dropped tail sum of squares, threshold, 0, then the top PTT_STAT_NSIG
+ * singular values of the bond (of the unnormalised tensor).  Synchronises. */
+#define PTT_STAT_NSIG 16
+#define PTT_STAT_LEN (8 + PTT_STAT_NSIG)
+PTT_API int ptt_round_stats(ptt_ctx* ctx, int d, double* out);
 /* z = a*x + b*y in formal form (attacFormalAXPBY, attac.c:81-112). */
 PTT_API int ptt_axpby(double a, const ptt_tt* x, double b, const ptt_tt* y, ptt_tt* z);
 /* z = x (.) y in formal form (attacHadamard, attac.c:128-136). */
@@ -91,6 +119,37 @@ PTT_API int ptt_mult_diag(ptt_tt* x, int mode, const double* vec);   /* paratt.c
 /* Centred periodic stencil along one mode (paratt.c:584-661); an even slen
  * is decremented.  slen <= 15. */
 PTT_API int ptt_stencil(ptt_tt* x, int mode, const double* sten, int slen);
+/* y = sum_i S_i x + shift*x where S_i applies the centred periodic stencil
+ * to mode i: an exact TT of rank 2 r_x (the formal sum of the d single-mode
+ * stencil applications has rank d r_x). */
+PTT_API int ptt_op_sum(const ptt_tt* x, const double* sten, int slen, double shift, ptt_tt* y);
+/* z = round(x (.) y) through a Gaussian TT sketch of ranks ell[k] (d+1
+ * entries, NULL = 72) without forming the rank r_x r_y product, then the
+ * deterministic truncation of ptt_round (tol, maxrank).  Reads the input
+ * ranks (synchronises).  Randomised: error ~ tail beyond ell, seeded. */
+PTT_API int ptt_round_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* ell,
+                               unsigned long long seed, double tol, const int* maxrank);
+
+/* ---- reaction-Burgers step-truncation RK2 ------------------------------- */
+typedef struct {
+    double dt;        /* time step                                            */
+    double tol;       /* absolute rounding tolerance (paratt_truncate meaning)  */
+    double nu;        /* diffusion coefficient                                */
+    double L;         /* box length, grid x_j = -L/2 + j L/n (periodic)         */
+    int maxrank;      /* rank cap of every rounding (<= 64)                   */
+    int sketch_pad;   /* product sketch rank = maxrank + sketch_pad            */
+    unsigned long long seed;
+} ptt_rxn_params;
+typedef struct ptt_rxn_ws ptt_rxn_ws;
+PTT_API ptt_rxn_ws* ptt_rxn_ws_create(ptt_ctx* ctx, int d, const int* n, int maxrank);
+PTT_API void ptt_rxn_ws_destroy(ptt_rxn_ws* ws);
+PTT_API int ptt_rxn_ws_counts(const ptt_rxn_ws* ws, long long* formal, long long* sketch);
+/* F = nu sum d2_i u - (1/d) sum d1_i (u^2/2) + u - u^2, rounded (see
+ * paratt_b200/csrc/host/rxn_burgers.c for the composition). */
+PTT_API int ptt_rxn_burgers_F(ptt_tt* u, ptt_tt* F, ptt_rxn_ws* ws, const ptt_rxn_params* p);
+/* u <- one step-truncation midpoint step of the reaction-Burgers equation. */
+PTT_API int ptt_rxn_burgers_rk2_step(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p);
+
 /* Reductions (these read a scalar back, so they synchronise). */
 PTT_API int ptt_dot(const ptt_tt* x, const ptt_tt* y, double* out);  /* <X,Y>/prod n */
 PTT_API int ptt_norm(const ptt_tt* x, double* out);                  /* RMS norm     */

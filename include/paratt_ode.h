@@ -40,6 +40,13 @@ void pattac_exp_midpoint_st(paratt* f_old_ptt, paratt* f_new_ptt, paratt* work_p
                             void (*vecField)(paratt*, paratt*, int, ...), double dt, double eps_1,
                             double eps_2, double eps_3);
 
+/* Extension: one step-truncation midpoint step of the reaction-Burgers
+ * equation u_t = 0.05 lap u - (1/d) sum_i d_i(u^2/2) + u(1-u) on the periodic
+ * box [-5,5)^d (second-order central differences), in place on f's host
+ * cores; tol is absolute (paratt_truncate semantics) for every rounding.
+ * The vector field and step are listed in paratt_b200/csrc/host/rxn_burgers.c. */
+void pattac_rxn_burgers_midpoint_st(paratt* f, double dt, double tol, int maxrank);
+
 #ifdef __cplusplus
 }
 #endif

@@ -284,3 +284,103 @@ def random_tt(dims, ranks, seed, std=1.0):
     rng = np.random.default_rng(seed)
     return [rng.standard_normal((ranks[k], dims[k], ranks[k + 1])) * std
             for k in range(len(dims))]
+
+
+# --------------------------------------------------------------------------
+# reaction-Burgers step-truncation RK2 (composition of the primitives above)
+# --------------------------------------------------------------------------
+def op_sum_apply(x, stens, shift=0.0):
+    """Y = sum_i S_i x + shift * x, S_i = periodic stencil stens[i] on mode i.
+
+    Exact rank-2r TT of the sum of d mode-local operators (the formal sum of
+    the d stencil applications of attac_apply_periodic_stencil, paratt.c:584,
+    has rank d*r and represents the same tensor).  Core k has 2x2 blocks
+    indexed by (applied-before-k, applied-up-to-k): [[x_k, S_k x_k], [0, x_k]];
+    the first core keeps block row 0, the last keeps block column 1, and the
+    shift is added to the block S_0 x_0.  For d == 1 it is (S_0 + shift) x_0."""
+    d = len(x)
+    if d == 1:
+        return [periodic_stencil_core(x[0], stens[0]) + shift * x[0]]
+    out = []
+    for k in range(d):
+        r, n, r1 = x[k].shape
+        sx = periodic_stencil_core(x[k], stens[k])
+        if k == 0:
+            out.append(np.concatenate([x[0], sx + shift * x[0]], axis=2))
+        elif k == d - 1:
+            out.append(np.concatenate([sx, x[k]], axis=0))
+        else:
+            c = np.zeros((2 * r, n, 2 * r1))
+            c[:r, :, :r1] = x[k]
+            c[:r, :, r1:] = sx
+            c[r:, :, r1:] = x[k]
+            out.append(c)
+    return out
+
+
+def burgers_stencils(d, n, L=10.0, nu=0.05):
+    """Second-order central differences on the periodic grid x_j = -L/2 + j h,
+    h = L/n: nu*[1,-2,1]/h^2 (diffusion) and -(1/d)*[-1,0,1]/(2h) applied to
+    u^2/2 (Burgers flux), i.e. -(1/(2d))*[-1,0,1]/(2h) applied to u*u."""
+    h = L / n
+    d2 = [nu / h**2, -2.0 * nu / h**2, nu / h**2]
+    d1 = [1.0 / (4.0 * d * h), 0.0, -1.0 / (4.0 * d * h)]
+    return d2, d1
+
+
+def rxn_burgers_F(u, tol, maxr, L=10.0, nu=0.05):
+    """F(u) = nu sum_i D2_i u - (1/d) sum_i D1_i (u^2/2) + u - u^2, every
+    intermediate rounded with paratt_truncate semantics (absolute tol):
+      w = T(u . u);  a = T(nu sum D2 u + u);  b = T(-(1/2d) sum D1 w - w)
+      F = T(a + b)"""
+    d = len(u)
+    n = u[0].shape[1]
+    d2, d1 = burgers_stencils(d, n, L, nu)
+    w = round_tt(hadamard(u, u), tol, maxr)
+    a = round_tt(op_sum_apply(u, [d2] * d, 1.0), tol, maxr)
+    b = round_tt(op_sum_apply(w, [d1] * d, -1.0), tol, maxr)
+    return round_tt(axpby(1.0, a, 1.0, b), tol, maxr)
+
+
+def rxn_burgers_rk2_step(u, dt, tol, maxr, L=10.0, nu=0.05):
+    """Step-truncation explicit midpoint (paratt_ode.h:77-112) with the stage
+    rounded too: f_s = T(u + dt/2 F(u)); u+ = T(u + dt F(f_s))."""
+    k1 = rxn_burgers_F(u, tol, maxr, L, nu)
+    us = round_tt(axpby(1.0, u, 0.5 * dt, k1), tol, maxr)
+    k2 = rxn_burgers_F(us, tol, maxr, L, nu)
+    return round_tt(axpby(1.0, u, dt, k2), tol, maxr)
+
+
+def grid(n, L=10.0):
+    return -L / 2 + np.arange(n) * (L / n)
+
+
+def gaussian_sum_ic(d, n, centres, widths, L=10.0):
+    """sum_g prod_i exp(-(x_i - c_gi)^2 / (2 w_g^2)) as a rank-G TT
+    (attac_sum_of_product layout: core 0 = [v_0 | v_1 | ...], diagonal
+    interior cores, stacked last core; paratt.c:517-568)."""
+    x = grid(n, L)
+    G = len(widths)
+    cores = []
+    for k in range(d):
+        vecs = [np.exp(-(x - centres[g][k]) ** 2 / (2 * widths[g] ** 2)) for g in range(G)]
+        if G == 1:
+            cores.append(vecs[0].reshape(1, n, 1))
+        elif k == 0:
+            cores.append(np.stack(vecs, axis=1).reshape(1, n, G))
+        elif k == d - 1:
+            cores.append(np.stack(vecs, axis=0).reshape(G, n, 1))
+        else:
+            c = np.zeros((G, n, G))
+            for g in range(G):
+                c[g, :, g] = vecs[g]
+            cores.append(c)
+    return cores
+
+
+def config_ic(d, n, ngauss, seed, L=10.0):
+    """Seeded sum of Gaussians: centres U[-2,2]^d, widths U[0.3,0.8]."""
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(-2.0, 2.0, size=(ngauss, d))
+    widths = rng.uniform(0.3, 0.8, size=ngauss)
+    return gaussian_sum_ic(d, n, centres, widths, L)

@@ -20,6 +20,10 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libparatt_b200.so")
 
+TIME_TSQR, TIME_SVD, TIME_GEMM = 1, 2, 3
+STAT_NSIG = 16
+STAT_LEN = 8 + STAT_NSIG
+
 PTT_OK, PTT_ERR_ARG, PTT_ERR_CUDA, PTT_ERR_CAPACITY, PTT_ERR_NUMERIC, PTT_ERR_NOGPU, PTT_ERR_TIMEOUT = range(7)
 
 
@@ -57,6 +61,7 @@ _SIGS = {
     "ptt_tt_copy": (_i, [_p, _p]),
     "ptt_tt_device_cores": (_i, [_p, _dpp, C.POINTER(_ip)]),
     "ptt_round": (_i, [_p, _d, _ip]),
+    "ptt_round_stats": (_i, [_p, _i, _dp]),
     "ptt_axpby": (_i, [_d, _p, _d, _p, _p]),
     "ptt_hadamard": (_i, [_p, _p, _p]),
     "ptt_scale": (_i, [_d, _p]),
@@ -65,7 +70,28 @@ _SIGS = {
     "ptt_dot": (_i, [_p, _p, _dp]),
     "ptt_norm": (_i, [_p, _dp]),
     "ptt_entry": (_i, [_p, _ip, _dp]),
+    "ptt_op_sum": (_i, [_p, _dp, _i, _d, _p]),
+    "ptt_ctx_mark": (_i, [_p, _i]),
+    "ptt_ctx_elapsed": (_i, [_p, _i, _i, _dp]),
+    "ptt_ctx_time_kernels": (_i, [_p, _i]),
+    "ptt_ctx_kernel_time": (_i, [_p, _dp, C.POINTER(C.c_longlong)]),
+    "ptt_ctx_kernel_work": (_i, [_p, _dp]),
+    "ptt_ctx_flush_l2": (_i, [_p]),
+    "ptt_host_pin": (_i, [_p, C.c_ulonglong]),
+    "ptt_host_unpin": (_i, [_p]),
+    "ptt_round_hadamard": (_i, [_p, _p, _p, _ip, C.c_ulonglong, _d, _ip]),
+    "ptt_rxn_ws_create": (_p, [_p, _i, _ip, _i]),
+    "ptt_rxn_ws_destroy": (None, [_p]),
+    "ptt_rxn_ws_counts": (_i, [_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "ptt_rxn_burgers_F": (_i, [_p, _p, _p, _p]),
+    "ptt_rxn_burgers_rk2_step": (_i, [_p, _p, _p]),
 }
+
+
+class RxnParams(C.Structure):
+    """ptt_rxn_params (include/paratt_b200.h)."""
+    _fields_ = [("dt", C.c_double), ("tol", C.c_double), ("nu", C.c_double), ("L", C.c_double),
+                ("maxrank", C.c_int), ("sketch_pad", C.c_int), ("seed", C.c_ulonglong)]
 
 
 def lib():
@@ -103,6 +129,38 @@ class Context:
 
     def sync(self):
         _check(lib().ptt_ctx_synchronize(self.h))
+
+    def round_stats(self, d):
+        """Per-bond records of the last rounding on this context: array of
+        shape (d, PTT_STAT_LEN) (row i = bond i; row 0 unused)."""
+        out = np.zeros((d, STAT_LEN))
+        _check(lib().ptt_round_stats(self.h, d, out.ctypes.data_as(_dp)))
+        return out
+
+    def mark(self, slot):
+        _check(lib().ptt_ctx_mark(self.h, slot))
+
+    def elapsed_ms(self, a, b):
+        v = C.c_double()
+        _check(lib().ptt_ctx_elapsed(self.h, a, b, C.byref(v)))
+        return v.value
+
+    def time_kernels(self, kind):
+        """Event-time every launch of one kernel class (TIME_TSQR/SVD/GEMM)."""
+        _check(lib().ptt_ctx_time_kernels(self.h, kind))
+
+    def kernel_time(self):
+        ms, n = C.c_double(), C.c_longlong()
+        _check(lib().ptt_ctx_kernel_time(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def kernel_work(self):
+        w = C.c_double()
+        _check(lib().ptt_ctx_kernel_work(self.h, C.byref(w)))
+        return w.value
+
+    def flush_l2(self):
+        _check(lib().ptt_ctx_flush_l2(self.h))
 
     @property
     def stream(self):
@@ -213,3 +271,45 @@ def axpby(a, x: TT, b, y: TT, z: TT):
 def hadamard(x: TT, y: TT, z: TT):
     _check(lib().ptt_hadamard(x.h, y.h, z.h))
     return z
+
+
+def op_sum(x: TT, sten, shift, y: TT):
+    s = np.ascontiguousarray(sten, dtype=np.float64)
+    _check(lib().ptt_op_sum(x.h, s.ctypes.data_as(_dp), len(s), float(shift), y.h))
+    return y
+
+
+def round_hadamard(x: TT, y: TT, z: TT, ell, seed, tol, maxrank=None):
+    e = _iarr(ell if hasattr(ell, "__len__") else [ell] * (x.d + 1))
+    mr = None if maxrank is None else _iarr(maxrank if hasattr(maxrank, "__len__") else [maxrank] * (x.d + 1))
+    _check(lib().ptt_round_hadamard(x.h, y.h, z.h, e, C.c_ulonglong(seed), float(tol), mr))
+    return z
+
+
+class RxnBurgers:
+    """Device workspace + parameters of the reaction-Burgers RK2 step."""
+
+    def __init__(self, ctx: Context, d, n, maxrank, dt, tol, nu=0.05, L=10.0, sketch_pad=8, seed=1):
+        self.ctx = ctx
+        self.p = RxnParams(dt, tol, nu, L, maxrank, sketch_pad, seed)
+        self.h = lib().ptt_rxn_ws_create(ctx.h, d, _iarr([n] * d), maxrank)
+        if not self.h:
+            _check(lib().ptt_last_error() or PTT_ERR_ARG)
+
+    def F(self, u: TT, out: TT):
+        _check(lib().ptt_rxn_burgers_F(u.h, out.h, self.h, C.byref(self.p)))
+        return out
+
+    def step(self, u: TT):
+        _check(lib().ptt_rxn_burgers_rk2_step(u.h, self.h, C.byref(self.p)))
+        return u
+
+    def counts(self):
+        f, s = C.c_longlong(), C.c_longlong()
+        _check(lib().ptt_rxn_ws_counts(self.h, C.byref(f), C.byref(s)))
+        return f.value, s.value
+
+    def close(self):
+        if self.h:
+            lib().ptt_rxn_ws_destroy(self.h)
+            self.h = None

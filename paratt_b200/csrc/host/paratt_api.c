@@ -485,3 +485,41 @@ paratt* pattac_load_tt_folder(char* folder, int ndims) {
     free(r);
     return p;
 }
+
+/* ------------------------------------------------------------------------ */
+/* reaction-Burgers midpoint step on host cores (extension)                 */
+/* ------------------------------------------------------------------------ */
+static ptt_rxn_ws* g_rxn = NULL;
+static int g_rxn_d = 0, g_rxn_n = 0, g_rxn_maxr = 0;
+
+void pattac_rxn_burgers_midpoint_st(paratt* f, double dt, double tol, int maxrank) {
+    attac_tt* x = f->x;
+    for (int k = 1; k < x->numDim; k++)
+        if (x->dim[k] != x->dim[0]) {
+            fprintf(stderr, "paratt_b200: rxn-burgers step needs one grid size for every mode\n");
+            g_err = PTT_ERR_ARG;
+            return;
+        }
+    if (!g_rxn || g_rxn_d != x->numDim || g_rxn_n != x->dim[0] || g_rxn_maxr != maxrank) {
+        ptt_rxn_ws_destroy(g_rxn);
+        g_rxn = ptt_rxn_ws_create(ctx(), x->numDim, x->dim, maxrank);
+        if (!g_rxn) fail("rxn workspace");
+        g_rxn_d = x->numDim;
+        g_rxn_n = x->dim[0];
+        g_rxn_maxr = maxrank;
+    }
+    int cap[PTT_MAX_DIM + 1];
+    for (int k = 0; k <= x->numDim; k++) cap[k] = (k == 0 || k == x->numDim) ? 1 : 2 * maxrank;
+    ptt_tt* m = mirror(x, cap);
+    if (check(ptt_tt_set(m, x->ttRank, (const double* const*)x->coreList), "upload")) fail("upload");
+    ptt_rxn_params p;
+    p.dt = dt;
+    p.tol = tol;
+    p.nu = 0.05;
+    p.L = 10.0;
+    p.maxrank = maxrank;
+    p.sketch_pad = 8;
+    p.seed = 0x5eed;
+    if (check(ptt_rxn_burgers_rk2_step(m, g_rxn, &p), "rxn-burgers step")) return;
+    download(x, m);
+}

@@ -36,11 +36,29 @@ struct ptt_ctx {
     // generic device workspace (grown on demand, never shrunk)
     void* ws;
     size_t ws_bytes;
+    void* ws2;                    // second workspace (sketch contractions)
+    size_t ws2_bytes;
     int* d_counters;              // zeroed, self-resetting tree counters
     size_t counters_n;
     double* d_scalars;            // small scratch for reductions
     double* h_scalars;            // pinned mirror
+    double* d_stats;              // per-bond record of the last rounding (PTT_STAT_LEN doubles each)
+    // measurement: user marks and per-launch timing of one kernel class
+    cudaEvent_t marks[64];
+    int tkind;                    // PTT_TIME_* class being timed (0 = none)
+    cudaEvent_t* tev;             // 2 events per timed launch
+    int tcount, tcap;
+    double tms;                   // accumulated milliseconds of resolved launches
+    long long tlaunches;
+    double* d_work;               // device accumulators of algorithmic work per class [4]
+    double hwork[4];              // host-known algorithmic work per class
+    void* flush;                  // L2 flush buffer
+    size_t flush_bytes;
 };
+
+// Event pair around a launch of kind `kind` when that class is being timed.
+void ptt_time_begin(ptt_ctx* c, int kind);
+void ptt_time_end(ptt_ctx* c, int kind);
 
 struct ptt_tt {
     ptt_ctx* ctx;
@@ -74,9 +92,18 @@ int ptt_cuda_check(cudaError_t e, const char* what);
 // Workspace: returns a device pointer with at least `bytes`, 256-aligned.
 int ptt_ws_reserve(ptt_ctx* ctx, size_t bytes);
 int ptt_counters_reserve(ptt_ctx* ctx, size_t n);
+int ptt_ws2_reserve(ptt_ctx* ctx, size_t bytes);
+int ptt_pull_desc(ptt_tt* t);
+int ptt_push_desc(ptt_tt* t);
+int ptt_set_ranks_async(ptt_tt* t, int k0, const int* vals, int cnt);
 
 // Swap core[k] <-> alt[k] for k in [k0, k1).
 int ptt_swap(ptt_tt* t, int k0, int k1);
+
+// Rounding stages (ptt_round.cu): phases 1 = orthogonalise, 2 = truncate
+// (input left-orthogonal), 4 = QR of core `only` alone.
+int ptt_round_phases(ptt_tt* x, double tol, const int* maxrank, int phases, int only);
+double ptt_round_threshold(const ptt_tt* x, double tol);
 
 // Round a size up to a multiple of 256 bytes.
 static inline size_t ptt_align(size_t b) { return (b + 255) & ~(size_t)255; }

@@ -63,7 +63,11 @@ extern "C" ptt_ctx* ptt_ctx_create(int device) {
         ptt_cuda_check(cudaMalloc(&c->d_status, sizeof(int)), "cudaMalloc status") ||
         ptt_cuda_check(cudaMemset(c->d_status, 0, sizeof(int)), "memset") ||
         ptt_cuda_check(cudaMalloc(&c->d_scalars, 512 * sizeof(double)), "cudaMalloc scalars") ||
-        ptt_cuda_check(cudaMallocHost(&c->h_scalars, 512 * sizeof(double)), "cudaMallocHost")) {
+        ptt_cuda_check(cudaMallocHost(&c->h_scalars, 512 * sizeof(double)), "cudaMallocHost") ||
+        ptt_cuda_check(cudaMalloc(&c->d_stats, sizeof(double) * PTT_STAT_LEN * (PTT_MAX_DIM + 1)), "cudaMalloc stats") ||
+        ptt_cuda_check(cudaMalloc(&c->d_work, sizeof(double) * 4), "cudaMalloc work") ||
+        ptt_cuda_check(cudaMemset(c->d_work, 0, sizeof(double) * 4), "memset") ||
+        ptt_cuda_check(cudaMemset(c->d_stats, 0, sizeof(double) * PTT_STAT_LEN * (PTT_MAX_DIM + 1)), "memset")) {
         free(c);
         return NULL;
     }
@@ -76,10 +80,18 @@ extern "C" void ptt_ctx_destroy(ptt_ctx* c) {
     cudaStreamSynchronize(c->stream);
     cudaStreamSynchronize(c->side);
     cudaFree(c->ws);
+    cudaFree(c->ws2);
     cudaFree(c->d_counters);
     cudaFree(c->d_status);
     cudaFree(c->d_scalars);
+    cudaFree(c->d_stats);
+    cudaFree(c->d_work);
     cudaFreeHost(c->h_scalars);
+    for (int i = 0; i < 64; i++)
+        if (c->marks[i]) cudaEventDestroy(c->marks[i]);
+    for (int i = 0; i < 2 * c->tcap; i++) cudaEventDestroy(c->tev[i]);
+    free(c->tev);
+    cudaFree(c->flush);
     cudaEventDestroy(c->ev_fork);
     cudaEventDestroy(c->ev_join);
     cudaStreamDestroy(c->stream);
@@ -88,6 +100,111 @@ extern "C" void ptt_ctx_destroy(ptt_ctx* c) {
 }
 
 extern "C" void* ptt_ctx_stream(ptt_ctx* c) { return c ? (void*)c->stream : NULL; }
+
+// ---------------------------------------------------------------------------
+// measurement helpers
+// ---------------------------------------------------------------------------
+extern "C" int ptt_ctx_mark(ptt_ctx* c, int slot) {
+    if (!c || slot < 0 || slot >= 64) return ptt_set_error(PTT_ERR_ARG, "ptt_ctx_mark: bad slot");
+    if (!c->marks[slot]) PTT_CUDA(cudaEventCreate(&c->marks[slot]));
+    PTT_CUDA(cudaEventRecord(c->marks[slot], c->stream));
+    return PTT_OK;
+}
+
+extern "C" int ptt_ctx_elapsed(ptt_ctx* c, int a, int b, double* ms) {
+    if (!c || a < 0 || a >= 64 || b < 0 || b >= 64 || !c->marks[a] || !c->marks[b] || !ms)
+        return ptt_set_error(PTT_ERR_ARG, "ptt_ctx_elapsed: bad slots");
+    PTT_CUDA(cudaEventSynchronize(c->marks[b]));
+    float f = 0.f;
+    PTT_CUDA(cudaEventElapsedTime(&f, c->marks[a], c->marks[b]));
+    *ms = f;
+    return PTT_OK;
+}
+
+void ptt_time_begin(ptt_ctx* c, int kind) {
+    if (c->tkind != kind || kind == 0) return;
+    if (c->tcount >= c->tcap) {
+        int ncap = c->tcap ? 2 * c->tcap : 1024;
+        cudaEvent_t* ev = (cudaEvent_t*)realloc(c->tev, sizeof(cudaEvent_t) * 2 * ncap);
+        for (int i = 2 * c->tcap; i < 2 * ncap; i++) cudaEventCreate(&ev[i]);
+        c->tev = ev;
+        c->tcap = ncap;
+    }
+    cudaEventRecord(c->tev[2 * c->tcount], c->stream);
+}
+
+void ptt_time_end(ptt_ctx* c, int kind) {
+    if (c->tkind != kind || kind == 0) return;
+    cudaEventRecord(c->tev[2 * c->tcount + 1], c->stream);
+    c->tcount++;
+}
+
+extern "C" int ptt_ctx_time_kernels(ptt_ctx* c, int kind) {
+    if (!c) return ptt_set_error(PTT_ERR_ARG, "null context");
+    c->tkind = kind;
+    c->tcount = 0;
+    c->tms = 0.0;
+    c->tlaunches = 0;
+    for (int i = 0; i < 4; i++) c->hwork[i] = 0.0;
+    PTT_CUDA(cudaMemsetAsync(c->d_work, 0, sizeof(double) * 4, c->stream));
+    return PTT_OK;
+}
+
+// Resolve the recorded launches: total milliseconds and launch count since
+// ptt_ctx_time_kernels (synchronises).
+extern "C" int ptt_ctx_kernel_work(ptt_ctx* c, double* work) {
+    if (!c || !work) return ptt_set_error(PTT_ERR_ARG, "bad arguments");
+    double w[4];
+    PTT_CUDA(cudaStreamSynchronize(c->stream));
+    PTT_CUDA(cudaMemcpy(w, c->d_work, sizeof(w), cudaMemcpyDeviceToHost));
+    const int k = c->tkind;
+    *work = (k >= 0 && k < 4) ? w[k] + c->hwork[k] : 0.0;
+    return PTT_OK;
+}
+
+extern "C" int ptt_ctx_kernel_time(ptt_ctx* c, double* ms, long long* count) {
+    if (!c) return ptt_set_error(PTT_ERR_ARG, "null context");
+    PTT_CUDA(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < c->tcount; i++) {
+        float f = 0.f;
+        PTT_CUDA(cudaEventElapsedTime(&f, c->tev[2 * i], c->tev[2 * i + 1]));
+        c->tms += f;
+    }
+    c->tlaunches += c->tcount;
+    c->tcount = 0;
+    if (ms) *ms = c->tms;
+    if (count) *count = c->tlaunches;
+    return PTT_OK;
+}
+
+__global__ void k_flush(double* p, long long n, double v) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+// Overwrite a buffer twice the size of L2 so the next kernel starts cold.
+extern "C" int ptt_ctx_flush_l2(ptt_ctx* c) {
+    if (!c) return ptt_set_error(PTT_ERR_ARG, "null context");
+    if (!c->flush) {
+        int l2 = 0;
+        PTT_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, c->device));
+        c->flush_bytes = (size_t)(l2 > 0 ? l2 : (128 << 20)) * 2;
+        PTT_CUDA(cudaMalloc(&c->flush, c->flush_bytes));
+    }
+    k_flush<<<1184, 256, 0, c->stream>>>((double*)c->flush, (long long)(c->flush_bytes / 8), 0.0);
+    PTT_LAUNCHED(c);
+    return PTT_OK;
+}
+
+extern "C" int ptt_host_pin(void* p, unsigned long long bytes) {
+    PTT_CUDA(cudaHostRegister(p, bytes, cudaHostRegisterDefault));
+    return PTT_OK;
+}
+
+extern "C" int ptt_host_unpin(void* p) {
+    PTT_CUDA(cudaHostUnregister(p));
+    return PTT_OK;
+}
 extern "C" long long ptt_ctx_launch_count(const ptt_ctx* c) { return c ? c->launches : 0; }
 
 extern "C" int ptt_ctx_synchronize(ptt_ctx* c) {
@@ -117,6 +234,29 @@ int ptt_ws_reserve(ptt_ctx* c, size_t bytes) {
     size_t b = ptt_align(bytes + bytes / 4);
     PTT_CUDA(cudaMalloc(&c->ws, b));
     c->ws_bytes = b;
+    return PTT_OK;
+}
+
+int ptt_ws2_reserve(ptt_ctx* c, size_t bytes) {
+    if (bytes <= c->ws2_bytes) return PTT_OK;
+    PTT_CUDA(cudaStreamSynchronize(c->stream));
+    PTT_CUDA(cudaStreamSynchronize(c->side));
+    if (c->ws2) PTT_CUDA(cudaFree(c->ws2));
+    c->ws2 = NULL;
+    c->ws2_bytes = 0;
+    size_t b = ptt_align(bytes + bytes / 4);
+    PTT_CUDA(cudaMalloc(&c->ws2, b));
+    c->ws2_bytes = b;
+    return PTT_OK;
+}
+
+// Write ranks r[k0 .. k0+cnt) of the device descriptor (stream-ordered).
+int ptt_set_ranks_async(ptt_tt* t, int k0, const int* vals, int cnt) {
+    int* h = (int*)(t->ctx->h_scalars + 256);  // pinned staging (second half)
+    cudaStreamSynchronize(t->ctx->stream);
+    memcpy(h, vals, sizeof(int) * cnt);
+    PTT_CUDA(cudaMemcpyAsync(t->dd->r + k0, h, sizeof(int) * cnt, cudaMemcpyHostToDevice, t->ctx->stream));
+    PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
     return PTT_OK;
 }
 
@@ -201,14 +341,14 @@ extern "C" int ptt_tt_shape(const ptt_tt* t, int* d, int* n, int* rank_cap) {
 }
 
 // Pull the device descriptor (current buffer order and ranks) to the host.
-static int pull_desc(ptt_tt* t) {
+int ptt_pull_desc(ptt_tt* t) {
     PTT_CUDA(cudaStreamSynchronize(t->ctx->side));
     PTT_CUDA(cudaMemcpyAsync(&t->hd, t->dd, sizeof(DevDesc), cudaMemcpyDeviceToHost, t->ctx->stream));
     PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
     return PTT_OK;
 }
 
-static int push_desc(ptt_tt* t) {
+int ptt_push_desc(ptt_tt* t) {
     PTT_CUDA(cudaMemcpyAsync(t->dd, &t->hd, sizeof(DevDesc), cudaMemcpyHostToDevice, t->ctx->stream));
     return PTT_OK;
 }
@@ -220,7 +360,7 @@ extern "C" int ptt_tt_reserve(ptt_tt* t, const int* rank_cap) {
     if (!grow) return PTT_OK;
     if (rank_cap[0] != 1 || rank_cap[t->d] != 1)
         return ptt_set_error(PTT_ERR_ARG, "ptt_tt_reserve: boundary ranks must be 1");
-    int rc = pull_desc(t);
+    int rc = ptt_pull_desc(t);
     if (rc) return rc;
     for (int k = 0; k <= t->d; k++)
         if (rank_cap[k] > t->rcap[k]) t->rcap[k] = t->hd.rcap[k] = rank_cap[k];
@@ -239,7 +379,7 @@ extern "C" int ptt_tt_reserve(ptt_tt* t, const int* rank_cap) {
         t->hd.alt[k] = na;
         t->cap[k] = t->hd.cap[k] = cap;
     }
-    rc = push_desc(t);
+    rc = ptt_push_desc(t);
     if (rc) return rc;
     PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
     return PTT_OK;
@@ -259,7 +399,7 @@ extern "C" int ptt_tt_set(ptt_tt* t, const int* ranks, const double* const* core
         int e = ptt_tt_reserve(t, rc);
         if (e) return e;
     }
-    int rc = pull_desc(t);
+    int rc = ptt_pull_desc(t);
     if (rc) return rc;
     for (int k = 0; k < t->d; k++) {
         size_t cnt = (size_t)ranks[k] * t->n[k] * ranks[k + 1];
@@ -267,7 +407,7 @@ extern "C" int ptt_tt_set(ptt_tt* t, const int* ranks, const double* const* core
                                  t->ctx->stream));
     }
     for (int k = 0; k <= t->d; k++) t->hd.r[k] = ranks[k];
-    rc = push_desc(t);
+    rc = ptt_push_desc(t);
     if (rc) return rc;
     PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
     return PTT_OK;
@@ -285,7 +425,7 @@ extern "C" int ptt_tt_get_ranks(ptt_tt* t, int* ranks) {
 
 extern "C" int ptt_tt_get(ptt_tt* t, int* ranks, double* const* cores) {
     if (!t) return ptt_set_error(PTT_ERR_ARG, "ptt_tt_get: null tt");
-    int rc = pull_desc(t);
+    int rc = ptt_pull_desc(t);
     if (rc) return rc;
     if (ranks) memcpy(ranks, t->hd.r, sizeof(int) * (t->d + 1));
     if (cores) {
@@ -301,7 +441,7 @@ extern "C" int ptt_tt_get(ptt_tt* t, int* ranks, double* const* cores) {
 
 extern "C" int ptt_tt_device_cores(const ptt_tt* t, double** cores, int** ranks) {
     if (!t) return ptt_set_error(PTT_ERR_ARG, "null tt");
-    int rc = pull_desc((ptt_tt*)t);
+    int rc = ptt_pull_desc((ptt_tt*)t);
     if (rc) return rc;
     if (cores)
         for (int k = 0; k < t->d; k++) cores[k] = t->hd.core[k];

@@ -112,6 +112,32 @@ __global__ void k_axpby(const DevDesc* X, const DevDesc* Y, DevDesc* Z, double a
     }
 }
 
+// Make z's rank capacity cover an op's output.  need[] is the bound from the
+// inputs' capacities; when z already covers it nothing happens (no sync).
+// Otherwise the inputs' actual ranks are read back (synchronises) and z is
+// grown only to the exact output ranks: op 0 = sum (r_x + r_y), 1 = product,
+// 2 = operator sum (2 r_x; y unused).
+static int fit_output(ptt_tt* z, const int* need, const ptt_tt* x, const ptt_tt* y, int op) {
+    const int d = z->d;
+    int ok = 1;
+    for (int k = 0; k <= d; k++) ok &= need[k] <= z->rcap[k];
+    if (ok) return PTT_OK;
+    int rx[PTT_MAX_DIM + 1], ry[PTT_MAX_DIM + 1], ex[PTT_MAX_DIM + 1];
+    int rc;
+    if ((rc = ptt_tt_get_ranks((ptt_tt*)x, rx))) return rc;
+    if (op != 2 && (rc = ptt_tt_get_ranks((ptt_tt*)y, ry))) return rc;
+    for (int k = 0; k <= d; k++) {
+        if (op == 0)
+            ex[k] = (k == 0 || k == d) ? 1 : rx[k] + ry[k];
+        else if (op == 1)
+            ex[k] = rx[k] * ry[k];
+        else
+            ex[k] = (k == 0 || k == d) ? 1 : 2 * rx[k];
+        if (ex[k] < z->rcap[k]) ex[k] = z->rcap[k];
+    }
+    return ptt_tt_reserve(z, ex);
+}
+
 static int check_same_modes(const ptt_tt* x, const ptt_tt* y) {
     if (!x || !y || x->d != y->d) return ptt_set_error(PTT_ERR_ARG, "mode count mismatch");
     for (int k = 0; k < x->d; k++)
@@ -126,7 +152,7 @@ extern "C" int ptt_axpby(double a, const ptt_tt* x, double b, const ptt_tt* y, p
     int need[PTT_MAX_DIM + 1];
     need[0] = need[d] = 1;
     for (int k = 1; k < d; k++) need[k] = x->rcap[k] + y->rcap[k];
-    if ((rc = ptt_tt_reserve(z, need))) return rc;
+    if ((rc = fit_output(z, need, x, y, 0))) return rc;
     ptt_ctx* c = z->ctx;
     int* newr = ranks_scratch(c, d);
     if (!newr) return ptt_set_error(PTT_ERR_ARG, "d too large");
@@ -177,7 +203,7 @@ extern "C" int ptt_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z) {
     const int d = x->d;
     int need[PTT_MAX_DIM + 1];
     for (int k = 0; k <= d; k++) need[k] = x->rcap[k] * y->rcap[k];
-    if ((rc = ptt_tt_reserve(z, need))) return rc;
+    if ((rc = fit_output(z, need, x, y, 1))) return rc;
     ptt_ctx* c = z->ctx;
     int* newr = ranks_scratch(c, d);
     if (!newr) return ptt_set_error(PTT_ERR_ARG, "d too large");
@@ -285,4 +311,92 @@ extern "C" int ptt_stencil(ptt_tt* x, int mode, const double* sten, int slen) {
     k_finalize<<<1, 32, 0, c->stream>>>(x->dd, NULL, mode, mode + 1, 0);
     PTT_LAUNCHED(c);
     return PTT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Y = sum_i S_i X + shift * X, S_i = the periodic stencil on mode i.
+// Exact rank-2r TT (the formal sum of the d single-mode stencil applications,
+// attac_apply_periodic_stencil paratt.c:584-661 summed with attacFormalSum,
+// represents the same tensor at rank d*r).  Core k in 2x2 blocks indexed by
+// (applied-before-k, applied-up-to-k): [[x_k, S x_k], [0, x_k]]; the first
+// core keeps block row 0 with the shift added to S x_0, the last core keeps
+// block column 1.  For d == 1: (S + shift) x_0.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double sten_at(const double* xc, int r, int n, int i, int j, int l, const Stencil& st) {
+    const int h = (st.len - 1) / 2;
+    double acc = 0.0;
+    for (int t = 0; t < st.len; t++) {
+        int s = j + t - h;
+        s = s < 0 ? s + n : (s >= n ? s - n : s);
+        acc += st.s[t] * xc[i + (long long)r * (s + (long long)n * l)];
+    }
+    return acc;
+}
+
+__global__ void k_opsum(const DevDesc* X, DevDesc* Y, Stencil st, double shift, int* newr, int* status) {
+    const int k = blockIdx.y;
+    const int d = X->d;
+    const int r = X->r[k], r1 = X->r[k + 1], n = X->n[k];
+    const int ry = (d == 1 || k == 0) ? 1 : 2 * r;
+    const int ry1 = (d == 1 || k == d - 1) ? 1 : 2 * r1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        newr[k] = ry;
+        if (k == d - 1) newr[d] = 1;
+    }
+    const long long cnt = (long long)ry * n * ry1;
+    if (ry > Y->rcap[k] || ry1 > Y->rcap[k + 1] || cnt > Y->cap[k]) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) PTT_STATUS_SET(status, PTT_ERR_CAPACITY);
+        return;
+    }
+    const double* xc = X->core[k];
+    double* yc = Y->alt[k];
+    const long long ryn = (long long)ry * n;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int l = (int)(e / ryn);
+        const long long rem = e - l * ryn;
+        const int j = (int)(rem / ry);
+        const int i = (int)(rem - (long long)j * ry);
+        double v;
+        if (d == 1) {
+            v = sten_at(xc, 1, n, 0, j, 0, st) + shift * xc[j];
+        } else if (k == 0) {
+            v = (l < r1) ? xc[j + (long long)n * l]
+                         : sten_at(xc, 1, n, 0, j, l - r1, st) + shift * xc[j + (long long)n * (l - r1)];
+        } else if (k == d - 1) {
+            v = (i < r) ? sten_at(xc, r, n, i, j, 0, st) : xc[(i - r) + (long long)r * j];
+        } else {
+            const bool a = i >= r, b = l >= r1;
+            if (!a && !b)
+                v = xc[i + (long long)r * (j + (long long)n * l)];
+            else if (!a && b)
+                v = sten_at(xc, r, n, i, j, l - r1, st);
+            else if (a && b)
+                v = xc[(i - r) + (long long)r * (j + (long long)n * (l - r1))];
+            else
+                v = 0.0;
+        }
+        yc[e] = v;
+    }
+}
+
+extern "C" int ptt_op_sum(const ptt_tt* x, const double* sten, int slen, double shift, ptt_tt* y) {
+    int rc = check_same_modes(x, y);
+    if (rc) return rc;
+    Stencil st;
+    if ((rc = ptt_make_stencil(sten, slen, &st))) return rc;
+    const int d = x->d;
+    for (int k = 0; k < d; k++)
+        if ((st.len - 1) / 2 >= x->n[k] && st.len > 1)
+            return ptt_set_error(PTT_ERR_ARG, "stencil half-width exceeds mode %d size", k);
+    int need[PTT_MAX_DIM + 1];
+    for (int k = 0; k <= d; k++) need[k] = (k == 0 || k == d) ? 1 : 2 * x->rcap[k];
+    if ((rc = fit_output(y, need, x, x, 2))) return rc;
+    ptt_ctx* c = y->ctx;
+    int* newr = ranks_scratch(c, d);
+    long long mx = 0;
+    for (int k = 0; k < d; k++) mx = y->cap[k] > mx ? y->cap[k] : mx;
+    k_opsum<<<dim3(elem_blocks(mx), d), 256, 0, c->stream>>>(x->dd, y->dd, st, shift, newr, c->d_status);
+    PTT_LAUNCHED(c);
+    return finalize(y, newr, 0, d, 1);
 }

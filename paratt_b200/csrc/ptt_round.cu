@@ -36,273 +36,7 @@ __device__ __forceinline__ double gsum8(double v, unsigned mask) {
     return v;
 }
 
-// ---------------------------------------------------------------------------
-// Householder kernels on shared-memory tiles (row stride S = CT + 1).
-// Thread tid: column slot cs = tid/8 (columns cs + 32u), row part tid%8
-// (rows part + 8v).  One block barrier per reflector.
-// ---------------------------------------------------------------------------
-template <int CT>
-__device__ void geqrt_smem(double* Rb, double* tau_s, int c, int tid) {
-    constexpr int S = CT + 1;
-    constexpr int NU = (CT + 31) / 32;
-    constexpr int NV = CT / 8;
-    const int cs = tid >> 3, part = tid & 7;
-    const unsigned gm = group_mask8(tid);
-    for (int j = 0; j < c; j++) {
-        if ((j & 31) == cs) {
-            const double alpha = Rb[j * S + j];
-            double s2 = 0.0;
-#pragma unroll
-            for (int v = 0; v < NV; v++) {
-                const int t = part + 8 * v;
-                if (t > j) {
-                    const double x = Rb[t * S + j];
-                    s2 += x * x;
-                }
-            }
-            s2 = gsum8(s2, gm);
-            double tau = 0.0, beta = alpha;
-            if (s2 > 0.0) {
-                beta = -copysign(sqrt(alpha * alpha + s2), alpha);
-                tau = (beta - alpha) / beta;
-                const double sc = 1.0 / (alpha - beta);
-#pragma unroll
-                for (int v = 0; v < NV; v++) {
-                    const int t = part + 8 * v;
-                    if (t > j) Rb[t * S + j] *= sc;
-                }
-            }
-            if (part == (j & 7)) Rb[j * S + j] = beta;
-            if (part == 0) tau_s[j] = tau;
-        }
-        __syncthreads();
-        const double tau = tau_s[j];
-        if (tau != 0.0) {
-#pragma unroll
-            for (int u = 0; u < NU; u++) {
-                const int l = cs + 32 * u;
-                const bool act = (l > j) && (l < c);
-                double pr = 0.0;
-                if (act) {
-#pragma unroll
-                    for (int v = 0; v < NV; v++) {
-                        const int t = part + 8 * v;
-                        if (t >= j) pr += (t == j ? 1.0 : Rb[t * S + j]) * Rb[t * S + l];
-                    }
-                }
-                pr = gsum8(pr, 0xffffffffu);
-                if (act) {
-                    const double tw = tau * pr;
-#pragma unroll
-                    for (int v = 0; v < NV; v++) {
-                        const int t = part + 8 * v;
-                        if (t >= j) Rb[t * S + l] -= tw * (t == j ? 1.0 : Rb[t * S + j]);
-                    }
-                }
-            }
-        }
-    }
-}
-
-// Eliminate an H-row chunk Ch into the upper triangle Rb (TSQRT): reflector j
-// has pivot Rb[j][j] and vector Ch[:, j]; on exit Ch holds the vectors.
-template <int CT>
-__device__ void tsqrt_smem(double* Rb, double* Ch, double* tau_s, int c, int tid) {
-    constexpr int S = CT + 1;
-    constexpr int NU = (CT + 31) / 32;
-    constexpr int NV = H / 8;
-    const int cs = tid >> 3, part = tid & 7;
-    const unsigned gm = group_mask8(tid);
-    for (int j = 0; j < c; j++) {
-        if ((j & 31) == cs) {
-            const double alpha = Rb[j * S + j];
-            double s2 = 0.0;
-#pragma unroll
-            for (int v = 0; v < NV; v++) {
-                const double x = Ch[(part + 8 * v) * S + j];
-                s2 += x * x;
-            }
-            s2 = gsum8(s2, gm);
-            double tau = 0.0, beta = alpha;
-            if (s2 > 0.0) {
-                beta = -copysign(sqrt(alpha * alpha + s2), alpha);
-                tau = (beta - alpha) / beta;
-                const double sc = 1.0 / (alpha - beta);
-#pragma unroll
-                for (int v = 0; v < NV; v++) Ch[(part + 8 * v) * S + j] *= sc;
-            }
-            if (part == 0) {
-                Rb[j * S + j] = beta;
-                tau_s[j] = tau;
-            }
-        }
-        __syncthreads();
-        const double tau = tau_s[j];
-        if (tau != 0.0) {
-#pragma unroll
-            for (int u = 0; u < NU; u++) {
-                const int l = cs + 32 * u;
-                const bool act = (l > j) && (l < c);
-                double pr = 0.0, rjl = 0.0;
-                if (act) {
-                    rjl = Rb[j * S + l];
-#pragma unroll
-                    for (int v = 0; v < NV; v++) {
-                        const int t = part + 8 * v;
-                        pr += Ch[t * S + j] * Ch[t * S + l];
-                    }
-                }
-                pr = gsum8(pr, 0xffffffffu);
-                if (act) {
-                    const double tw = tau * (rjl + pr);
-                    if (part == 0) Rb[j * S + l] = rjl - tw;
-#pragma unroll
-                    for (int v = 0; v < NV; v++) {
-                        const int t = part + 8 * v;
-                        Ch[t * S + l] -= tw * Ch[t * S + j];
-                    }
-                }
-            }
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// factor kernel: leaves + last-arriver tree
-// ---------------------------------------------------------------------------
-template <int CT>
-__global__ void __launch_bounds__(NT) k_tsqr_factor(const DevDesc* D, int kcore, int mode, Plan pl, double* ws,
-                                                    int* status) {
-    extern __shared__ double sm[];
-    constexpr int S = CT + 1;
-    double* Rb = sm;
-    double* Ch = Rb + CT * S;
-    double* tau_s = Ch + H * S;
-    __shared__ int s_flag;
-    const int tid = threadIdx.x;
-    const View A = make_view(D, kcore, mode, false);
-    const int m = A.m, c = A.c;
-    const int P = pl.P, p = blockIdx.x;
-    double* Rn = ws + pl.o_Rn;
-    const bool bad = (c > CT || c < 1 || m < 1);
-    if (p == 0 && tid == 0) {
-        pl.info->m = m;
-        pl.info->c = c;
-        pl.info->q = m < c ? m : c;
-        pl.info->rank = 0;
-        pl.info->status = bad ? 1 : 0;
-        if (bad) PTT_STATUS_SET(status, PTT_ERR_CAPACITY);
-    }
-    if (bad) return;
-    int r0, r1;
-    leaf_range(m, pl.L, P, p, &r0, &r1);
-    const int rows = r1 - r0;
-    const int slot = P - 1 + p;
-    double* tau_leaf = ws + pl.o_tau_leaf + (long long)p * pl.KL * CT;
-    if (rows > 0) {
-        const int rb = rows < c ? rows : c;
-        for (int e = tid; e < CT * CT; e += NT) {
-            const int t = e / CT, l = e - (e / CT) * CT;
-            Rb[t * S + l] = (t < rb && l < c) ? A.p[(long long)(r0 + t) * A.rs + (long long)l * A.cs] : 0.0;
-        }
-        __syncthreads();
-        geqrt_smem<CT>(Rb, tau_s, c, tid);
-        __syncthreads();
-        for (int e = tid; e < CT * CT; e += NT) {
-            const int t = e / CT, l = e - (e / CT) * CT;
-            if (t > l) {
-                if (t < rb && l < c) A.p[(long long)(r0 + t) * A.rs + (long long)l * A.cs] = Rb[t * S + l];
-                Rb[t * S + l] = 0.0;
-            }
-        }
-        for (int j = tid; j < CT; j += NT) tau_leaf[j] = j < c ? tau_s[j] : 0.0;
-        __syncthreads();
-        int s = 0;
-        for (int t0 = r0 + rb; t0 < r1; t0 += H, s++) {
-            const int h = (r1 - t0) < H ? (r1 - t0) : H;
-            for (int e = tid; e < H * CT; e += NT) {
-                const int t = e / CT, l = e - (e / CT) * CT;
-                Ch[t * S + l] = (t < h && l < c) ? A.p[(long long)(t0 + t) * A.rs + (long long)l * A.cs] : 0.0;
-            }
-            __syncthreads();
-            tsqrt_smem<CT>(Rb, Ch, tau_s, c, tid);
-            __syncthreads();
-            for (int e = tid; e < H * CT; e += NT) {
-                const int t = e / CT, l = e - (e / CT) * CT;
-                if (t < h && l < c) A.p[(long long)(t0 + t) * A.rs + (long long)l * A.cs] = Ch[t * S + l];
-            }
-            for (int j = tid; j < CT; j += NT) tau_leaf[(long long)(1 + s) * CT + j] = j < c ? tau_s[j] : 0.0;
-            __syncthreads();
-        }
-        double* Ro = Rn + (long long)slot * CT * CT;
-        for (int e = tid; e < CT * CT; e += NT) {
-            const int t = e / CT, l = e - (e / CT) * CT;
-            Ro[e] = (t <= l) ? Rb[t * S + l] : 0.0;
-        }
-    }
-    if (tid == 0) pl.qn[slot] = rows > 0 ? (rows < c ? rows : c) : 0;
-
-    int node = slot;
-    while (node > 0) {
-        const int par = (node - 1) >> 1;
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) s_flag = atomicAdd(&pl.cnt[par], 1);
-        __syncthreads();
-        if (s_flag == 0) return;
-        __threadfence();
-        if (tid == 0) pl.cnt[par] = 0;
-        const int cl = 2 * par + 1, cr = 2 * par + 2;
-        const int qL = ldcg(&pl.qn[cl]), qR = ldcg(&pl.qn[cr]);
-        double* Rp = Rn + (long long)par * CT * CT;
-        if (qL > 0 && qR > 0) {
-            if ((qL != c || qR != c) && tid == 0) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
-            const double* RL = Rn + (long long)cl * CT * CT;
-            double* RR = Rn + (long long)cr * CT * CT;
-            for (int e = tid; e < CT * CT; e += NT) {
-                const int t = e / CT, l = e - (e / CT) * CT;
-                Rb[t * S + l] = ldcg(RL + e);
-            }
-            for (int half = 0; half < pl.NH; half++) {
-                const int h0 = half * H;
-                __syncthreads();
-                for (int e = tid; e < H * CT; e += NT) {
-                    const int t = e / CT, l = e - (e / CT) * CT;
-                    Ch[t * S + l] = (h0 + t < c) ? ldcg(RR + (long long)(h0 + t) * CT + l) : 0.0;
-                }
-                __syncthreads();
-                if (h0 < c) tsqrt_smem<CT>(Rb, Ch, tau_s, c, tid);
-                __syncthreads();
-                for (int e = tid; e < H * CT; e += NT) {
-                    const int t = e / CT, l = e - (e / CT) * CT;
-                    if (h0 + t < CT) RR[(long long)(h0 + t) * CT + l] = Ch[t * S + l];
-                }
-                double* tn = ws + pl.o_tau_node + ((long long)par * pl.NH + half) * CT;
-                for (int j = tid; j < CT; j += NT) tn[j] = (h0 < c && j < c) ? tau_s[j] : 0.0;
-            }
-            __syncthreads();
-            for (int e = tid; e < CT * CT; e += NT) {
-                const int t = e / CT, l = e - (e / CT) * CT;
-                Rp[e] = (t <= l) ? Rb[t * S + l] : 0.0;
-            }
-            if (tid == 0) {
-                pl.qn[par] = c;
-                pl.pass[par] = 0;
-            }
-        } else {
-            const int which = qL > 0 ? 1 : (qR > 0 ? 2 : 3);
-            if (which != 3) {
-                const double* src = Rn + (long long)(which == 1 ? cl : cr) * CT * CT;
-                for (int e = tid; e < CT * CT; e += NT) Rp[e] = ldcg(src + e);
-            }
-            if (tid == 0) {
-                pl.qn[par] = which == 1 ? qL : (which == 2 ? qR : 0);
-                pl.pass[par] = which;
-            }
-        }
-        node = par;
-    }
-}
+#include "ptt_factor.cuh"
 
 // ---------------------------------------------------------------------------
 // Q application: out = Q * B, B = Bn[root] (q x k), k read from device.
@@ -505,83 +239,115 @@ __device__ __forceinline__ int circle_col(int pos, int round, int qq) {
 
 constexpr int SVD_NT = 512;
 
+// One-sided Jacobi on the columns of L (c rows, q columns).  Each column pair
+// is handled by 8 lanes (rows p + 8v), 64 pairs per pass, so one circle-order
+// round is a single pass for q <= 128.  Column norms are tracked through the
+// rotations (a_p' = a_p - t a_pq ...) and recomputed at the start of a sweep.
 template <int CT>
-__global__ void __launch_bounds__(SVD_NT) k_svd_jacobi(Plan pl, double* ws, double delta, int maxr, int* status) {
+__global__ void __launch_bounds__(SVD_NT) k_svd_jacobi(Plan pl, double* ws, double delta, int maxr, int bond,
+                                                       int* status) {
     extern __shared__ double sm[];
     constexpr int S = CT + 1;
+    constexpr int NG = CT / 8;
     double* Lc = sm;                   // (CT+1) columns x S
-    __shared__ double s_sig[CT + 1];
-    __shared__ int s_ord[CT + 1];
+    __shared__ double s_nrm[CT + 2];
+    __shared__ double s_sig[CT + 2];
+    __shared__ int s_ord[CT + 2];
     __shared__ int s_rot;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int NW = SVD_NT / 32;
+    const int tid = threadIdx.x;
+    const int grp = tid >> 3, p = tid & 7;  // 64 pair slots x 8 lanes
+    const unsigned gm = group_mask8(tid);
     Info* info = pl.info;
     if (info->status) return;
     const int c = info->c, q = info->q;
     const int qq = q + (q & 1);
-    const double* R = ws + pl.o_Rn;  // root, row-major CT x CT
+    const double* R = ws + pl.o_Rn;  // root factor, row-major CT x CT; L = R^T
     for (int e = tid; e < qq * S; e += SVD_NT) {
         const int j = e / S, t = e - (e / S) * S;
         Lc[e] = (j < q && t < c) ? R[(long long)j * CT + t] : 0.0;
     }
     __syncthreads();
     double2* rot = (double2*)(ws + pl.o_rot);
-    const double tol = sqrt((double)c) * 1.1102230246251565e-16;
+    const int npair = (CT + 2) / 2;
+    const double tol = (double)(c < 16 ? 16 : c) * 2.220446049250313e-16;
     int sweeps = 0;
-    if (qq >= 2) {
-        for (int sw = 0; sw < MAXSW; sw++) {
-            if (tid == 0) s_rot = 0;
-            __syncthreads();
-            int myrot = 0;
-            for (int rd = 0; rd < qq - 1; rd++) {
-                for (int i = warp; i < qq / 2; i += NW) {
-                    const int pc = circle_col(i, rd, qq), qc = circle_col(qq - 1 - i, rd, qq);
-                    double* ap = Lc + pc * S;
-                    double* aq = Lc + qc * S;
-                    double al = 0.0, be = 0.0, ga = 0.0;
-                    for (int t = lane; t < c; t += 32) {
-                        const double x = ap[t], y = aq[t];
-                        al += x * x;
-                        be += y * y;
-                        ga += x * y;
-                    }
-                    al = warp_sum(al);
-                    be = warp_sum(be);
-                    ga = warp_sum(ga);
-                    double cs = 1.0, sn = 0.0;
-                    if (ga != 0.0 && fabs(ga) > tol * sqrt(al) * sqrt(be)) {
-                        const double zeta = (be - al) / (2.0 * ga);
-                        double t;
-                        if (fabs(zeta) > 1e150)
-                            t = 0.5 / zeta;
-                        else
-                            t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                        cs = 1.0 / sqrt(1.0 + t * t);
-                        sn = cs * t;
-                        for (int tt = lane; tt < c; tt += 32) {
-                            const double x = ap[tt], y = aq[tt];
-                            ap[tt] = cs * x - sn * y;
-                            aq[tt] = sn * x + cs * y;
-                        }
-                        myrot = 1;
-                    }
-                    if (lane == 0) rot[((long long)sw * (CT + 1) + rd) * ((CT + 2) / 2) + i] = make_double2(cs, sn);
-                }
-                __syncthreads();
+    bool conv = (qq < 2);
+    for (int sw = 0; sw < MAXSW && !conv; sw++) {
+        // exact column norms at the start of every sweep
+        for (int j = tid >> 3; j < qq; j += SVD_NT / 8) {
+            double s2 = 0.0;
+#pragma unroll
+            for (int v = 0; v < NG; v++) {
+                const double x = Lc[j * S + p + 8 * v];
+                s2 += x * x;
             }
-            if (myrot && lane == 0) atomicOr(&s_rot, 1);
-            __syncthreads();
-            sweeps = sw + 1;
-            if (s_rot == 0) break;
+            s2 = gsum8(s2, gm);
+            if (p == 0) s_nrm[j] = s2;
         }
-        if (s_rot != 0 && tid == 0) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
+        if (tid == 0) s_rot = 0;
+        __syncthreads();
+        int myrot = 0;
+        for (int rd = 0; rd < qq - 1; rd++) {
+            for (int i = grp; i < qq / 2; i += SVD_NT / 8) {
+                const int pc = circle_col(i, rd, qq), qc = circle_col(qq - 1 - i, rd, qq);
+                double* ap = Lc + pc * S;
+                double* aq = Lc + qc * S;
+                double xa[NG], xb[NG];
+                double g0 = 0.0, g1 = 0.0;
+#pragma unroll
+                for (int v = 0; v < NG; v++) {
+                    xa[v] = ap[p + 8 * v];
+                    xb[v] = aq[p + 8 * v];
+                }
+#pragma unroll
+                for (int v = 0; v < NG; v += 2) {
+                    g0 = fma(xa[v], xb[v], g0);
+                    g1 = fma(xa[v + 1], xb[v + 1], g1);
+                }
+                const double ga = gsum8(g0 + g1, gm);
+                const double al = s_nrm[pc], be = s_nrm[qc];
+                double cs = 1.0, sn = 0.0;
+                if (ga != 0.0 && fabs(ga) > tol * sqrt(al * be)) {
+                    // t = tan(theta) = sign(z)/(|z| + sqrt(1+z^2)), z = (be-al)/(2 ga),
+                    // written as g2/(dd + sign(dd) sqrt(dd^2 + g2^2)): one sqrt, one reciprocal
+                    const double dd = be - al, g2 = 2.0 * ga;
+                    const double t = g2 * __drcp_rn(dd + copysign(sqrt(fma(dd, dd, g2 * g2)), dd));
+                    cs = rsqrt(fma(t, t, 1.0));
+                    sn = cs * t;
+#pragma unroll
+                    for (int v = 0; v < NG; v++) {
+                        ap[p + 8 * v] = cs * xa[v] - sn * xb[v];
+                        aq[p + 8 * v] = sn * xa[v] + cs * xb[v];
+                    }
+                    if (p == 0) {
+                        s_nrm[pc] = al - t * ga;
+                        s_nrm[qc] = be + t * ga;
+                    }
+                    myrot = 1;
+                }
+                if (p == 0) rot[((long long)sw * (CT + 1) + rd) * npair + i] = make_double2(cs, sn);
+            }
+            __syncthreads();
+        }
+        if (myrot) atomicOr(&s_rot, 1);
+        __syncthreads();
+        if (s_rot == 0) {
+            conv = true;
+        } else {
+            sweeps = sw + 1;
+        }
     }
-    // singular values and descending order
-    for (int j = warp; j < qq; j += NW) {
+    if (!conv && tid == 0) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
+    // singular values (column norms) and descending order
+    for (int j = tid >> 3; j < qq; j += SVD_NT / 8) {
         double s2 = 0.0;
-        for (int t = lane; t < c; t += 32) s2 += Lc[j * S + t] * Lc[j * S + t];
-        s2 = warp_sum(s2);
-        if (lane == 0) s_sig[j] = (j < q) ? sqrt(s2) : -1.0;
+#pragma unroll
+        for (int v = 0; v < NG; v++) {
+            const double x = Lc[j * S + p + 8 * v];
+            s2 += x * x;
+        }
+        s2 = gsum8(s2, gm);
+        if (p == 0) s_sig[j] = (j < q) ? sqrt(s2) : -1.0;
     }
     __syncthreads();
     for (int j = tid; j < qq; j += SVD_NT) {
@@ -622,6 +388,18 @@ __global__ void __launch_bounds__(SVD_NT) k_svd_jacobi(Plan pl, double* ws, doub
         double tail = 0.0;
         for (int j = rank; j < q; j++) tail += s_sig[s_ord[j]] * s_sig[s_ord[j]];
         info->tail = tail;
+        if (pl.stats) {
+            double* st = pl.stats + (long long)bond * PTT_STAT_LEN;
+            st[0] = rank;
+            st[1] = nsv;
+            st[2] = sweeps;
+            st[3] = q;
+            st[4] = c;
+            st[5] = tail;
+            st[6] = delta;
+            st[7] = 0.0;
+            for (int j = 0; j < PTT_STAT_NSIG; j++) st[8 + j] = j < q ? s_sig[s_ord[j]] : 0.0;
+        }
     }
     for (int j = tid; j < CT; j += SVD_NT) {
         sig_out[j] = j < q ? s_sig[s_ord[j]] : 0.0;
@@ -636,13 +414,16 @@ __global__ void __launch_bounds__(SVD_NT) k_svd_jacobi(Plan pl, double* ws, doub
     }
 }
 
-// Rebuild rows of V from the recorded rotations; write V_r into Bn[root].
+// Rebuild rows of V (q x q, V = product of the recorded rotations) and write
+// V_r = V[:, order[0:rank]] into Bn[root].  One warp per row; each sweep's
+// rotation table is staged in shared memory once per block.
 __global__ void __launch_bounds__(256) k_svd_replay(Plan pl, double* ws) {
     extern __shared__ double sm[];
     const int CT = pl.CT, KC = pl.KC;
     const int SR = CT + 2;
-    double* vrow = sm + (threadIdx.x >> 5) * SR;  // 8 rows
-    double2* rbuf = (double2*)(sm + 8 * SR);       // (CT+2)/2 pairs
+    const int npair = (CT + 2) / 2;
+    double* vrow = sm + (threadIdx.x >> 5) * SR;   // 8 rows
+    double2* tab = (double2*)(sm + 8 * SR);         // (CT+1) rounds x npair
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int row = blockIdx.x * 8 + warp;
     const Info* info = pl.info;
@@ -650,16 +431,16 @@ __global__ void __launch_bounds__(256) k_svd_replay(Plan pl, double* ws) {
     const int q = info->q, qq = q + (q & 1), sweeps = info->sweeps, rank = info->rank;
     for (int j = lane; j < SR; j += 32) vrow[j] = (j == row) ? 1.0 : 0.0;
     const double2* rot = (const double2*)(ws + pl.o_rot);
-    const int npair = (CT + 2) / 2;
     for (int sw = 0; sw < sweeps; sw++) {
-        for (int rd = 0; rd < qq - 1; rd++) {
-            __syncthreads();
-            for (int i = threadIdx.x; i < qq / 2; i += blockDim.x)
-                rbuf[i] = rot[((long long)sw * (CT + 1) + rd) * npair + i];
-            __syncthreads();
-            if (row < q) {
+        __syncthreads();
+        const long long base = (long long)sw * (CT + 1) * npair;
+        const int cnt = (qq - 1) * npair;
+        for (int e = threadIdx.x; e < cnt; e += blockDim.x) tab[e] = rot[base + e];
+        __syncthreads();
+        if (row < q) {
+            for (int rd = 0; rd < qq - 1; rd++) {
                 for (int i = lane; i < qq / 2; i += 32) {
-                    const double2 r = rbuf[i];
+                    const double2 r = tab[rd * npair + i];
                     if (r.y != 0.0) {
                         const int pc = circle_col(i, rd, qq), qc = circle_col(qq - 1 - i, rd, qq);
                         const double x = vrow[pc], y = vrow[qc];
@@ -667,8 +448,8 @@ __global__ void __launch_bounds__(256) k_svd_replay(Plan pl, double* ws) {
                         vrow[qc] = r.y * x + r.x * y;
                     }
                 }
+                __syncwarp();
             }
-            __syncwarp();
         }
     }
     __syncthreads();
@@ -772,9 +553,11 @@ __global__ void k_bond_finalize(DevDesc* D, int kq, int ka, int kb, const int* v
         double* t = D->core[ka];
         D->core[ka] = D->alt[ka];
         D->alt[ka] = t;
-        t = D->core[kb];
-        D->core[kb] = D->alt[kb];
-        D->alt[kb] = t;
+        if (kb >= 0) {
+            t = D->core[kb];
+            D->core[kb] = D->alt[kb];
+            D->alt[kb] = t;
+        }
     }
 }
 
@@ -832,7 +615,7 @@ static long long carve(Plan* pl, int PMAX, int LMAXKL) {
 
 template <int CT>
 static size_t factor_smem() {
-    return sizeof(double) * ((size_t)CT * (CT + 1) + (size_t)H * (CT + 1) + CT);
+    return sizeof(double) * ((size_t)CT * CT + 2 * (size_t)FCfg<CT>::VB + CT);
 }
 template <int CT>
 static size_t apply_smem() {
@@ -842,6 +625,11 @@ static size_t apply_smem() {
 template <int CT>
 static size_t svd_smem() {
     return sizeof(double) * (size_t)(CT + 2) * (CT + 1);
+}
+// 8 V rows + one sweep's rotation table ((CT+1) rounds x (CT+2)/2 pairs)
+template <int CT>
+static size_t replay_smem() {
+    return sizeof(double) * (8 * (size_t)(CT + 2) + 2 * (size_t)(CT + 1) * ((CT + 2) / 2));
 }
 
 template <int CT>
@@ -856,6 +644,8 @@ static int set_attrs() {
                                   (int)apply_smem<CT>()));
     PTT_CUDA(cudaFuncSetAttribute(k_svd_jacobi<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)svd_smem<CT>()));
+    PTT_CUDA(cudaFuncSetAttribute(k_svd_replay, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)replay_smem<128>()));
     done = true;
     return PTT_OK;
 }
@@ -863,7 +653,9 @@ static int set_attrs() {
 // Factor the unfolding (mode) of core k; R lands at the root slot.
 template <int CT>
 static int launch_factor(ptt_ctx* c, ptt_tt* x, int k, int mode, Plan& pl, double* ws) {
+    ptt_time_begin(c, PTT_TIME_TSQR);
     k_tsqr_factor<CT><<<pl.P, NT, factor_smem<CT>(), c->stream>>>(x->dd, k, mode, pl, ws, c->d_status);
+    ptt_time_end(c, PTT_TIME_TSQR);
     PTT_LAUNCHED(c);
     return PTT_OK;
 }
@@ -884,8 +676,10 @@ static int launch_apply(ptt_ctx* c, ptt_tt* x, int k, int mode, Plan& pl, double
     return PTT_OK;
 }
 
+// phases: 1 = left-to-right orthogonalisation, 2 = right-to-left truncation,
+// 4 = QR of the single core `only` (left unfolding; core <- Q, r_{only+1} <- q).
 template <int CT>
-static int round_impl(ptt_tt* x, double delta, const int* maxr) {
+static int round_impl(ptt_tt* x, double delta, const int* maxr, int phases, int only) {
     ptt_ctx* c = x->ctx;
     const int d = x->d;
     int rc = set_attrs<CT>();
@@ -925,11 +719,24 @@ static int round_impl(ptt_tt* x, double delta, const int* maxr) {
         pl.qn = ints;
         pl.pass = ints + 2 * PMAX;
         pl.info = info;
+        pl.stats = c->d_stats;
+        pl.work = (c->tkind == PTT_TIME_TSQR) ? c->d_work + PTT_TIME_TSQR : nullptr;
         return pl;
     };
 
+    if (phases & 4) {
+        const int i = only;
+        Plan pl = mkplan((long long)x->rcap[i] * x->n[i]);
+        if ((rc = launch_factor<CT>(c, x, i, LEFT, pl, ws))) return rc;
+        k_set_identity<<<32, 256, 0, c->stream>>>(pl, ws);
+        PTT_LAUNCHED(c);
+        if ((rc = launch_apply<CT>(c, x, i, LEFT, pl, ws, &info->q, CT))) return rc;
+        k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i, -1, &info->q, info);
+        PTT_LAUNCHED(c);
+        return PTT_OK;
+    }
     // left-to-right orthogonalisation
-    for (int i = 0; i < d - 1; i++) {
+    for (int i = 0; i < d - 1 && (phases & 1); i++) {
         Plan pl = mkplan((long long)x->rcap[i] * x->n[i]);
         if ((rc = launch_factor<CT>(c, x, i, LEFT, pl, ws))) return rc;
         {
@@ -946,13 +753,15 @@ static int round_impl(ptt_tt* x, double delta, const int* maxr) {
         PTT_LAUNCHED(c);
     }
     // right-to-left truncation
-    for (int i = d - 1; i >= 1; i--) {
+    for (int i = d - 1; i >= 1 && (phases & 2); i--) {
         Plan pl = mkplan((long long)x->n[i] * x->rcap[i + 1]);
         if ((rc = launch_factor<CT>(c, x, i, RIGHT_T, pl, ws))) return rc;
         const int mr = maxr ? maxr[i] : x->rcap[i];
-        k_svd_jacobi<CT><<<1, SVD_NT, svd_smem<CT>(), c->stream>>>(pl, ws, delta, mr, c->d_status);
+        ptt_time_begin(c, PTT_TIME_SVD);
+        k_svd_jacobi<CT><<<1, SVD_NT, svd_smem<CT>(), c->stream>>>(pl, ws, delta, mr, i, c->d_status);
+        ptt_time_end(c, PTT_TIME_SVD);
         PTT_LAUNCHED(c);
-        k_svd_replay<<<(CT + 7) / 8, 256, sizeof(double) * (8 * (CT + 2) + (CT + 2)), c->stream>>>(pl, ws);
+        k_svd_replay<<<(CT + 7) / 8, 256, replay_smem<CT>(), c->stream>>>(pl, ws);
         PTT_LAUNCHED(c);
         if ((rc = launch_apply<CT>(c, x, i, RIGHT_T, pl, ws, &info->rank, CT))) return rc;
         {
@@ -979,7 +788,14 @@ double ptt_round_threshold(const ptt_tt* x, double tol) {
     return tol / sqrt(d - 1.0) * exp(0.5 * lg);
 }
 
-extern "C" int ptt_round(ptt_tt* x, double tol, const int* maxrank) {
+extern "C" int ptt_round_stats(ptt_ctx* c, int d, double* out) {
+    if (!c || !out || d < 1 || d > PTT_MAX_DIM) return ptt_set_error(PTT_ERR_ARG, "ptt_round_stats: bad arguments");
+    PTT_CUDA(cudaStreamSynchronize(c->stream));
+    PTT_CUDA(cudaMemcpy(out, c->d_stats, sizeof(double) * PTT_STAT_LEN * (size_t)d, cudaMemcpyDeviceToHost));
+    return PTT_OK;
+}
+
+int ptt_round_phases(ptt_tt* x, double tol, const int* maxrank, int phases, int only) {
     if (!x) return ptt_set_error(PTT_ERR_ARG, "ptt_round: null tt");
     if (x->d < 2) return PTT_OK;
     if (!(tol >= 0.0)) return ptt_set_error(PTT_ERR_ARG, "ptt_round: tol must be >= 0");
@@ -987,8 +803,12 @@ extern "C" int ptt_round(ptt_tt* x, double tol, const int* maxrank) {
     for (int k = 0; k <= x->d; k++) rmax = x->rcap[k] > rmax ? x->rcap[k] : rmax;
     const double delta = ptt_round_threshold(x, tol);
     cudaSetDevice(x->ctx->device);
-    if (rmax <= 32) return round_impl<32>(x, delta, maxrank);
-    if (rmax <= 64) return round_impl<64>(x, delta, maxrank);
-    if (rmax <= 128) return round_impl<128>(x, delta, maxrank);
+    if (rmax <= 32) return round_impl<32>(x, delta, maxrank, phases, only);
+    if (rmax <= 64) return round_impl<64>(x, delta, maxrank, phases, only);
+    if (rmax <= 128) return round_impl<128>(x, delta, maxrank, phases, only);
     return ptt_set_error(PTT_ERR_CAPACITY, "ptt_round: rank capacity %d > 128 not supported", rmax);
+}
+
+extern "C" int ptt_round(ptt_tt* x, double tol, const int* maxrank) {
+    return ptt_round_phases(x, tol, maxrank, 3, 0);
 }

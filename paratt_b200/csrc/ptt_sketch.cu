@@ -1,0 +1,314 @@
+// Randomised TT rounding of a Hadamard product without forming it.
+//
+// z ~= round(x (.) y), where the formal product (attacHadamard, attac.c:
+// 128-136) would have ranks r_x r_y: a Gaussian TT sketch G with ranks l_k
+// is contracted with the product right-to-left, W_k = sum_j (x_k[:,j,:] (x)
+// y_k[:,j,:]) W_{k+1} G_k[:,j,:]^T  (r_x r_y x l_k), then the product is
+// orthogonalised left-to-right against the sketch (Y = Z_k W_{k+1}, QR,
+// carry Q^T Z_k), which is the "randomize-then-orthogonalize" rounding of
+// Al Daas, Ballard, Cazeaux, Hallman, Miedlar, Pasha, Reid and Saibaba,
+// "Randomized algorithms for rounding in the tensor-train format", SISC 2023.
+// The result is left-orthogonal with ranks <= l_k and is finished by the
+// deterministic right-to-left SVD truncation of ptt_round (tol, maxrank).
+//
+// Every contraction is a batched strided FP64 GEMM over the Kronecker
+// structure, so no r_x r_y x n x r_x r_y core is ever stored.
+#include "ptt_common.cuh"
+
+#include <stdio.h>
+#include <string.h>
+
+namespace {
+
+struct GemmB {
+    const double* A;
+    long long ars, acs, ab1, ab2;
+    const double* B;
+    long long brs, bcs, bb1, bb2;
+    double* C;
+    long long crs, ccs, cb1, cb2;
+    int M, N, K, nb1, nb2;
+    double alpha, beta;
+};
+
+// C[b] = alpha * A[b] B[b] + beta * C[b]; batch b = b1 + nb1 * b2.
+template <int TM>
+__global__ void __launch_bounds__(256) k_gemm_b(GemmB g, int zoff) {
+    constexpr int BK = 16;
+    constexpr int RT = TM / 16;
+    __shared__ double sA[BK][TM + 1];
+    __shared__ double sB[BK][TM + 1];
+    const int bz = blockIdx.z + zoff;
+    const int b1 = bz % g.nb1, b2 = bz / g.nb1;
+    const double* A = g.A + b1 * g.ab1 + b2 * g.ab2;
+    const double* B = g.B + b1 * g.bb1 + b2 * g.bb2;
+    double* C = g.C + b1 * g.cb1 + b2 * g.cb2;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TM;
+    const bool a_colmajor = (g.ars == 1);
+    const bool b_rowfast = (g.bcs == 1);
+    double acc[RT][RT];
+#pragma unroll
+    for (int i = 0; i < RT; i++)
+#pragma unroll
+        for (int j = 0; j < RT; j++) acc[i][j] = 0.0;
+    for (int k0 = 0; k0 < g.K; k0 += BK) {
+        for (int e = tid; e < TM * BK; e += 256) {
+            int r, kk;
+            if (a_colmajor) {
+                r = e % TM;
+                kk = e / TM;
+            } else {
+                kk = e % BK;
+                r = e / BK;
+            }
+            const int gr = m0 + r, gk = k0 + kk;
+            sA[kk][r] = (gr < g.M && gk < g.K) ? A[(long long)gr * g.ars + (long long)gk * g.acs] : 0.0;
+        }
+        for (int e = tid; e < TM * BK; e += 256) {
+            int cn, kk;
+            if (b_rowfast) {
+                cn = e % TM;
+                kk = e / TM;
+            } else {
+                kk = e % BK;
+                cn = e / BK;
+            }
+            const int gk = k0 + kk, gc = n0 + cn;
+            sB[kk][cn] = (gk < g.K && gc < g.N) ? B[(long long)gk * g.brs + (long long)gc * g.bcs] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; kk++) {
+            double a[RT], b[RT];
+#pragma unroll
+            for (int i = 0; i < RT; i++) a[i] = sA[kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < RT; j++) b[j] = sB[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < RT; i++)
+#pragma unroll
+                for (int j = 0; j < RT; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < RT; i++) {
+        const int gr = m0 + ty + 16 * i;
+        if (gr >= g.M) continue;
+#pragma unroll
+        for (int j = 0; j < RT; j++) {
+            const int gc = n0 + tx + 16 * j;
+            if (gc >= g.N) continue;
+            double* cp = C + (long long)gr * g.crs + (long long)gc * g.ccs;
+            *cp = (g.beta != 0.0) ? fma(g.alpha, acc[i][j], g.beta * *cp) : g.alpha * acc[i][j];
+        }
+    }
+}
+
+int gemm(ptt_ctx* c, const GemmB& g) {
+    if (g.M <= 0 || g.N <= 0 || g.nb1 <= 0 || g.nb2 <= 0) return PTT_OK;
+    const long long nb = (long long)g.nb1 * g.nb2;
+    if (c->tkind == PTT_TIME_GEMM) c->hwork[PTT_TIME_GEMM] += 2.0 * g.M * (double)g.N * g.K * (double)nb;
+    const bool big = g.M >= 48 && g.N >= 48;
+    const int TM = big ? 64 : 32;
+    dim3 grid((g.M + TM - 1) / TM, (g.N + TM - 1) / TM, 1);
+    for (long long z0 = 0; z0 < nb; z0 += 65535) {
+        grid.z = (unsigned)((nb - z0) < 65535 ? (nb - z0) : 65535);
+        ptt_time_begin(c, PTT_TIME_GEMM);
+        if (big)
+            k_gemm_b<64><<<grid, 256, 0, c->stream>>>(g, (int)z0);
+        else
+            k_gemm_b<32><<<grid, 256, 0, c->stream>>>(g, (int)z0);
+        ptt_time_end(c, PTT_TIME_GEMM);
+        PTT_LAUNCHED(c);
+    }
+    return PTT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Gaussian sketch cores from a counter-based generator: splitmix64 (Vigna)
+// hashes (seed, core, index); Box-Muller turns two uniforms into a normal.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__global__ void k_gauss(double* G, long long cnt, unsigned long long seed, int core) {
+    const unsigned long long base = splitmix64(seed ^ (0xD1B54A32D192ED03ull * (unsigned long long)(core + 1)));
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt;
+         e += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long h1 = splitmix64(base + 2ull * (unsigned long long)e);
+        const unsigned long long h2 = splitmix64(base + 2ull * (unsigned long long)e + 1ull);
+        const double u1 = ((double)(h1 >> 11) + 0.5) * 1.1102230246251565e-16;  // (0,1)
+        const double u2 = (double)(h2 >> 11) * 1.1102230246251565e-16;          // [0,1)
+        G[e] = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+    }
+}
+
+__global__ void k_fill(double* p, long long cnt, double v) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt;
+         e += (long long)gridDim.x * blockDim.x)
+        p[e] = v;
+}
+
+static int blocks_for(long long cnt) {
+    long long b = (cnt + 255) / 256;
+    return (int)(b < 1 ? 1 : (b > 2048 ? 2048 : b));
+}
+
+}  // namespace
+
+extern "C" int ptt_round_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* ell, unsigned long long seed,
+                                  double tol, const int* maxrank) {
+    if (!x || !y || !z || x->d != y->d || x->d != z->d)
+        return ptt_set_error(PTT_ERR_ARG, "ptt_round_hadamard: shape mismatch");
+    if (z == x || z == y) return ptt_set_error(PTT_ERR_ARG, "ptt_round_hadamard: output aliases an input");
+    const int d = x->d;
+    for (int k = 0; k < d; k++)
+        if (x->n[k] != y->n[k] || x->n[k] != z->n[k])
+            return ptt_set_error(PTT_ERR_ARG, "ptt_round_hadamard: mode %d differs", k);
+    ptt_ctx* c = z->ctx;
+    int rc;
+    int rx[PTT_MAX_DIM + 1], ry[PTT_MAX_DIM + 1], L[PTT_MAX_DIM + 1];
+    long long R[PTT_MAX_DIM + 1];
+    if ((rc = ptt_tt_get_ranks((ptt_tt*)x, rx)) || (rc = ptt_tt_get_ranks((ptt_tt*)y, ry))) return rc;
+    const int* n = x->n;
+    for (int k = 0; k <= d; k++) R[k] = (long long)rx[k] * ry[k];
+    L[0] = L[d] = 1;
+    for (int k = 1; k < d; k++) {
+        long long l = ell ? ell[k] : 72;
+        if (l > R[k]) l = R[k];
+        if (l > 128) l = 128;
+        if (l < 1) l = 1;
+        L[k] = (int)l;
+    }
+    // z capacity: ranks <= L
+    {
+        int cap[PTT_MAX_DIM + 1];
+        for (int k = 0; k <= d; k++) cap[k] = L[k] > z->rcap[k] ? L[k] : z->rcap[k];
+        if ((rc = ptt_tt_reserve(z, cap))) return rc;
+    }
+    // workspace: G_1..G_{d-1}, W_1..W_d, then temporaries
+    long long oG[PTT_MAX_DIM + 1], oW[PTT_MAX_DIM + 1], off = 0;
+    for (int k = 1; k < d; k++) {
+        oG[k] = off;
+        off += (long long)L[k] * n[k] * L[k + 1];
+    }
+    for (int k = 1; k <= d; k++) {
+        oW[k] = off;
+        off += R[k] * L[k];
+    }
+    long long szA = 1, szB = 1, szP = 1, szZ = 1, szM = 1;
+    for (int k = 0; k < d; k++) {
+        const long long Rp = R[k + 1];
+        szA = (long long)n[k] * Rp * L[k] > szA ? (long long)n[k] * Rp * L[k] : szA;
+        szB = (long long)rx[k] * L[k] * n[k] * ry[k + 1] > szB ? (long long)rx[k] * L[k] * n[k] * ry[k + 1] : szB;
+        szP = (long long)rx[k] * n[k] * ry[k + 1] * L[k] > szP ? (long long)rx[k] * n[k] * ry[k + 1] * L[k] : szP;
+        szZ = (long long)L[k] * n[k] * Rp > szZ ? (long long)L[k] * n[k] * Rp : szZ;
+        szM = (long long)L[k] * R[k] > szM ? (long long)L[k] * R[k] : szM;
+    }
+    const long long oA = off, oB = oA + szA, oP = oB + szB, oZ = oP + szP, oM0 = oZ + szZ, oM1 = oM0 + szM;
+    const long long total = oM1 + szM + 64;
+    if ((rc = ptt_ws2_reserve(c, (size_t)total * sizeof(double)))) return rc;
+    double* ws = (double*)c->ws2;
+    // input core pointers
+    if ((rc = ptt_pull_desc((ptt_tt*)x)) || (rc = ptt_pull_desc((ptt_tt*)y))) return rc;
+    const double* const* xc = x->hd.core;
+    const double* const* yc = y->hd.core;
+
+    for (int k = 1; k < d; k++) {
+        const long long cnt = (long long)L[k] * n[k] * L[k + 1];
+        k_gauss<<<blocks_for(cnt), 256, 0, c->stream>>>(ws + oG[k], cnt, seed, k);
+        PTT_LAUNCHED(c);
+    }
+    k_fill<<<1, 32, 0, c->stream>>>(ws + oW[d], 1, 1.0);
+    PTT_LAUNCHED(c);
+
+    // ---- right-to-left sketch contractions -------------------------------
+    for (int k = d - 1; k >= 1; k--) {
+        const long long Rp = R[k + 1];
+        const int Lk = L[k], Lp = L[k + 1], nk = n[k];
+        const int rxk = rx[k], ryk = ry[k], rxp = rx[k + 1], ryp = ry[k + 1];
+        GemmB g;
+        // A_j = W_{k+1} G_j^T   (Rp x Lk), j < n
+        g = GemmB{ws + oW[k + 1], 1, Rp, 0, 0,
+                  ws + oG[k], (long long)Lk * nk, 1, Lk, 0,
+                  ws + oA, 1, Rp, Rp * Lk, 0,
+                  (int)Rp, Lk, Lp, nk, 1, 1.0, 0.0};
+        if ((rc = gemm(c, g))) return rc;
+        // Bt[ix][c][j + n ly] = sum_jx x[ix, j, jx] A_j[ly + ryp jx, c]
+        g = GemmB{xc[k], 1, (long long)rxk * nk, rxk, 0,
+                  ws + oA, ryp, Rp, Rp * Lk, 1,
+                  ws + oB, (long long)Lk * nk * ryp, (long long)nk * ryp, 1, nk,
+                  rxk, Lk, rxp, nk, ryp, 1.0, 0.0};
+        if ((rc = gemm(c, g))) return rc;
+        // W_k[ky + ryk ix, c] = sum_q y_right[ky, q] Bt[ix][c][q]
+        g = GemmB{yc[k], 1, ryk, 0, 0,
+                  ws + oB, 1, (long long)nk * ryp, (long long)Lk * nk * ryp, 0,
+                  ws + oW[k], 1, R[k], ryk, 0,
+                  ryk, Lk, nk * ryp, rxk, 1, 1.0, 0.0};
+        if ((rc = gemm(c, g))) return rc;
+    }
+
+    // ---- left-to-right orthogonalisation against the sketch ----------------
+    double* M = ws + oM0;
+    double* Mn = ws + oM1;
+    k_fill<<<1, 32, 0, c->stream>>>(M, 1, 1.0);
+    PTT_LAUNCHED(c);
+    int r = 1;
+    int zr[PTT_MAX_DIM + 1];
+    zr[0] = 1;
+    if ((rc = ptt_pull_desc(z))) return rc;
+    for (int k = 0; k < d; k++) {
+        const long long Rp = R[k + 1];
+        const int nk = n[k], rxk = rx[k], ryk = ry[k], rxp = rx[k + 1], ryp = ry[k + 1];
+        GemmB g;
+        // P[ix][q][c] = sum_ky M[c, ky + ryk ix] y_right[ky, q]
+        g = GemmB{M, 1, r, (long long)r * ryk, 0,
+                  yc[k], 1, ryk, 0, 0,
+                  ws + oP, 1, r, (long long)r * nk * ryp, 0,
+                  r, nk * ryp, ryk, rxk, 1, 1.0, 0.0};
+        if ((rc = gemm(c, g))) return rc;
+        // Z[c + r j, ly + ryp jx] = sum_ix P[ix][j + n ly][c] x[ix, j, jx]
+        double* Zp = (k == d - 1) ? z->hd.core[k] : ws + oZ;
+        g = GemmB{ws + oP, 1, (long long)r * nk * ryp, r, (long long)r * nk,
+                  xc[k], 1, (long long)rxk * nk, rxk, 0,
+                  Zp, 1, (long long)r * nk * ryp, r, (long long)r * nk,
+                  r, rxp, rxk, nk, ryp, 1.0, 0.0};
+        if ((rc = gemm(c, g))) return rc;
+        if (k == d - 1) {
+            zr[k] = r;
+            zr[d] = 1;
+            break;
+        }
+        const int Lp = L[k + 1];
+        // Y = Z W_{k+1} into z core k, then QR in place (core k <- Q)
+        g = GemmB{ws + oZ, 1, (long long)r * nk, 0, 0,
+                  ws + oW[k + 1], 1, Rp, 0, 0,
+                  z->hd.core[k], 1, (long long)r * nk, 0, 0,
+                  r * nk, Lp, (int)Rp, 1, 1, 1.0, 0.0};
+        if ((rc = gemm(c, g))) return rc;
+        int rr[2] = {r, Lp};
+        if ((rc = ptt_set_ranks_async(z, k, rr, 2))) return rc;
+        if ((rc = ptt_round_phases(z, 0.0, NULL, 4, k))) return rc;
+        if ((rc = ptt_pull_desc(z))) return rc;
+        const int q = r * nk < Lp ? r * nk : Lp;
+        // M' = Q^T Z   (q x Rp)
+        g = GemmB{z->hd.core[k], (long long)r * nk, 1, 0, 0,
+                  ws + oZ, 1, (long long)r * nk, 0, 0,
+                  Mn, 1, q, 0, 0,
+                  q, (int)Rp, r * nk, 1, 1, 1.0, 0.0};
+        if ((rc = gemm(c, g))) return rc;
+        double* t = M;
+        M = Mn;
+        Mn = t;
+        zr[k] = r;
+        r = q;
+    }
+    if ((rc = ptt_set_ranks_async(z, 0, zr, d + 1))) return rc;
+    return ptt_round_phases(z, tol, maxrank, 2, 0);
+}

@@ -80,6 +80,8 @@ struct Plan {
     int* pass;        // device ints [P-1]
     int* cnt;         // device counters [P-1]
     Info* info;       // device
+    double* stats;    // device, per-bond records of the rounding (may be null)
+    double* work;     // device accumulator of algorithmic bytes (may be null)
 };
 
 // Leaf row range (identical on host and device).  The non-empty leaves are

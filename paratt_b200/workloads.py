@@ -1,0 +1,61 @@
+"""Seeded synthetic inputs for the paratt_b200 benchmark and examples.
+
+Gaussian-sum initial conditions on the periodic box [-L/2, L/2)^d with grid
+x_j = -L/2 + j L/n, stored as rank-G tensor trains in the layout the
+reference's attac_sum_of_product builds (paratt.c:517-568): core 0 =
+[v_0 | v_1 | ...], diagonal interior cores, stacked last core.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+# Reaction-Burgers configurations (d, n, rank cap, tol, dt, steps, Gaussians, seed)
+CONFIGS = {
+    "c0": dict(d=20, n=64, maxrank=20, tol=1e-8, dt=1e-3, steps=100, ngauss=1, seed=0),
+    "c2": dict(d=40, n=128, maxrank=32, tol=1e-8, dt=1e-3, steps=500, ngauss=3, seed=3),
+    "c4": dict(d=40, n=256, maxrank=64, tol=1e-8, dt=1e-3, steps=1000, ngauss=3, seed=3),
+}
+
+
+def grid(n, L=10.0):
+    return -L / 2 + np.arange(n) * (L / n)
+
+
+def gaussian_sum_tt(d, n, centres, widths, L=10.0):
+    x = grid(n, L)
+    G = len(widths)
+    cores = []
+    for k in range(d):
+        vecs = [np.exp(-(x - centres[g][k]) ** 2 / (2 * widths[g] ** 2)) for g in range(G)]
+        if G == 1:
+            cores.append(vecs[0].reshape(1, n, 1))
+        elif k == 0:
+            cores.append(np.stack(vecs, axis=1).reshape(1, n, G))
+        elif k == d - 1:
+            cores.append(np.stack(vecs, axis=0).reshape(G, n, 1))
+        else:
+            c = np.zeros((G, n, G))
+            for g in range(G):
+                c[g, :, g] = vecs[g]
+            cores.append(c)
+    return cores
+
+
+def initial_condition(d, n, ngauss, seed, L=10.0):
+    """Sum of `ngauss` Gaussians, centres U[-2,2]^d and widths U[0.3,0.8]
+    (ngauss == 1 with seed 0: the centred Gaussian of width 0.5)."""
+    if ngauss == 1 and seed == 0:
+        return gaussian_sum_tt(d, n, np.zeros((1, d)), np.array([0.5]), L)
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(-2.0, 2.0, size=(ngauss, d))
+    widths = rng.uniform(0.3, 0.8, size=ngauss)
+    return gaussian_sum_tt(d, n, centres, widths, L)
+
+
+def rms_norm(cores):
+    """||X||_F / sqrt(prod n) by transfer matrices (host, small ranks only)."""
+    a = np.ones((1, 1))
+    for c in cores:
+        t = np.einsum("ik,kjd->ijd", a, c)
+        a = np.einsum("ijb,ijd->bd", c, t) / c.shape[1]
+    return float(np.sqrt(max(a[0, 0], 0.0)))
