@@ -155,6 +155,7 @@ PTT_API int ptt_dot(const ptt_tt* x, const ptt_tt* y, double* out);  /* <X,Y>/pr
 PTT_API int ptt_norm(const ptt_tt* x, double* out);                  /* RMS norm     */
 PTT_API int ptt_entry(const ptt_tt* x, const int* idx, double* out);
 
+
 #ifdef __cplusplus
 }
 #endif

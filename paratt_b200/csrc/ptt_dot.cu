@@ -135,3 +135,4 @@ extern "C" int ptt_entry(const ptt_tt* x, const int* idx, double* out) {
     *out = c->h_scalars[0];
     return PTT_OK;
 }
+
