@@ -155,6 +155,19 @@ PTT_API int ptt_dot(const ptt_tt* x, const ptt_tt* y, double* out);  /* <X,Y>/pr
 PTT_API int ptt_norm(const ptt_tt* x, double* out);                  /* RMS norm     */
 PTT_API int ptt_entry(const ptt_tt* x, const int* idx, double* out);
 
+/* ptt_dot without any device allocation.  No counterpart in the reference:
+ * for callers that must not have a library call cudaMalloc (a framework that
+ * owns the GPU's memory pool, a loop that cannot afford cudaMalloc's implicit
+ * synchronisation, an embedding that forbids allocation after start-up).
+ * Scratch lives in a fixed device array of PTT_DOT_NOALLOC_MAX_DOUBLES
+ * doubles (4 MiB, held by every GPU that loads the library until exit); a
+ * call needs 2*max_k(rx_k ry_k) + max_k(rx_k n_k ry_{k+1}) doubles and fails
+ * with PTT_ERR_CAPACITY beyond that.  The first call on a device looks up the
+ * array's address on that device: make it before any stream capture.  All
+ * calls share the array, so calls that overlap on the GPU race.  Reads the
+ * ranks and the result back (synchronises). */
+#define PTT_DOT_NOALLOC_MAX_DOUBLES (1 << 19)
+PTT_API int ptt_dot_noalloc(const ptt_tt* x, const ptt_tt* y, double* out);
 
 #ifdef __cplusplus
 }

@@ -68,6 +68,7 @@ _SIGS = {
     "ptt_mult_diag": (_i, [_p, _i, _dp]),
     "ptt_stencil": (_i, [_p, _i, _dp, _i]),
     "ptt_dot": (_i, [_p, _p, _dp]),
+    "ptt_dot_noalloc": (_i, [_p, _p, _dp]),
     "ptt_norm": (_i, [_p, _dp]),
     "ptt_entry": (_i, [_p, _ip, _dp]),
     "ptt_op_sum": (_i, [_p, _dp, _i, _d, _p]),
@@ -241,6 +242,12 @@ class TT:
     def dot(self, other):
         v = C.c_double()
         _check(lib().ptt_dot(self.h, other.h, C.byref(v)))
+        return v.value
+
+    def dot_noalloc(self, other):
+        """ptt_dot using the fixed device scratch array (no allocation)."""
+        v = C.c_double()
+        _check(lib().ptt_dot_noalloc(self.h, other.h, C.byref(v)))
         return v.value
 
     def norm(self):

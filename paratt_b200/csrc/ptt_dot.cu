@@ -136,3 +136,93 @@ extern "C" int ptt_entry(const ptt_tt* x, const int* idx, double* out) {
     return PTT_OK;
 }
 
+// ---------------------------------------------------------------------------
+// ptt_dot_noalloc: the same inner product with no device allocation.
+//
+// Some callers cannot let a library call cudaMalloc: a host framework that
+// has already reserved the GPU's memory for its own pool, a latency-bound
+// loop where cudaMalloc's implicit device-wide synchronisation would stall
+// work on other streams, or an embedding that forbids allocation after
+// start-up.  This variant keeps its scratch (two transfer matrices and the
+// partial contraction T) in a fixed file-scope device array instead of the
+// context workspace.  The array is PTT_DOT_NOALLOC_MAX_DOUBLES doubles
+// (4 MiB) and exists on every GPU that loads the library until the process
+// exits.  Requests that do not fit are rejected with PTT_ERR_CAPACITY.
+//
+// The array is shared by every call: it keeps the last call's contents, and
+// nothing in it has to start at zero (the start value of the transfer matrix
+// is written by a kernel of each call).  Two calls whose kernels overlap on
+// the GPU (different streams or contexts on one device) race on it.
+//
+// Host code cannot use the array's name as a device address, so its address
+// is looked up once per device (cudaGetSymbolAddress, with that device
+// current) on the first call made on that device; make that first call
+// before any stream capture on the device.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_dot_scratch[PTT_DOT_NOALLOC_MAX_DOUBLES];
+
+#define PTT_NOALLOC_MAX_DEVICES 64
+static double* g_dot_scratch_addr[PTT_NOALLOC_MAX_DEVICES];
+
+static int dot_scratch(int device, double** out) {
+    if (device < 0 || device >= PTT_NOALLOC_MAX_DEVICES)
+        return ptt_set_error(PTT_ERR_ARG, "ptt_dot_noalloc: device %d out of range", device);
+    if (!g_dot_scratch_addr[device]) {
+        void* p = NULL;
+        PTT_CUDA(cudaSetDevice(device));
+        PTT_CUDA(cudaGetSymbolAddress(&p, g_dot_scratch));
+        g_dot_scratch_addr[device] = (double*)p;
+    }
+    *out = g_dot_scratch_addr[device];
+    return PTT_OK;
+}
+
+extern "C" int ptt_dot_noalloc(const ptt_tt* x, const ptt_tt* y, double* out) {
+    if (!x || !y || !out || x->d != y->d) return ptt_set_error(PTT_ERR_ARG, "ptt_dot_noalloc: bad arguments");
+    for (int k = 0; k < x->d; k++)
+        if (x->n[k] != y->n[k]) return ptt_set_error(PTT_ERR_ARG, "ptt_dot_noalloc: mode %d differs", k);
+    ptt_ctx* c = x->ctx;
+    if (y->ctx != c) {
+        PTT_CUDA(cudaEventRecord(y->ctx->ev_fork, y->ctx->stream));
+        PTT_CUDA(cudaStreamWaitEvent(c->stream, y->ctx->ev_fork, 0));
+    }
+    double* scratch = NULL;
+    int rc = dot_scratch(c->device, &scratch);
+    if (rc) return rc;
+    // size the scratch from the actual ranks (reading them synchronises)
+    int rx[PTT_MAX_DIM + 1], ry[PTT_MAX_DIM + 1];
+    if ((rc = ptt_tt_get_ranks((ptt_tt*)x, rx)) || (rc = ptt_tt_get_ranks((ptt_tt*)y, ry))) return rc;
+    long long amax = 1, tmax = 1;
+    for (int k = 0; k <= x->d; k++) amax = (long long)rx[k] * ry[k] > amax ? (long long)rx[k] * ry[k] : amax;
+    for (int k = 0; k < x->d; k++) {
+        const long long t = (long long)rx[k] * x->n[k] * ry[k + 1];
+        tmax = t > tmax ? t : tmax;
+    }
+    if (2 * amax + tmax > PTT_DOT_NOALLOC_MAX_DOUBLES)
+        return ptt_set_error(PTT_ERR_CAPACITY,
+                             "ptt_dot_noalloc: needs %lld doubles of scratch, the fixed array holds %d "
+                             "(use ptt_dot, which allocates)",
+                             2 * amax + tmax, (int)PTT_DOT_NOALLOC_MAX_DOUBLES);
+    double* A0 = scratch;
+    double* A1 = A0 + amax;
+    double* T = A1 + amax;
+    k_set_one<<<1, 1, 0, c->stream>>>(A0);
+    PTT_LAUNCHED(c);
+    for (int k = 0; k < x->d; k++) {
+        const long long tc = (long long)rx[k] * x->n[k] * ry[k + 1];
+        int bx = (int)((tc + 255) / 256);
+        if (bx > 4096) bx = 4096;
+        k_dot_t<<<bx, 256, 0, c->stream>>>(x->dd, y->dd, k, A0, T);
+        PTT_LAUNCHED(c);
+        k_dot_a<<<dim3(ry[k + 1], rx[k + 1]), 256, 0, c->stream>>>(x->dd, y->dd, k, T, A1);
+        PTT_LAUNCHED(c);
+        double* s = A0;
+        A0 = A1;
+        A1 = s;
+    }
+    PTT_CUDA(cudaMemcpyAsync(c->h_scalars, A0, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    rc = ptt_ctx_synchronize(c);
+    if (rc) return rc;
+    *out = c->h_scalars[0];
+    return PTT_OK;
+}
