@@ -103,6 +103,11 @@ PTT_API int ptt_tt_device_cores(const ptt_tt* t, double** cores, int** ranks);
  * absolute on the grid-normalised norm ||X||_F / sqrt(prod n_k); per-bond
  * threshold tol/sqrt(d-1); maxrank has d+1 entries (NULL = capacity). */
 PTT_API int ptt_round(ptt_tt* x, double tol, const int* maxrank);
+/* By default ptt_round reads the actual ranks back (one synchronisation) and
+ * sizes its tiles and trees from them.  With fixed plans on, it sizes them
+ * from the rank capacity instead and never synchronises (for stream capture
+ * of a whole step).  Results are identical either way. */
+PTT_API int ptt_ctx_fixed_plans(ptt_ctx* ctx, int on);
 /* Per-bond record of the context's last ptt_round (bond i = 1..d-1, record i;
  * PTT_STAT_LEN doubles each): rank, numerical rank, Jacobi sweeps, q, r_i,
  * dropped tail sum of squares, threshold, 0, then the top PTT_STAT_NSIG

@@ -73,6 +73,7 @@ _SIGS = {
     "ptt_entry": (_i, [_p, _ip, _dp]),
     "ptt_op_sum": (_i, [_p, _dp, _i, _d, _p]),
     "ptt_ctx_mark": (_i, [_p, _i]),
+    "ptt_ctx_fixed_plans": (_i, [_p, _i]),
     "ptt_ctx_elapsed": (_i, [_p, _i, _i, _dp]),
     "ptt_ctx_time_kernels": (_i, [_p, _i]),
     "ptt_ctx_kernel_time": (_i, [_p, _dp, C.POINTER(C.c_longlong)]),
@@ -137,6 +138,10 @@ class Context:
         out = np.zeros((d, STAT_LEN))
         _check(lib().ptt_round_stats(self.h, d, out.ctypes.data_as(_dp)))
         return out
+
+    def fixed_plans(self, on=True):
+        """Size rounding plans by capacity (no rank read-back) when on."""
+        _check(lib().ptt_ctx_fixed_plans(self.h, 1 if on else 0))
 
     def mark(self, slot):
         _check(lib().ptt_ctx_mark(self.h, slot))

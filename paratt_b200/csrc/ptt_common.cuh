@@ -32,6 +32,7 @@ struct ptt_ctx {
     cudaStream_t side;            // second stream for overlapped work
     cudaEvent_t ev_fork, ev_join;
     int* d_status;                // device status word (first error wins)
+    int fixed_plans;              // 1: size rounding plans by capacity (no rank read-back)
     long long launches;
     // generic device workspace (grown on demand, never shrunk)
     void* ws;

@@ -678,8 +678,10 @@ static int launch_apply(ptt_ctx* c, ptt_tt* x, int k, int mode, Plan& pl, double
 
 // phases: 1 = left-to-right orthogonalisation, 2 = right-to-left truncation,
 // 4 = QR of the single core `only` (left unfolding; core <- Q, r_{only+1} <- q).
+// rk[k]: upper bound of rank k for the whole call (the capacity, or the
+// actual ranks when they were read back; ranks only shrink while rounding).
 template <int CT>
-static int round_impl(ptt_tt* x, double delta, const int* maxr, int phases, int only) {
+static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, int phases, int only) {
     ptt_ctx* c = x->ctx;
     const int d = x->d;
     int rc = set_attrs<CT>();
@@ -689,7 +691,7 @@ static int round_impl(ptt_tt* x, double delta, const int* maxr, int phases, int 
     int PMAX = 1, KLMAX = 1;
     for (int i = 0; i < d; i++) {
         Plan t;
-        long long ml = (long long)x->rcap[i] * x->n[i], mr = (long long)x->n[i] * x->rcap[i + 1];
+        long long ml = (long long)rk[i] * x->n[i], mr = (long long)x->n[i] * rk[i + 1];
         plan_bond(CT, ml > mr ? ml : mr, KC, &t);
         if (t.P > PMAX) PMAX = t.P;
         if (t.KL > KLMAX) KLMAX = t.KL;
@@ -726,7 +728,7 @@ static int round_impl(ptt_tt* x, double delta, const int* maxr, int phases, int 
 
     if (phases & 4) {
         const int i = only;
-        Plan pl = mkplan((long long)x->rcap[i] * x->n[i]);
+        Plan pl = mkplan((long long)rk[i] * x->n[i]);
         if ((rc = launch_factor<CT>(c, x, i, LEFT, pl, ws))) return rc;
         k_set_identity<<<32, 256, 0, c->stream>>>(pl, ws);
         PTT_LAUNCHED(c);
@@ -737,10 +739,10 @@ static int round_impl(ptt_tt* x, double delta, const int* maxr, int phases, int 
     }
     // left-to-right orthogonalisation
     for (int i = 0; i < d - 1 && (phases & 1); i++) {
-        Plan pl = mkplan((long long)x->rcap[i] * x->n[i]);
+        Plan pl = mkplan((long long)rk[i] * x->n[i]);
         if ((rc = launch_factor<CT>(c, x, i, LEFT, pl, ws))) return rc;
         {
-            const long long ncap = (long long)x->n[i + 1] * x->rcap[i + 2];
+            const long long ncap = (long long)x->n[i + 1] * rk[i + 2];
             int gy = (int)((ncap + GT - 1) / GT);
             if (gy > 4096) gy = 4096;
             k_gemm_rx<<<dim3((CT + GT - 1) / GT, gy), 256, 0, c->stream>>>(x->dd, i + 1, pl, ws);
@@ -754,9 +756,9 @@ static int round_impl(ptt_tt* x, double delta, const int* maxr, int phases, int 
     }
     // right-to-left truncation
     for (int i = d - 1; i >= 1 && (phases & 2); i--) {
-        Plan pl = mkplan((long long)x->n[i] * x->rcap[i + 1]);
+        Plan pl = mkplan((long long)x->n[i] * rk[i + 1]);
         if ((rc = launch_factor<CT>(c, x, i, RIGHT_T, pl, ws))) return rc;
-        const int mr = maxr ? maxr[i] : x->rcap[i];
+        const int mr = maxr ? maxr[i] : rk[i];
         ptt_time_begin(c, PTT_TIME_SVD);
         k_svd_jacobi<CT><<<1, SVD_NT, svd_smem<CT>(), c->stream>>>(pl, ws, delta, mr, i, c->d_status);
         ptt_time_end(c, PTT_TIME_SVD);
@@ -765,7 +767,7 @@ static int round_impl(ptt_tt* x, double delta, const int* maxr, int phases, int 
         PTT_LAUNCHED(c);
         if ((rc = launch_apply<CT>(c, x, i, RIGHT_T, pl, ws, &info->rank, CT))) return rc;
         {
-            const long long mcap = (long long)x->rcap[i - 1] * x->n[i - 1];
+            const long long mcap = (long long)rk[i - 1] * x->n[i - 1];
             int gx = (int)((mcap + GT - 1) / GT);
             if (gx > 4096) gx = 4096;
             k_gemm_xm<<<dim3(gx, (CT + GT - 1) / GT), 256, 0, c->stream>>>(x->dd, i - 1, pl, ws);
@@ -799,14 +801,30 @@ int ptt_round_phases(ptt_tt* x, double tol, const int* maxrank, int phases, int 
     if (!x) return ptt_set_error(PTT_ERR_ARG, "ptt_round: null tt");
     if (x->d < 2) return PTT_OK;
     if (!(tol >= 0.0)) return ptt_set_error(PTT_ERR_ARG, "ptt_round: tol must be >= 0");
-    int rmax = 1;
-    for (int k = 0; k <= x->d; k++) rmax = x->rcap[k] > rmax ? x->rcap[k] : rmax;
-    const double delta = ptt_round_threshold(x, tol);
+    int rk[PTT_MAX_DIM + 1];
     cudaSetDevice(x->ctx->device);
-    if (rmax <= 32) return round_impl<32>(x, delta, maxrank, phases, only);
-    if (rmax <= 64) return round_impl<64>(x, delta, maxrank, phases, only);
-    if (rmax <= 128) return round_impl<128>(x, delta, maxrank, phases, only);
-    return ptt_set_error(PTT_ERR_CAPACITY, "ptt_round: rank capacity %d > 128 not supported", rmax);
+    if (x->ctx->fixed_plans) {
+        // capacity-sized plan: no host synchronisation (stream capture)
+        for (int k = 0; k <= x->d; k++) rk[k] = x->rcap[k];
+    } else {
+        // plan from the actual ranks (one read-back): tiles, trees and grids
+        // then match the tensor instead of its capacity
+        int rc = ptt_tt_get_ranks(x, rk);
+        if (rc) return rc;
+    }
+    int rmax = 1;
+    for (int k = 0; k <= x->d; k++) rmax = rk[k] > rmax ? rk[k] : rmax;
+    const double delta = ptt_round_threshold(x, tol);
+    if (rmax <= 32) return round_impl<32>(x, rk, delta, maxrank, phases, only);
+    if (rmax <= 64) return round_impl<64>(x, rk, delta, maxrank, phases, only);
+    if (rmax <= 128) return round_impl<128>(x, rk, delta, maxrank, phases, only);
+    return ptt_set_error(PTT_ERR_CAPACITY, "ptt_round: rank %d > 128 not supported", rmax);
+}
+
+extern "C" int ptt_ctx_fixed_plans(ptt_ctx* c, int on) {
+    if (!c) return ptt_set_error(PTT_ERR_ARG, "null context");
+    c->fixed_plans = on ? 1 : 0;
+    return PTT_OK;
 }
 
 extern "C" int ptt_round(ptt_tt* x, double tol, const int* maxrank) {

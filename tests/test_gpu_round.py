@@ -82,3 +82,20 @@ def test_round_small_modes(ctx):
     got = X.get()
     assert O.ranks_of(got) == O.ranks_of(ref)
     assert O.rel_diff_exact(got, ref) <= 1e-12
+
+
+def test_fixed_plans_same_result(ctx):
+    """Capacity-sized plans (no rank read-back) give the same rounding."""
+    x = gapped_tt([6, 5, 7, 4, 6], [1, 6, 8, 9, 6, 1], 11, [1, 3, 4, 5, 2, 1])
+    tol = 1e-6 * O.norm(x)
+    A = P.TT.from_cores(ctx, x, [1] + [100] * 4 + [1])
+    B = P.TT.from_cores(ctx, x, [1] + [100] * 4 + [1])
+    A.round(tol, 64)
+    ctx.fixed_plans(True)
+    try:
+        B.round(tol, 64)
+    finally:
+        ctx.fixed_plans(False)
+    a, b = A.get(), B.get()
+    assert O.ranks_of(a) == O.ranks_of(b)
+    assert O.rel_diff_exact(a, b) <= 1e-13
