@@ -135,6 +135,14 @@ PTT_API int ptt_op_sum(const ptt_tt* x, const double* sten, int slen, double shi
 PTT_API int ptt_round_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* ell,
                                unsigned long long seed, double tol, const int* maxrank);
 
+/* Randomised rounding of x (y == NULL) or of x (.) y, as ptt_round_hadamard,
+ * plus the acceptance check of the sketch: *accepted = 1 when every bond's
+ * truncated rank stayed at least `pad` below its sketch rank (or the sketch
+ * spanned the whole bond), else 0 -- the caller then falls back to the
+ * deterministic rounding.  Reads ranks (synchronises). */
+PTT_API int ptt_round_sketch(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* ell,
+                             unsigned long long seed, double tol, const int* maxrank, int pad, int* accepted);
+
 /* ---- reaction-Burgers step-truncation RK2 ------------------------------- */
 typedef struct {
     double dt;        /* time step                                            */
@@ -154,6 +162,36 @@ PTT_API int ptt_rxn_ws_counts(const ptt_rxn_ws* ws, long long* formal, long long
 PTT_API int ptt_rxn_burgers_F(ptt_tt* u, ptt_tt* F, ptt_rxn_ws* ws, const ptt_rxn_params* p);
 /* u <- one step-truncation midpoint step of the reaction-Burgers equation. */
 PTT_API int ptt_rxn_burgers_rk2_step(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p);
+
+/* The same step with every rounding done by a Gaussian TT sketch of per-bond
+ * ranks ell[k] (d+1 entries) plus the deterministic truncation, F taken as one
+ * sketch of the formal sum a + b; a rounding whose sketch fails the check of
+ * ptt_round_sketch (margin `pad`) is redone deterministically. */
+PTT_API int ptt_rxn_burgers_rk2_step_sketch(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int* ell,
+                                            int pad);
+PTT_API int ptt_rxn_ws_sketch_counts(const ptt_rxn_ws* ws, long long* calls, long long* fallbacks);
+/* Logging (reads each rounding's statistics back): per step the largest kept
+ * rank of every bond over the step's roundings, and the top PTT_STAT_NSIG
+ * singular values of every bond of the last rounding with its threshold. */
+PTT_API int ptt_rxn_ws_log(ptt_rxn_ws* ws, int on);
+PTT_API int ptt_rxn_ws_last_step(const ptt_rxn_ws* ws, int* ranks, double* sig, double* delta);
+
+/* ---- sketch-rank proposer: MLP nin -> width -> width -> 1 (ReLU), BF16
+ * weights, FP32 accumulation, trained with hand-written kernels (Adam) ---- */
+typedef struct ptt_mlp ptt_mlp;
+PTT_API ptt_mlp* ptt_mlp_create(ptt_ctx* ctx, int nin, int width, unsigned long long seed);
+PTT_API void ptt_mlp_destroy(ptt_mlp* m);
+PTT_API long long ptt_mlp_num_params(const ptt_mlp* m);
+/* parameter vector (FP32 master copy): W1[w x nin] b1[w] W2[w x w] b2[w] W3[w] b3 */
+PTT_API int ptt_mlp_get_params(ptt_mlp* m, float* out);
+PTT_API int ptt_mlp_set_params(ptt_mlp* m, const float* in);
+/* host buffers: x[B x nin] row-major, y[B], t[B] */
+PTT_API int ptt_mlp_forward(ptt_mlp* m, const float* x, int B, float* y);
+/* loss = mean(a (y - t)^2), a = under-weight if y < t else 1; gradients of
+ * the BF16-weight network with respect to the parameters */
+PTT_API int ptt_mlp_grads(ptt_mlp* m, const float* x, const float* t, int B, float* grads, float* loss);
+PTT_API int ptt_mlp_train_step(ptt_mlp* m, const float* x, const float* t, int B, float lr, float* loss);
+PTT_API int ptt_mlp_set_under_weight(ptt_mlp* m, float w);
 
 /* Reductions (these read a scalar back, so they synchronise). */
 PTT_API int ptt_dot(const ptt_tt* x, const ptt_tt* y, double* out);  /* <X,Y>/prod n */

@@ -87,6 +87,22 @@ _SIGS = {
     "ptt_rxn_ws_counts": (_i, [_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "ptt_rxn_burgers_F": (_i, [_p, _p, _p, _p]),
     "ptt_rxn_burgers_rk2_step": (_i, [_p, _p, _p]),
+    "ptt_round_sketch": (_i, [_p, _p, _p, _ip, C.c_ulonglong, _d, _ip, _i, _ip]),
+    "ptt_rxn_burgers_rk2_step_sketch": (_i, [_p, _p, _p, _ip, _i]),
+    "ptt_rxn_ws_sketch_counts": (_i, [_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "ptt_rxn_ws_log": (_i, [_p, _i]),
+    "ptt_rxn_ws_last_step": (_i, [_p, _ip, _dp, _dp]),
+    "ptt_mlp_create": (_p, [_p, _i, _i, C.c_ulonglong]),
+    "ptt_mlp_destroy": (None, [_p]),
+    "ptt_mlp_num_params": (C.c_longlong, [_p]),
+    "ptt_mlp_get_params": (_i, [_p, C.POINTER(C.c_float)]),
+    "ptt_mlp_set_params": (_i, [_p, C.POINTER(C.c_float)]),
+    "ptt_mlp_forward": (_i, [_p, C.POINTER(C.c_float), _i, C.POINTER(C.c_float)]),
+    "ptt_mlp_grads": (_i, [_p, C.POINTER(C.c_float), C.POINTER(C.c_float), _i, C.POINTER(C.c_float),
+                           C.POINTER(C.c_float)]),
+    "ptt_mlp_train_step": (_i, [_p, C.POINTER(C.c_float), C.POINTER(C.c_float), _i, C.c_float,
+                                C.POINTER(C.c_float)]),
+    "ptt_mlp_set_under_weight": (_i, [_p, C.c_float]),
 }
 
 
@@ -316,6 +332,28 @@ class RxnBurgers:
         _check(lib().ptt_rxn_burgers_rk2_step(u.h, self.h, C.byref(self.p)))
         return u
 
+    def step_sketch(self, u: TT, ell, pad=4):
+        e = _iarr(ell)
+        _check(lib().ptt_rxn_burgers_rk2_step_sketch(u.h, self.h, C.byref(self.p), e, int(pad)))
+        return u
+
+    def sketch_counts(self):
+        c, f = C.c_longlong(), C.c_longlong()
+        _check(lib().ptt_rxn_ws_sketch_counts(self.h, C.byref(c), C.byref(f)))
+        return c.value, f.value
+
+    def log(self, on=True):
+        _check(lib().ptt_rxn_ws_log(self.h, 1 if on else 0))
+
+    def last_step(self, d):
+        """(max kept rank per bond over the last step's roundings [d+1],
+        top-16 singular values per bond of the last rounding [d+1, 16], threshold)"""
+        r = (C.c_int * (d + 1))()
+        sig = np.zeros((d + 1, STAT_NSIG))
+        dl = C.c_double()
+        _check(lib().ptt_rxn_ws_last_step(self.h, r, sig.ctypes.data_as(_dp), C.byref(dl)))
+        return list(r), sig, dl.value
+
     def counts(self):
         f, s = C.c_longlong(), C.c_longlong()
         _check(lib().ptt_rxn_ws_counts(self.h, C.byref(f), C.byref(s)))
@@ -324,4 +362,68 @@ class RxnBurgers:
     def close(self):
         if self.h:
             lib().ptt_rxn_ws_destroy(self.h)
+            self.h = None
+
+
+def round_sketch(x: TT, y, z: TT, ell, seed, tol, maxrank=None, pad=4):
+    """Sketch rounding of x (y None) or x (.) y; returns whether accepted."""
+    e = _iarr(ell if hasattr(ell, "__len__") else [ell] * (x.d + 1))
+    mr = None if maxrank is None else _iarr(maxrank if hasattr(maxrank, "__len__") else [maxrank] * (x.d + 1))
+    ok = C.c_int()
+    _check(lib().ptt_round_sketch(x.h, y.h if y is not None else None, z.h, e, C.c_ulonglong(seed), float(tol), mr,
+                                  int(pad), C.byref(ok)))
+    return bool(ok.value)
+
+
+_fp = C.POINTER(C.c_float)
+
+
+class MLP:
+    """Sketch-rank proposer (ptt_mlp): nin -> width -> width -> 1."""
+
+    def __init__(self, ctx: Context, nin, width=64, seed=1):
+        self.ctx, self.nin, self.width = ctx, nin, width
+        self.h = lib().ptt_mlp_create(ctx.h, nin, width, C.c_ulonglong(seed))
+        if not self.h:
+            _check(lib().ptt_last_error() or PTT_ERR_ARG)
+        self.np = int(lib().ptt_mlp_num_params(self.h))
+
+    def params(self):
+        out = np.zeros(self.np, dtype=np.float32)
+        _check(lib().ptt_mlp_get_params(self.h, out.ctypes.data_as(_fp)))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(lib().ptt_mlp_set_params(self.h, p.ctypes.data_as(_fp)))
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros(x.shape[0], dtype=np.float32)
+        _check(lib().ptt_mlp_forward(self.h, x.ctypes.data_as(_fp), x.shape[0], y.ctypes.data_as(_fp)))
+        return y
+
+    def grads(self, x, t):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.zeros(self.np, dtype=np.float32)
+        loss = C.c_float()
+        _check(lib().ptt_mlp_grads(self.h, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), x.shape[0],
+                                   g.ctypes.data_as(_fp), C.byref(loss)))
+        return g, loss.value
+
+    def train_step(self, x, t, lr):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = C.c_float()
+        _check(lib().ptt_mlp_train_step(self.h, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), x.shape[0],
+                                        C.c_float(lr), C.byref(loss)))
+        return loss.value
+
+    def set_under_weight(self, w):
+        _check(lib().ptt_mlp_set_under_weight(self.h, C.c_float(w)))
+
+    def close(self):
+        if self.h:
+            lib().ptt_mlp_destroy(self.h)
             self.h = None

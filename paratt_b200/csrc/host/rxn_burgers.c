@@ -21,6 +21,14 @@
  * u . u is formed formally (attacHadamard) while r_u^2 fits the rounding
  * kernels (<= 128) and is otherwise rounded through a Gaussian TT sketch of
  * rank min(r_u^2, maxrank + sketch_pad) without forming it.
+ *
+ * Sketch step (ptt_rxn_burgers_rk2_step_sketch): the same step with every
+ * rounding done by a Gaussian TT sketch of per-bond ranks ell[k] followed by
+ * the deterministic truncation, and F = T(a + b) taken in one sketch of the
+ * formal sum (no separate roundings of a and b).  A sketch is accepted when
+ * each bond's truncated rank stays `pad` below its sketch rank; otherwise
+ * that rounding is redone deterministically (the plain composition), and
+ * the fallback is counted.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -30,9 +38,14 @@
 
 struct ptt_rxn_ws {
     ptt_ctx* ctx;
-    int d;
-    ptt_tt *w, *a, *b, *k, *us;
-    long long hadamard_formal, hadamard_sketch;
+    int d, maxrank;
+    ptt_tt *w, *a, *b, *k, *us, *s, *t;
+    long long hadamard_formal, hadamard_sketch, sketch_calls, sketch_fallbacks;
+    int log;
+    int step_rank[PTT_MAX_DIM + 1];                   /* max kept rank per bond in this step */
+    double sig[(PTT_MAX_DIM + 1) * PTT_STAT_NSIG];   /* top spectra of the last rounding */
+    double delta;                                     /* its per-bond threshold */
+    double stats[(PTT_MAX_DIM + 1) * PTT_STAT_LEN];
 };
 
 #define FORMAL_MAX 128
@@ -48,12 +61,15 @@ ptt_rxn_ws* ptt_rxn_ws_create(ptt_ctx* c, int d, const int* n, int maxrank) {
     ptt_rxn_ws* ws = (ptt_rxn_ws*)calloc(1, sizeof(ptt_rxn_ws));
     ws->ctx = c;
     ws->d = d;
+    ws->maxrank = maxrank;
     ws->w = mk(c, d, n, FORMAL_MAX);
     ws->a = mk(c, d, n, 2 * maxrank);
     ws->b = mk(c, d, n, 2 * maxrank);
     ws->k = mk(c, d, n, 2 * maxrank);
     ws->us = mk(c, d, n, 2 * maxrank);
-    if (!ws->w || !ws->a || !ws->b || !ws->k || !ws->us) {
+    ws->s = mk(c, d, n, 4 * maxrank);
+    ws->t = mk(c, d, n, 2 * maxrank);
+    if (!ws->w || !ws->a || !ws->b || !ws->k || !ws->us || !ws->s || !ws->t) {
         ptt_rxn_ws_destroy(ws);
         return NULL;
     }
@@ -67,6 +83,8 @@ void ptt_rxn_ws_destroy(ptt_rxn_ws* ws) {
     ptt_tt_destroy(ws->b);
     ptt_tt_destroy(ws->k);
     ptt_tt_destroy(ws->us);
+    ptt_tt_destroy(ws->s);
+    ptt_tt_destroy(ws->t);
     free(ws);
 }
 
@@ -75,6 +93,47 @@ int ptt_rxn_ws_counts(const ptt_rxn_ws* ws, long long* formal, long long* sketch
     if (formal) *formal = ws->hadamard_formal;
     if (sketch) *sketch = ws->hadamard_sketch;
     return PTT_OK;
+}
+
+int ptt_rxn_ws_sketch_counts(const ptt_rxn_ws* ws, long long* calls, long long* fallbacks) {
+    if (!ws) return PTT_ERR_ARG;
+    if (calls) *calls = ws->sketch_calls;
+    if (fallbacks) *fallbacks = ws->sketch_fallbacks;
+    return PTT_OK;
+}
+
+int ptt_rxn_ws_log(ptt_rxn_ws* ws, int on) {
+    if (!ws) return PTT_ERR_ARG;
+    ws->log = on ? 1 : 0;
+    return PTT_OK;
+}
+
+int ptt_rxn_ws_last_step(const ptt_rxn_ws* ws, int* ranks, double* sig, double* delta) {
+    if (!ws) return PTT_ERR_ARG;
+    if (ranks) memcpy(ranks, ws->step_rank, sizeof(int) * (ws->d + 1));
+    if (sig) memcpy(sig, ws->sig, sizeof(double) * (ws->d + 1) * PTT_STAT_NSIG);
+    if (delta) *delta = ws->delta;
+    return PTT_OK;
+}
+
+/* After a rounding: fold its per-bond ranks into the step maximum and keep
+ * its spectra (logging mode only: reads the statistics back). */
+static int logged(ptt_rxn_ws* ws, int rc) {
+    if (rc || !ws->log) return rc;
+    const int d = ws->d;
+    if ((rc = ptt_round_stats(ws->ctx, d, ws->stats))) return rc;
+    for (int k = 1; k < d; k++) {
+        const double* st = ws->stats + (size_t)k * PTT_STAT_LEN;
+        const int r = (int)st[0];
+        if (r > ws->step_rank[k]) ws->step_rank[k] = r;
+        memcpy(ws->sig + (size_t)k * PTT_STAT_NSIG, st + 8, sizeof(double) * PTT_STAT_NSIG);
+        ws->delta = st[6];
+    }
+    return PTT_OK;
+}
+
+static void step_begin(ptt_rxn_ws* ws) {
+    for (int k = 0; k <= ws->d; k++) ws->step_rank[k] = 0;
 }
 
 static void stencils(const ptt_rxn_params* p, int d, int n, double* d2, double* d1) {
@@ -88,34 +147,45 @@ static void stencils(const ptt_rxn_params* p, int d, int n, double* d2, double* 
     d1[2] = -1.0 / (4.0 * d * h);
 }
 
-int ptt_rxn_burgers_F(ptt_tt* u, ptt_tt* F, ptt_rxn_ws* ws, const ptt_rxn_params* p) {
-    int rc, d, n[PTT_MAX_DIM], r[PTT_MAX_DIM + 1], mr[PTT_MAX_DIM + 1];
-    if (!u || !F || !ws || !p) return PTT_ERR_ARG;
-    if ((rc = ptt_tt_shape(u, &d, n, NULL))) return rc;
-    for (int k = 1; k < d; k++)
+static int shape(ptt_tt* u, int* d, int* n) {
+    int rc = ptt_tt_shape(u, d, n, NULL);
+    if (rc) return rc;
+    for (int k = 1; k < *d; k++)
         if (n[k] != n[0]) return PTT_ERR_ARG; /* one grid for every mode */
-    for (int k = 0; k <= d; k++) mr[k] = p->maxrank;
-    double d2[3], d1[3];
-    stencils(p, d, n[0], d2, d1);
+    return PTT_OK;
+}
+
+/* w = T(u . u): formal while r^2 fits, else through a sketch of rank ell. */
+static int product(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int* mr, const int* ell_sketch) {
+    int rc, r[PTT_MAX_DIM + 1], d = ws->d;
     if ((rc = ptt_tt_get_ranks(u, r))) return rc;
     int rmax = 1;
     for (int k = 0; k <= d; k++) rmax = r[k] > rmax ? r[k] : rmax;
-    if (rmax * rmax <= FORMAL_MAX) {
+    if (!ell_sketch && rmax * rmax <= FORMAL_MAX) {
         if ((rc = ptt_hadamard(u, u, ws->w))) return rc;
-        if ((rc = ptt_round(ws->w, p->tol, mr))) return rc;
         ws->hadamard_formal++;
-    } else {
-        int ell[PTT_MAX_DIM + 1];
-        for (int k = 0; k <= d; k++) ell[k] = p->maxrank + p->sketch_pad;
-        if ((rc = ptt_round_hadamard(u, u, ws->w, ell, p->seed, p->tol, mr))) return rc;
-        ws->hadamard_sketch++;
+        return logged(ws, ptt_round(ws->w, p->tol, mr));
     }
+    int ell[PTT_MAX_DIM + 1];
+    for (int k = 0; k <= d; k++) ell[k] = ell_sketch ? ell_sketch[k] : p->maxrank + p->sketch_pad;
+    ws->hadamard_sketch++;
+    return logged(ws, ptt_round_hadamard(u, u, ws->w, ell, p->seed, p->tol, mr));
+}
+
+int ptt_rxn_burgers_F(ptt_tt* u, ptt_tt* F, ptt_rxn_ws* ws, const ptt_rxn_params* p) {
+    int rc, d, n[PTT_MAX_DIM], mr[PTT_MAX_DIM + 1];
+    if (!u || !F || !ws || !p) return PTT_ERR_ARG;
+    if ((rc = shape(u, &d, n))) return rc;
+    for (int k = 0; k <= d; k++) mr[k] = p->maxrank;
+    double d2[3], d1[3];
+    stencils(p, d, n[0], d2, d1);
+    if ((rc = product(u, ws, p, mr, NULL))) return rc;
     if ((rc = ptt_op_sum(u, d2, 3, 1.0, ws->a))) return rc;
-    if ((rc = ptt_round(ws->a, p->tol, mr))) return rc;
+    if ((rc = logged(ws, ptt_round(ws->a, p->tol, mr)))) return rc;
     if ((rc = ptt_op_sum(ws->w, d1, 3, -1.0, ws->b))) return rc;
-    if ((rc = ptt_round(ws->b, p->tol, mr))) return rc;
+    if ((rc = logged(ws, ptt_round(ws->b, p->tol, mr)))) return rc;
     if ((rc = ptt_axpby(1.0, ws->a, 1.0, ws->b, F))) return rc;
-    return ptt_round(F, p->tol, mr);
+    return logged(ws, ptt_round(F, p->tol, mr));
 }
 
 int ptt_rxn_burgers_rk2_step(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p) {
@@ -123,10 +193,82 @@ int ptt_rxn_burgers_rk2_step(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p)
     if (!u || !ws || !p) return PTT_ERR_ARG;
     if ((rc = ptt_tt_shape(u, &d, NULL, NULL))) return rc;
     for (int k = 0; k <= d; k++) mr[k] = p->maxrank;
+    step_begin(ws);
     if ((rc = ptt_rxn_burgers_F(u, ws->k, ws, p))) return rc;
     if ((rc = ptt_axpby(1.0, u, 0.5 * p->dt, ws->k, ws->us))) return rc;
-    if ((rc = ptt_round(ws->us, p->tol, mr))) return rc;
+    if ((rc = logged(ws, ptt_round(ws->us, p->tol, mr)))) return rc;
     if ((rc = ptt_rxn_burgers_F(ws->us, ws->k, ws, p))) return rc;
     if ((rc = ptt_axpby(1.0, u, p->dt, ws->k, u))) return rc;
-    return ptt_round(u, p->tol, mr);
+    return logged(ws, ptt_round(u, p->tol, mr));
+}
+
+/* ------------------------------------------------------------------------ */
+/* sketch step                                                              */
+/* ------------------------------------------------------------------------ */
+
+/* dst <- T(src) by a sketch of ranks ell (src != dst); on rejection
+ * deterministic rounding of src in place and copy.  src must fit the
+ * deterministic kernels (rank <= 128) for the fallback. */
+static int sketch_or_round(ptt_tt* src, ptt_tt* dst, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int* mr,
+                           const int* ell, int pad, unsigned long long salt) {
+    int ok = 0, rc;
+    ws->sketch_calls++;
+    rc = logged(ws, ptt_round_sketch(src, NULL, dst, ell, p->seed ^ salt, p->tol, mr, pad, &ok));
+    if (rc) return rc;
+    if (ok) return PTT_OK;
+    ws->sketch_fallbacks++;
+    if ((rc = logged(ws, ptt_round(src, p->tol, mr)))) return rc;
+    return ptt_tt_copy(dst, src);
+}
+
+static int F_sketch(ptt_tt* u, ptt_tt* F, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int* ell, int pad,
+                    unsigned long long salt) {
+    int rc, d, n[PTT_MAX_DIM], mr[PTT_MAX_DIM + 1];
+    if ((rc = shape(u, &d, n))) return rc;
+    for (int k = 0; k <= d; k++) mr[k] = p->maxrank;
+    double d2[3], d1[3];
+    stencils(p, d, n[0], d2, d1);
+    /* product: sketch of rank ell, with the fixed-rank sketch as fallback */
+    {
+        int ok = 0, r[PTT_MAX_DIM + 1], full[PTT_MAX_DIM + 1];
+        if ((rc = ptt_tt_get_ranks(u, r))) return rc;
+        for (int k = 0; k <= d; k++) full[k] = r[k] * r[k];
+        ws->sketch_calls++;
+        ws->hadamard_sketch++;
+        rc = logged(ws, ptt_round_sketch(u, u, ws->w, ell, p->seed ^ (salt * 7 + 1), p->tol, mr, pad, &ok));
+        if (rc) return rc;
+        if (!ok) {
+            ws->sketch_fallbacks++;
+            if ((rc = product(u, ws, p, mr, NULL))) return rc;
+        }
+        (void)full;
+    }
+    if ((rc = ptt_op_sum(u, d2, 3, 1.0, ws->a))) return rc;
+    if ((rc = ptt_op_sum(ws->w, d1, 3, -1.0, ws->b))) return rc;
+    if ((rc = ptt_axpby(1.0, ws->a, 1.0, ws->b, ws->s))) return rc;
+    int ok = 0;
+    ws->sketch_calls++;
+    rc = logged(ws, ptt_round_sketch(ws->s, NULL, F, ell, p->seed ^ (salt * 7 + 2), p->tol, mr, pad, &ok));
+    if (rc) return rc;
+    if (ok) return PTT_OK;
+    /* fallback: the deterministic composition T(T(a) + T(b)) */
+    ws->sketch_fallbacks++;
+    if ((rc = logged(ws, ptt_round(ws->a, p->tol, mr)))) return rc;
+    if ((rc = logged(ws, ptt_round(ws->b, p->tol, mr)))) return rc;
+    if ((rc = ptt_axpby(1.0, ws->a, 1.0, ws->b, F))) return rc;
+    return logged(ws, ptt_round(F, p->tol, mr));
+}
+
+int ptt_rxn_burgers_rk2_step_sketch(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int* ell, int pad) {
+    int rc, d, mr[PTT_MAX_DIM + 1];
+    if (!u || !ws || !p || !ell) return PTT_ERR_ARG;
+    if ((rc = ptt_tt_shape(u, &d, NULL, NULL))) return rc;
+    for (int k = 0; k <= d; k++) mr[k] = p->maxrank;
+    step_begin(ws);
+    if ((rc = F_sketch(u, ws->k, ws, p, ell, pad, 1))) return rc;
+    if ((rc = ptt_axpby(1.0, u, 0.5 * p->dt, ws->k, ws->t))) return rc;
+    if ((rc = sketch_or_round(ws->t, ws->us, ws, p, mr, ell, pad, 3))) return rc;
+    if ((rc = F_sketch(ws->us, ws->k, ws, p, ell, pad, 4))) return rc;
+    if ((rc = ptt_axpby(1.0, u, p->dt, ws->k, ws->t))) return rc;
+    return sketch_or_round(ws->t, u, ws, p, mr, ell, pad, 5);
 }

@@ -53,6 +53,8 @@ struct ptt_ctx {
     long long tlaunches;
     double* d_work;               // device accumulators of algorithmic work per class [4]
     double hwork[4];              // host-known algorithmic work per class
+    double* d_ones;               // vector of ones (the all-ones rank-1 train)
+    int ones_n;
     void* flush;                  // L2 flush buffer
     size_t flush_bytes;
 };
@@ -97,6 +99,7 @@ int ptt_ws2_reserve(ptt_ctx* ctx, size_t bytes);
 int ptt_pull_desc(ptt_tt* t);
 int ptt_push_desc(ptt_tt* t);
 int ptt_set_ranks_async(ptt_tt* t, int k0, const int* vals, int cnt);
+int ptt_ones(ptt_ctx* c, int n);  // make c->d_ones hold at least n ones
 
 // Swap core[k] <-> alt[k] for k in [k0, k1).
 int ptt_swap(ptt_tt* t, int k0, int k1);

@@ -81,6 +81,7 @@ extern "C" void ptt_ctx_destroy(ptt_ctx* c) {
     cudaStreamSynchronize(c->side);
     cudaFree(c->ws);
     cudaFree(c->ws2);
+    cudaFree(c->d_ones);
     cudaFree(c->d_counters);
     cudaFree(c->d_status);
     cudaFree(c->d_scalars);
@@ -257,6 +258,21 @@ int ptt_set_ranks_async(ptt_tt* t, int k0, const int* vals, int cnt) {
     memcpy(h, vals, sizeof(int) * cnt);
     PTT_CUDA(cudaMemcpyAsync(t->dd->r + k0, h, sizeof(int) * cnt, cudaMemcpyHostToDevice, t->ctx->stream));
     PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
+    return PTT_OK;
+}
+
+__global__ void k_ones(double* p, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 1.0;
+}
+
+int ptt_ones(ptt_ctx* c, int n) {
+    if (n <= c->ones_n) return PTT_OK;
+    PTT_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->d_ones) PTT_CUDA(cudaFree(c->d_ones));
+    PTT_CUDA(cudaMalloc(&c->d_ones, sizeof(double) * (size_t)n));
+    k_ones<<<(n + 255) / 256, 256, 0, c->stream>>>(c->d_ones, n);
+    PTT_LAUNCHED(c);
+    c->ones_n = n;
     return PTT_OK;
 }
 

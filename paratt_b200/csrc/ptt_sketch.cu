@@ -162,20 +162,27 @@ static int blocks_for(long long cnt) {
 
 }  // namespace
 
-extern "C" int ptt_round_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* ell, unsigned long long seed,
-                                  double tol, const int* maxrank) {
-    if (!x || !y || !z || x->d != y->d || x->d != z->d)
-        return ptt_set_error(PTT_ERR_ARG, "ptt_round_hadamard: shape mismatch");
-    if (z == x || z == y) return ptt_set_error(PTT_ERR_ARG, "ptt_round_hadamard: output aliases an input");
+// Sketch-round x (.) y (y == NULL: the all-ones rank-1 train, i.e. x
+// itself).  On return used[k] holds the sketch rank of bond k.
+static int sketch_round(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* ell, unsigned long long seed,
+                        double tol, const int* maxrank, int* used) {
+    if (!x || !z || x->d != z->d || (y && y->d != x->d))
+        return ptt_set_error(PTT_ERR_ARG, "sketch rounding: shape mismatch");
+    if (z == x || z == y) return ptt_set_error(PTT_ERR_ARG, "sketch rounding: output aliases an input");
     const int d = x->d;
     for (int k = 0; k < d; k++)
-        if (x->n[k] != y->n[k] || x->n[k] != z->n[k])
-            return ptt_set_error(PTT_ERR_ARG, "ptt_round_hadamard: mode %d differs", k);
+        if ((y && x->n[k] != y->n[k]) || x->n[k] != z->n[k])
+            return ptt_set_error(PTT_ERR_ARG, "sketch rounding: mode %d differs", k);
     ptt_ctx* c = z->ctx;
     int rc;
     int rx[PTT_MAX_DIM + 1], ry[PTT_MAX_DIM + 1], L[PTT_MAX_DIM + 1];
     long long R[PTT_MAX_DIM + 1];
-    if ((rc = ptt_tt_get_ranks((ptt_tt*)x, rx)) || (rc = ptt_tt_get_ranks((ptt_tt*)y, ry))) return rc;
+    if ((rc = ptt_tt_get_ranks((ptt_tt*)x, rx))) return rc;
+    if (y) {
+        if ((rc = ptt_tt_get_ranks((ptt_tt*)y, ry))) return rc;
+    } else {
+        for (int k = 0; k <= d; k++) ry[k] = 1;
+    }
     const int* n = x->n;
     for (int k = 0; k <= d; k++) R[k] = (long long)rx[k] * ry[k];
     L[0] = L[d] = 1;
@@ -215,10 +222,21 @@ extern "C" int ptt_round_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, c
     const long long total = oM1 + szM + 64;
     if ((rc = ptt_ws2_reserve(c, (size_t)total * sizeof(double)))) return rc;
     double* ws = (double*)c->ws2;
-    // input core pointers
-    if ((rc = ptt_pull_desc((ptt_tt*)x)) || (rc = ptt_pull_desc((ptt_tt*)y))) return rc;
+    // input core pointers (the ones train points every core at one ones vector)
+    if ((rc = ptt_pull_desc((ptt_tt*)x))) return rc;
     const double* const* xc = x->hd.core;
-    const double* const* yc = y->hd.core;
+    const double* yones[PTT_MAX_DIM];
+    const double* const* yc;
+    if (y) {
+        if ((rc = ptt_pull_desc((ptt_tt*)y))) return rc;
+        yc = y->hd.core;
+    } else {
+        int nmax = 1;
+        for (int k = 0; k < d; k++) nmax = n[k] > nmax ? n[k] : nmax;
+        if ((rc = ptt_ones(c, nmax))) return rc;
+        for (int k = 0; k < d; k++) yones[k] = c->d_ones;
+        yc = yones;
+    }
 
     for (int k = 1; k < d; k++) {
         const long long cnt = (long long)L[k] * n[k] * L[k + 1];
@@ -310,5 +328,46 @@ extern "C" int ptt_round_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, c
         r = q;
     }
     if ((rc = ptt_set_ranks_async(z, 0, zr, d + 1))) return rc;
+    if (used)
+        for (int k = 0; k <= d; k++) used[k] = L[k];
     return ptt_round_phases(z, tol, maxrank, 2, 0);
+}
+
+extern "C" int ptt_round_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* ell, unsigned long long seed,
+                                  double tol, const int* maxrank) {
+    if (!y) return ptt_set_error(PTT_ERR_ARG, "ptt_round_hadamard: null factor");
+    return sketch_round(x, y, z, ell, seed, tol, maxrank, NULL);
+}
+
+// Accept the sketch when every bond kept at most used[k] - pad ranks after
+// the deterministic truncation, or when the sketch spanned the full bond
+// rank (then nothing was lost).  Randomized range finding with oversampling
+// p loses ~sigma_{l-p+1}; a truncation that stops p below l shows that
+// sigma_{l-p+1} already lies in the dropped tail, below the threshold.
+static int check_sketch(ptt_tt* z, const int* used, const int* full, int pad, int* accepted) {
+    int r[PTT_MAX_DIM + 1];
+    int rc = ptt_tt_get_ranks(z, r);
+    if (rc) return rc;
+    int ok = 1;
+    for (int k = 1; k < z->d; k++)
+        if (used[k] < full[k] && r[k] > used[k] - pad) ok = 0;
+    *accepted = ok;
+    return PTT_OK;
+}
+
+extern "C" int ptt_round_sketch(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* ell, unsigned long long seed,
+                                double tol, const int* maxrank, int pad, int* accepted) {
+    int used[PTT_MAX_DIM + 1], rx[PTT_MAX_DIM + 1], ry[PTT_MAX_DIM + 1], full[PTT_MAX_DIM + 1];
+    if (!x || !z) return ptt_set_error(PTT_ERR_ARG, "ptt_round_sketch: null tensor");
+    int rc = ptt_tt_get_ranks((ptt_tt*)x, rx);
+    if (rc) return rc;
+    if (y) {
+        if ((rc = ptt_tt_get_ranks((ptt_tt*)y, ry))) return rc;
+    } else {
+        for (int k = 0; k <= x->d; k++) ry[k] = 1;
+    }
+    for (int k = 0; k <= x->d; k++) full[k] = rx[k] * ry[k];
+    if ((rc = sketch_round(x, y, z, ell, seed, tol, maxrank, used))) return rc;
+    if (accepted) return check_sketch(z, used, full, pad, accepted);
+    return PTT_OK;
 }

@@ -1,0 +1,111 @@
+"""Learned sketch ranks for the reaction-Burgers sketch step.
+
+Features of bond k (k = 1..d-1) at step t: the top-16 singular values of that
+bond after the last rounding of step t-1, as log10(sigma_j / delta) clipped
+to [-4, 16] and scaled by 1/4 (delta = the bond's truncation threshold, so
+the count of values above 0 is the deterministic rank when it is <= 16), the
+bond position k/d, and log10(dt) + 3.  Target: the largest rank bond k keeps
+in any rounding of step t (logged from plain, deterministic runs).  The
+proposal is ell_k = ceil(prediction) + pad, clamped to [pad + 1, maxrank + pad].
+
+Training data comes from plain runs of the config-2 shape (d=40, n=128,
+rank cap 32, tol 1e-8) at several seeds; training and inference run on the
+GPU through the MLP kernels (ptt_mlp_*).
+
+    python -m paratt_b200.learned --out paratt_b200/models/sketch_rank_mlp.npz
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import time
+
+import numpy as np
+
+from . import STAT_NSIG, MLP, Context, RxnBurgers, TT
+from . import workloads as W
+
+NIN = STAT_NSIG + 2
+MODEL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "models", "sketch_rank_mlp.npz")
+
+
+def features(sig, delta, d, dt):
+    """sig: (d+1, 16) bond spectra (row k = bond k); returns (d-1, NIN)."""
+    s = np.maximum(np.asarray(sig[1:d], dtype=np.float64), 1e-300)
+    lg = np.clip(np.log10(s / max(delta, 1e-300)), -4.0, 16.0) / 4.0
+    k = (np.arange(1, d) / d)[:, None]
+    t = np.full((d - 1, 1), np.log10(dt) + 3.0)
+    return np.hstack([lg, k, t]).astype(np.float32)
+
+
+def propose(mlp, sig, delta, d, dt, pad, maxrank):
+    y = mlp.forward(features(sig, delta, d, dt))
+    ell = np.clip(np.ceil(y).astype(int) + pad, pad + 1, maxrank + pad)
+    return [1] + [int(v) for v in ell] + [1]
+
+
+def collect(ctx, cfg, seed, steps, warm=1):
+    """Plain run with logging; returns features (previous step's spectra)
+    and targets (this step's largest kept rank) for every bond and step."""
+    d, n = cfg["d"], cfg["n"]
+    u0 = W.initial_condition(d, n, cfg["ngauss"], seed)
+    tol = cfg["tol"] * W.rms_norm(u0)
+    sim = RxnBurgers(ctx, d, n, maxrank=cfg["maxrank"], dt=cfg["dt"], tol=tol, seed=seed)
+    sim.log(True)
+    U = TT(ctx, [n] * d, [1] + [2 * cfg["maxrank"]] * (d - 1) + [1], u0)
+    X, T = [], []
+    prev = None
+    for s in range(steps):
+        sim.step(U)
+        ranks, sig, delta = sim.last_step(d)
+        if prev is not None and s >= warm:
+            X.append(features(prev[0], prev[1], d, cfg["dt"]))
+            T.append(np.asarray(ranks[1:d], dtype=np.float32))
+        prev = (sig.copy(), delta)
+    sim.close()
+    U.close()
+    return np.vstack(X), np.concatenate(T)
+
+
+def train(mlp, X, T, epochs=300, lr=3e-3, batch=512, seed=0):
+    rng = np.random.default_rng(seed)
+    losses = []
+    for ep in range(epochs):
+        idx = rng.permutation(len(T))
+        for b in range(0, len(T), batch):
+            j = idx[b:b + batch]
+            losses.append(mlp.train_step(X[j], T[j], lr))
+    return losses
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=MODEL)
+    ap.add_argument("--seeds", type=int, nargs="*", default=[10, 11, 12, 13])
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--epochs", type=int, default=300)
+    args = ap.parse_args()
+    ctx = Context(0)
+    cfg = dict(W.CONFIGS["c2"])
+    t0 = time.time()
+    Xs, Ts = [], []
+    for sd in args.seeds:
+        X, T = collect(ctx, cfg, sd, args.steps)
+        Xs.append(X)
+        Ts.append(T)
+        print(f"seed {sd}: {len(T)} samples, target ranks {T.min():.0f}..{T.max():.0f}", flush=True)
+    X, T = np.vstack(Xs), np.concatenate(Ts)
+    mlp = MLP(ctx, NIN, 64, seed=1)
+    losses = train(mlp, X, T, epochs=args.epochs)
+    pred = mlp.forward(X)
+    under = float(np.mean(np.ceil(pred) < T))
+    print(f"{len(T)} samples, final loss {losses[-1]:.4f}, under-predicted {100 * under:.1f}%, "
+          f"{time.time() - t0:.0f} s", flush=True)
+    os.makedirs(os.path.dirname(args.out), exist_ok=True)
+    np.savez(args.out, params=mlp.params(), nin=NIN, width=64, X=X, T=T)
+    mlp.close()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()
