@@ -119,6 +119,11 @@ PTT_API int ptt_round_stats(ptt_ctx* ctx, int d, double* out);
 PTT_API int ptt_axpby(double a, const ptt_tt* x, double b, const ptt_tt* y, ptt_tt* z);
 /* z = x (.) y in formal form (attacHadamard, attac.c:128-136). */
 PTT_API int ptt_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z);
+/* z = x (.) x as an exact TT of ranks r_k (r_k + 1) / 2 instead of r_k^2:
+ * the formal product restricted to the symmetric subspace of R^r (x) R^r.
+ * No counterpart in the reference (which forms the rank r^2 product); the
+ * tensor is the same, so its rounding matches to rounding error. */
+PTT_API int ptt_square_sym(const ptt_tt* x, ptt_tt* z);
 PTT_API int ptt_scale(double a, ptt_tt* x);                          /* paratt.c:271 */
 PTT_API int ptt_mult_diag(ptt_tt* x, int mode, const double* vec);   /* paratt.c:571 */
 /* Centred periodic stencil along one mode (paratt.c:584-661); an even slen

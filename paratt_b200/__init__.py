@@ -64,6 +64,7 @@ _SIGS = {
     "ptt_round_stats": (_i, [_p, _i, _dp]),
     "ptt_axpby": (_i, [_d, _p, _d, _p, _p]),
     "ptt_hadamard": (_i, [_p, _p, _p]),
+    "ptt_square_sym": (_i, [_p, _p]),
     "ptt_scale": (_i, [_d, _p]),
     "ptt_mult_diag": (_i, [_p, _i, _dp]),
     "ptt_stencil": (_i, [_p, _i, _dp, _i]),
@@ -298,6 +299,12 @@ def axpby(a, x: TT, b, y: TT, z: TT):
 
 def hadamard(x: TT, y: TT, z: TT):
     _check(lib().ptt_hadamard(x.h, y.h, z.h))
+    return z
+
+
+def square_sym(x: TT, z: TT):
+    """z = x (.) x at ranks r (r + 1) / 2 (same tensor as hadamard(x, x))."""
+    _check(lib().ptt_square_sym(x.h, z.h))
     return z
 
 

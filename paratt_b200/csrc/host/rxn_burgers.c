@@ -18,9 +18,11 @@
  *   u_s = T(u + dt/2 F(u)),  u+ = T(u + dt F(u_s))
  *
  * T = paratt_truncate semantics with an absolute tolerance.  The product
- * u . u is formed formally (attacHadamard) while r_u^2 fits the rounding
- * kernels (<= 128) and is otherwise rounded through a Gaussian TT sketch of
- * rank min(r_u^2, maxrank + sketch_pad) without forming it.
+ * u . u is formed exactly at rank r_u (r_u + 1) / 2 (ptt_square_sym: the
+ * same tensor as the reference's rank r_u^2 attacHadamard, restricted to
+ * its symmetric subspace) while that fits the rounding kernels (<= 128),
+ * and is otherwise rounded through a Gaussian TT sketch of rank
+ * min(r_u^2, maxrank + sketch_pad) without forming it.
  *
  * Sketch step (ptt_rxn_burgers_rk2_step_sketch): the same step with every
  * rounding done by a Gaussian TT sketch of per-bond ranks ell[k] followed by
@@ -155,14 +157,14 @@ static int shape(ptt_tt* u, int* d, int* n) {
     return PTT_OK;
 }
 
-/* w = T(u . u): formal while r^2 fits, else through a sketch of rank ell. */
+/* w = T(u . u): exact symmetric square while r(r+1)/2 fits, else through a sketch of rank ell. */
 static int product(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int* mr, const int* ell_sketch) {
     int rc, r[PTT_MAX_DIM + 1], d = ws->d;
     if ((rc = ptt_tt_get_ranks(u, r))) return rc;
     int rmax = 1;
     for (int k = 0; k <= d; k++) rmax = r[k] > rmax ? r[k] : rmax;
-    if (!ell_sketch && rmax * rmax <= FORMAL_MAX) {
-        if ((rc = ptt_hadamard(u, u, ws->w))) return rc;
+    if (!ell_sketch && rmax * (rmax + 1) / 2 <= FORMAL_MAX) {
+        if ((rc = ptt_square_sym(u, ws->w))) return rc;
         ws->hadamard_formal++;
         return logged(ws, ptt_round(ws->w, p->tol, mr));
     }

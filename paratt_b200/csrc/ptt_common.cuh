@@ -39,6 +39,8 @@ struct ptt_ctx {
     size_t ws_bytes;
     void* ws2;                    // second workspace (sketch contractions)
     size_t ws2_bytes;
+    void* ws3;                    // split-K partial products of the batched GEMMs
+    size_t ws3_bytes;
     int* d_counters;              // zeroed, self-resetting tree counters
     size_t counters_n;
     double* d_scalars;            // small scratch for reductions
@@ -97,6 +99,7 @@ int ptt_ws_reserve(ptt_ctx* ctx, size_t bytes);
 int ptt_counters_reserve(ptt_ctx* ctx, size_t n);
 int ptt_ws2_reserve(ptt_ctx* ctx, size_t bytes);
 int ptt_pull_desc(ptt_tt* t);
+int ptt_ws3_reserve(ptt_ctx* c, size_t bytes);
 int ptt_push_desc(ptt_tt* t);
 int ptt_set_ranks_async(ptt_tt* t, int k0, const int* vals, int cnt);
 int ptt_ones(ptt_ctx* c, int n);  // make c->d_ones hold at least n ones
@@ -107,6 +110,7 @@ int ptt_swap(ptt_tt* t, int k0, int k1);
 // Rounding stages (ptt_round.cu): phases 1 = orthogonalise, 2 = truncate
 // (input left-orthogonal), 4 = QR of core `only` alone.
 int ptt_round_phases(ptt_tt* x, double tol, const int* maxrank, int phases, int only);
+int ptt_round_phases_rk(ptt_tt* x, const int* rk, double tol, const int* maxrank, int phases, int only);
 double ptt_round_threshold(const ptt_tt* x, double tol);
 
 // Round a size up to a multiple of 256 bytes.

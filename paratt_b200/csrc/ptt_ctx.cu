@@ -81,6 +81,7 @@ extern "C" void ptt_ctx_destroy(ptt_ctx* c) {
     cudaStreamSynchronize(c->side);
     cudaFree(c->ws);
     cudaFree(c->ws2);
+    cudaFree(c->ws3);
     cudaFree(c->d_ones);
     cudaFree(c->d_counters);
     cudaFree(c->d_status);
@@ -238,6 +239,19 @@ int ptt_ws_reserve(ptt_ctx* c, size_t bytes) {
     return PTT_OK;
 }
 
+int ptt_ws3_reserve(ptt_ctx* c, size_t bytes) {
+    if (bytes <= c->ws3_bytes) return PTT_OK;
+    PTT_CUDA(cudaStreamSynchronize(c->stream));
+    PTT_CUDA(cudaStreamSynchronize(c->side));
+    if (c->ws3) PTT_CUDA(cudaFree(c->ws3));
+    c->ws3 = NULL;
+    c->ws3_bytes = 0;
+    size_t b = ptt_align(bytes + bytes / 4);
+    PTT_CUDA(cudaMalloc(&c->ws3, b));
+    c->ws3_bytes = b;
+    return PTT_OK;
+}
+
 int ptt_ws2_reserve(ptt_ctx* c, size_t bytes) {
     if (bytes <= c->ws2_bytes) return PTT_OK;
     PTT_CUDA(cudaStreamSynchronize(c->stream));
@@ -252,12 +266,22 @@ int ptt_ws2_reserve(ptt_ctx* c, size_t bytes) {
 }
 
 // Write ranks r[k0 .. k0+cnt) of the device descriptor (stream-ordered).
+// The values travel as a kernel argument, so the call neither stages through
+// host memory nor waits for the stream.
+struct RankVals {
+    int v[PTT_MAX_DIM + 1];
+};
+
+__global__ void k_set_ranks(DevDesc* D, int k0, int cnt, RankVals rv) {
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) D->r[k0 + i] = rv.v[i];
+}
+
 int ptt_set_ranks_async(ptt_tt* t, int k0, const int* vals, int cnt) {
-    int* h = (int*)(t->ctx->h_scalars + 256);  // pinned staging (second half)
-    cudaStreamSynchronize(t->ctx->stream);
-    memcpy(h, vals, sizeof(int) * cnt);
-    PTT_CUDA(cudaMemcpyAsync(t->dd->r + k0, h, sizeof(int) * cnt, cudaMemcpyHostToDevice, t->ctx->stream));
-    PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
+    if (k0 < 0 || cnt < 0 || k0 + cnt > t->d + 1) return ptt_set_error(PTT_ERR_ARG, "rank range");
+    RankVals rv;
+    memcpy(rv.v, vals, sizeof(int) * cnt);
+    k_set_ranks<<<1, 128, 0, t->ctx->stream>>>(t->dd, k0, cnt, rv);
+    PTT_LAUNCHED(t->ctx);
     return PTT_OK;
 }
 

@@ -2,6 +2,7 @@
 //
 //  axpby     attacFormalAXPBY   attac.c:81-112, wrapper paratt.c:237-268
 //  hadamard  attacHadamard      attac.c:128-136 with attacKron utilities.c:112-129
+//  square_sym  x (.) x at rank r(r+1)/2 (no reference counterpart; same tensor)
 //  scale     attac_tt_scale     paratt.c:271-281
 //  diag      attac_mult_diag_mat paratt.c:571-581
 //  stencil   attac_apply_periodic_stencil paratt.c:584-661
@@ -116,7 +117,7 @@ __global__ void k_axpby(const DevDesc* X, const DevDesc* Y, DevDesc* Z, double a
 // inputs' capacities; when z already covers it nothing happens (no sync).
 // Otherwise the inputs' actual ranks are read back (synchronises) and z is
 // grown only to the exact output ranks: op 0 = sum (r_x + r_y), 1 = product,
-// 2 = operator sum (2 r_x; y unused).
+// 2 = operator sum (2 r_x; y unused), 3 = symmetric square (r_x (r_x + 1) / 2).
 static int fit_output(ptt_tt* z, const int* need, const ptt_tt* x, const ptt_tt* y, int op) {
     const int d = z->d;
     int ok = 1;
@@ -125,12 +126,14 @@ static int fit_output(ptt_tt* z, const int* need, const ptt_tt* x, const ptt_tt*
     int rx[PTT_MAX_DIM + 1], ry[PTT_MAX_DIM + 1], ex[PTT_MAX_DIM + 1];
     int rc;
     if ((rc = ptt_tt_get_ranks((ptt_tt*)x, rx))) return rc;
-    if (op != 2 && (rc = ptt_tt_get_ranks((ptt_tt*)y, ry))) return rc;
+    if (op < 2 && (rc = ptt_tt_get_ranks((ptt_tt*)y, ry))) return rc;
     for (int k = 0; k <= d; k++) {
         if (op == 0)
             ex[k] = (k == 0 || k == d) ? 1 : rx[k] + ry[k];
         else if (op == 1)
             ex[k] = rx[k] * ry[k];
+        else if (op == 3)
+            ex[k] = rx[k] * (rx[k] + 1) / 2;
         else
             ex[k] = (k == 0 || k == d) ? 1 : 2 * rx[k];
         if (ex[k] < z->rcap[k]) ex[k] = z->rcap[k];
@@ -210,6 +213,77 @@ extern "C" int ptt_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z) {
     long long mx = 0;
     for (int k = 0; k < d; k++) mx = z->cap[k] > mx ? z->cap[k] : mx;
     k_hadamard<<<dim3(elem_blocks(mx), d), 256, 0, c->stream>>>(x->dd, y->dd, z->dd, newr, c->d_status);
+    PTT_LAUNCHED(c);
+    return finalize(z, newr, 0, d, 1);
+}
+
+// ---------------------------------------------------------------------------
+// symmetric square: x (.) x restricted to the symmetric subspace.
+// The formal core x_k (x) x_k (per mode index j) maps Sym^2(R^r) into
+// Sym^2(R^r') and both interface vectors of x (.) x are symmetric, so with
+// the orthonormal basis e_(a,a) and (e_(a,b) + e_(b,a))/sqrt2 (a < b) of
+// Sym^2 the compressed core
+//   z[s, j, s'] = (x[a,j,a'] x[b,j,b'] + x[a,j,b'] x[b,j,a']) f(s) f(s'),
+//   f(s) = 1/sqrt2 if a == b else 1,
+// gives exactly the same tensor at rank r (r + 1) / 2 instead of r^2.
+// Pairs are packed s = b (b + 1) / 2 + a, a <= b.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void sym_pair(int s, int* a, int* b) {
+    int bb = (int)((sqrt(8.0 * s + 1.0) - 1.0) * 0.5);
+    while ((bb + 1) * (bb + 2) / 2 <= s) bb++;
+    while (bb * (bb + 1) / 2 > s) bb--;
+    *b = bb;
+    *a = s - bb * (bb + 1) / 2;
+}
+
+__global__ void k_square_sym(const DevDesc* X, DevDesc* Z, int* newr, int* status) {
+    const int k = blockIdx.y;
+    const int d = X->d;
+    const int rx = X->r[k], rx1 = X->r[k + 1];
+    const int n = X->n[k];
+    const int rz = rx * (rx + 1) / 2, rz1 = rx1 * (rx1 + 1) / 2;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        newr[k] = rz;
+        if (k == d - 1) newr[d] = rz1;
+    }
+    const long long cnt = (long long)rz * n * rz1;
+    if (rz > Z->rcap[k] || rz1 > Z->rcap[k + 1] || cnt > Z->cap[k]) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) PTT_STATUS_SET(status, PTT_ERR_CAPACITY);
+        return;
+    }
+    const double* xc = X->core[k];
+    double* zc = Z->alt[k];
+    const long long rzn = (long long)rz * n;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const double h = 0.70710678118654752440;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += stride) {
+        const int sz1 = (int)(e / rzn);
+        const long long rem = e - sz1 * rzn;
+        const int j = (int)(rem / rz);
+        const int sz = (int)(rem - (long long)j * rz);
+        int a, b, a1, b1;
+        sym_pair(sz, &a, &b);
+        sym_pair(sz1, &a1, &b1);
+        const double* xj = xc + (long long)rx * j;
+        const long long ls = (long long)rx * n;
+        const double v = xj[a + ls * a1] * xj[b + ls * b1] + xj[a + ls * b1] * xj[b + ls * a1];
+        zc[e] = v * (a == b ? h : 1.0) * (a1 == b1 ? h : 1.0);
+    }
+}
+
+extern "C" int ptt_square_sym(const ptt_tt* x, ptt_tt* z) {
+    int rc = check_same_modes(x, z);
+    if (rc) return rc;
+    const int d = x->d;
+    int need[PTT_MAX_DIM + 1];
+    for (int k = 0; k <= d; k++) need[k] = x->rcap[k] * (x->rcap[k] + 1) / 2;
+    if ((rc = fit_output(z, need, x, x, 3))) return rc;
+    ptt_ctx* c = z->ctx;
+    int* newr = ranks_scratch(c, d);
+    if (!newr) return ptt_set_error(PTT_ERR_ARG, "d too large");
+    long long mx = 0;
+    for (int k = 0; k < d; k++) mx = z->cap[k] > mx ? z->cap[k] : mx;
+    k_square_sym<<<dim3(elem_blocks(mx), d), 256, 0, c->stream>>>(x->dd, z->dd, newr, c->d_status);
     PTT_LAUNCHED(c);
     return finalize(z, newr, 0, d, 1);
 }

@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(SVD_NT) k_svd_jacobi(Plan pl, double* ws, doub
 // Rebuild rows of V (q x q, V = product of the recorded rotations) and write
 // V_r = V[:, order[0:rank]] into Bn[root].  One warp per row; each sweep's
 // rotation table is staged in shared memory once per block.
-__global__ void __launch_bounds__(256) k_svd_replay(Plan pl, double* ws) {
+__device__ void svd_replay_body(const Plan& pl, double* ws, const Info* info, int bx) {
     extern __shared__ double sm[];
     const int CT = pl.CT, KC = pl.KC;
     const int SR = CT + 2;
@@ -425,8 +425,7 @@ __global__ void __launch_bounds__(256) k_svd_replay(Plan pl, double* ws) {
     double* vrow = sm + (threadIdx.x >> 5) * SR;   // 8 rows
     double2* tab = (double2*)(sm + 8 * SR);         // (CT+1) rounds x npair
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int row = blockIdx.x * 8 + warp;
-    const Info* info = pl.info;
+    const int row = bx * 8 + warp;
     if (info->status) return;
     const int q = info->q, qq = q + (q & 1), sweeps = info->sweeps, rank = info->rank;
     for (int j = lane; j < SR; j += 32) vrow[j] = (j == row) ? 1.0 : 0.0;
@@ -457,6 +456,16 @@ __global__ void __launch_bounds__(256) k_svd_replay(Plan pl, double* ws) {
     const int* ord = (const int*)(ws + pl.o_sig + CT);
     double* B = ws + pl.o_Bn + (long long)row * KC;
     for (int b = lane; b < KC; b += 32) B[b] = (row < q && b < rank) ? vrow[ord[b]] : 0.0;
+}
+
+__global__ void __launch_bounds__(256) k_svd_replay(Plan pl, double* ws) {
+    svd_replay_body(pl, ws, pl.info, blockIdx.x);
+}
+
+// the same for bonds k0 .. k0 + gridDim.y - 1, bond k's records at ws + k * stride
+__global__ void __launch_bounds__(256) k_svd_replay_b(Plan pl, double* ws, long long stride, int k0) {
+    double* wsb = ws + (long long)(k0 + blockIdx.y) * stride;
+    svd_replay_body(pl, wsb, (const Info*)(wsb + pl.o_info_d), blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -779,6 +788,151 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
     return PTT_OK;
 }
 
+#include "ptt_wtsqr.cuh"
+
+// Rounding of a train whose ranks stay <= 32 on the warp-level TSQR.
+// Per bond only the factorisation, the small product that moves R (or U S)
+// into the neighbour core and the rank update run in sequence; Q (and V_r Q)
+// is formed for all bonds of a sweep in one launch after the sweep; the
+// one-warp SVD accumulates V itself.
+// Every bond k has its own record region (ws + k * stride) so the deferred
+// launches find each bond's reflectors.  Same phases as round_impl.
+static bool wt_fits(const ptt_tt* x, const int* rk) {
+    for (int i = 0; i < x->d; i++) {
+        const long long ml = (long long)rk[i] * x->n[i], mr = (long long)x->n[i] * rk[i + 1];
+        const long long mx = ml > mr ? ml : mr;
+        if (mx > 32LL * wt::PMAX) return false;
+    }
+    return true;
+}
+
+static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr, int phases, int only) {
+    using namespace wt;
+    ptt_ctx* c = x->ctx;
+    const int d = x->d;
+    int rc = set_attrs<32>();
+    if (rc) return rc;
+    static bool wattr = false;
+    if (!wattr) {
+        PTT_CUDA(cudaFuncSetAttribute(k_wfactor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wfactor_smem()));
+        wattr = true;
+    }
+    int Wl[PTT_MAX_DIM], Wr[PTT_MAX_DIM], Pcap = 1;
+    for (int i = 0; i < d; i++) {
+        const long long ml = (long long)rk[i] * x->n[i], mr = (long long)x->n[i] * rk[i + 1];
+        Wl[i] = (int)((ml + 31) / 32);
+        Wr[i] = (int)((mr + 31) / 32);
+        const int pw = pow2_ge(Wl[i] > Wr[i] ? Wl[i] : Wr[i]);
+        if (pw > Pcap) Pcap = pw;
+    }
+    Plan base;
+    plan_bond(32, 1, 32, &base);
+    base.NH = 1;
+    long long o = carve(&base, 1, 1);
+    WP wp;
+    wp.o_R = o;
+    o += (2LL * Pcap - 1) * SLOT;
+    wp.o_tl = o;
+    o += (long long)Pcap * 32;
+    wp.o_tn = o;
+    o += (long long)Pcap * 32;
+    wp.stride = (o + 31) / 32 * 32;
+    wp.Pcap = Pcap;
+    base.o_Rn = wp.o_R;  // root R = slot 0 (read by the SVD and the R product)
+    if ((rc = ptt_ws_reserve(c, (size_t)wp.stride * d * sizeof(double) + 256))) return rc;
+    if ((rc = ptt_counters_reserve(c, (size_t)Pcap * d + 64))) return rc;
+    double* ws = (double*)c->ws;
+    wp.cnt = c->d_counters;
+    base.cnt = c->d_counters;
+    base.qn = nullptr;
+    base.pass = nullptr;
+    base.stats = c->d_stats;
+    base.work = (c->tkind == PTT_TIME_TSQR) ? c->d_work + PTT_TIME_TSQR : nullptr;
+    auto bond = [&](int i, double** wsb) {
+        Plan pl = base;
+        *wsb = ws + (long long)i * wp.stride;
+        pl.info = (Info*)(*wsb + base.o_info_d);
+        return pl;
+    };
+    auto factor = [&](int i, int mode, int W, const Plan& pl, double* wsb) -> int {
+        ptt_time_begin(c, PTT_TIME_TSQR);
+        k_wfactor<<<(W + FPB - 1) / FPB, 32 * FPB, wfactor_smem(), c->stream>>>(x->dd, i, mode, pl, wp, wsb,
+                                                                                c->d_status);
+        ptt_time_end(c, PTT_TIME_TSQR);
+        PTT_LAUNCHED(c);
+        return PTT_OK;
+    };
+    if (phases & 4) {
+        const int i = only;
+        double* wsb;
+        Plan pl = bond(i, &wsb);
+        if ((rc = factor(i, LEFT, Wl[i], pl, wsb))) return rc;
+        k_wapply<<<dim3((Wl[i] + WPB - 1) / WPB, 1), 32 * WPB, 0, c->stream>>>(x->dd, i, LEFT, base, wp, ws);
+        PTT_LAUNCHED(c);
+        k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i, -1, &pl.info->q, pl.info);
+        PTT_LAUNCHED(c);
+        return PTT_OK;
+    }
+    if (phases & 1) {
+        int Wmax = 1;
+        for (int i = 0; i < d - 1; i++) {
+            double* wsb;
+            Plan pl = bond(i, &wsb);
+            if ((rc = factor(i, LEFT, Wl[i], pl, wsb))) return rc;
+            Wmax = Wl[i] > Wmax ? Wl[i] : Wmax;
+            const long long ncap = (long long)x->n[i + 1] * rk[i + 2];
+            int gy = (int)((ncap + GT - 1) / GT);
+            if (gy > 4096) gy = 4096;
+            k_gemm_rx<<<dim3(1, gy), 256, 0, c->stream>>>(x->dd, i + 1, pl, wsb);
+            PTT_LAUNCHED(c);
+            k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i + 1, -1, &pl.info->q, pl.info);
+            PTT_LAUNCHED(c);
+        }
+        if (d > 1) {
+            k_wapply<<<dim3((Wmax + WPB - 1) / WPB, d - 1), 32 * WPB, 0, c->stream>>>(x->dd, 0, LEFT, base, wp, ws);
+            PTT_LAUNCHED(c);
+            k_wswap<<<1, 64, 0, c->stream>>>(x->dd, 0, d - 1, c->d_status);
+            PTT_LAUNCHED(c);
+        }
+    }
+    if (phases & 2) {
+        int Wmax = 1;
+        for (int i = d - 1; i >= 1; i--) {
+            double* wsb;
+            Plan pl = bond(i, &wsb);
+            if ((rc = factor(i, RIGHT_T, Wr[i], pl, wsb))) return rc;
+            Wmax = Wr[i] > Wmax ? Wr[i] : Wmax;
+            const int mr = maxr ? maxr[i] : rk[i];
+            ptt_time_begin(c, PTT_TIME_SVD);
+#ifdef WT_WSVD
+            k_wsvd<<<1, 32, 0, c->stream>>>(pl, wsb, delta, mr, i, c->d_status);
+#else
+            k_svd_jacobi<32><<<1, SVD_NT, svd_smem<32>(), c->stream>>>(pl, wsb, delta, mr, i, c->d_status);
+#endif
+            ptt_time_end(c, PTT_TIME_SVD);
+            PTT_LAUNCHED(c);
+            const long long mcap = (long long)rk[i - 1] * x->n[i - 1];
+            int gx = (int)((mcap + GT - 1) / GT);
+            if (gx > 4096) gx = 4096;
+            k_gemm_xm<<<dim3(gx, 1), 256, 0, c->stream>>>(x->dd, i - 1, pl, wsb);
+            PTT_LAUNCHED(c);
+            k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i, i - 1, -1, &pl.info->rank, pl.info);
+            PTT_LAUNCHED(c);
+        }
+        if (d > 1) {
+#ifndef WT_WSVD
+            k_svd_replay_b<<<dim3(4, d - 1), 256, replay_smem<32>(), c->stream>>>(base, ws, wp.stride, 1);
+            PTT_LAUNCHED(c);
+#endif
+            k_wapply<<<dim3((Wmax + WPB - 1) / WPB, d - 1), 32 * WPB, 0, c->stream>>>(x->dd, 1, RIGHT_T, base, wp, ws);
+            PTT_LAUNCHED(c);
+            k_wswap<<<1, 64, 0, c->stream>>>(x->dd, 1, d, c->d_status);
+            PTT_LAUNCHED(c);
+        }
+    }
+    return PTT_OK;
+}
+
 }  // namespace
 
 // Per-bond threshold of the reference applied to the unnormalised tensor.
@@ -800,7 +954,6 @@ extern "C" int ptt_round_stats(ptt_ctx* c, int d, double* out) {
 int ptt_round_phases(ptt_tt* x, double tol, const int* maxrank, int phases, int only) {
     if (!x) return ptt_set_error(PTT_ERR_ARG, "ptt_round: null tt");
     if (x->d < 2) return PTT_OK;
-    if (!(tol >= 0.0)) return ptt_set_error(PTT_ERR_ARG, "ptt_round: tol must be >= 0");
     int rk[PTT_MAX_DIM + 1];
     cudaSetDevice(x->ctx->device);
     if (x->ctx->fixed_plans) {
@@ -812,9 +965,20 @@ int ptt_round_phases(ptt_tt* x, double tol, const int* maxrank, int phases, int 
         int rc = ptt_tt_get_ranks(x, rk);
         if (rc) return rc;
     }
+    return ptt_round_phases_rk(x, rk, tol, maxrank, phases, only);
+}
+
+// The same with upper bounds rk[0..d] of the ranks known to the caller (no
+// read-back).
+int ptt_round_phases_rk(ptt_tt* x, const int* rk, double tol, const int* maxrank, int phases, int only) {
+    if (!x) return ptt_set_error(PTT_ERR_ARG, "ptt_round: null tt");
+    if (x->d < 2) return PTT_OK;
+    if (!(tol >= 0.0)) return ptt_set_error(PTT_ERR_ARG, "ptt_round: tol must be >= 0");
+    cudaSetDevice(x->ctx->device);
     int rmax = 1;
     for (int k = 0; k <= x->d; k++) rmax = rk[k] > rmax ? rk[k] : rmax;
     const double delta = ptt_round_threshold(x, tol);
+    if (rmax <= 32 && wt_fits(x, rk)) return round_impl_w(x, rk, delta, maxrank, phases, only);
     if (rmax <= 32) return round_impl<32>(x, rk, delta, maxrank, phases, only);
     if (rmax <= 64) return round_impl<64>(x, rk, delta, maxrank, phases, only);
     if (rmax <= 128) return round_impl<128>(x, rk, delta, maxrank, phases, only);

@@ -32,14 +32,22 @@ struct GemmB {
 };
 
 // C[b] = alpha * A[b] B[b] + beta * C[b]; batch b = b1 + nb1 * b2.
+// With split-K (part != NULL) grid z runs over (batch, slice): slice s sums
+// k in [s kper, (s+1) kper) and writes its tile to part[s][b][M][N]; a
+// second kernel adds the slices in order (deterministic).
 template <int TM>
-__global__ void __launch_bounds__(256) k_gemm_b(GemmB g, int zoff) {
+__global__ void __launch_bounds__(256) k_gemm_b(GemmB g, long long zoff, int kper, double* part) {
     constexpr int BK = 16;
     constexpr int RT = TM / 16;
     __shared__ double sA[BK][TM + 1];
     __shared__ double sB[BK][TM + 1];
-    const int bz = blockIdx.z + zoff;
+    const long long nb = (long long)g.nb1 * g.nb2;
+    const long long zz = blockIdx.z + zoff;
+    const int sl = (int)(zz / nb);
+    const int bz = (int)(zz - (long long)sl * nb);
     const int b1 = bz % g.nb1, b2 = bz / g.nb1;
+    const int kbeg = sl * kper;
+    const int kend = (kbeg + kper) < g.K ? (kbeg + kper) : g.K;
     const double* A = g.A + b1 * g.ab1 + b2 * g.ab2;
     const double* B = g.B + b1 * g.bb1 + b2 * g.bb2;
     double* C = g.C + b1 * g.cb1 + b2 * g.cb2;
@@ -52,7 +60,7 @@ __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, int zoff) {
     for (int i = 0; i < RT; i++)
 #pragma unroll
         for (int j = 0; j < RT; j++) acc[i][j] = 0.0;
-    for (int k0 = 0; k0 < g.K; k0 += BK) {
+    for (int k0 = kbeg; k0 < kend; k0 += BK) {
         for (int e = tid; e < TM * BK; e += 256) {
             int r, kk;
             if (a_colmajor) {
@@ -63,7 +71,7 @@ __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, int zoff) {
                 r = e / BK;
             }
             const int gr = m0 + r, gk = k0 + kk;
-            sA[kk][r] = (gr < g.M && gk < g.K) ? A[(long long)gr * g.ars + (long long)gk * g.acs] : 0.0;
+            sA[kk][r] = (gr < g.M && gk < kend) ? A[(long long)gr * g.ars + (long long)gk * g.acs] : 0.0;
         }
         for (int e = tid; e < TM * BK; e += 256) {
             int cn, kk;
@@ -75,7 +83,7 @@ __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, int zoff) {
                 cn = e / BK;
             }
             const int gk = k0 + kk, gc = n0 + cn;
-            sB[kk][cn] = (gk < g.K && gc < g.N) ? B[(long long)gk * g.brs + (long long)gc * g.bcs] : 0.0;
+            sB[kk][cn] = (gk < kend && gc < g.N) ? B[(long long)gk * g.brs + (long long)gc * g.bcs] : 0.0;
         }
         __syncthreads();
 #pragma unroll
@@ -100,9 +108,30 @@ __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, int zoff) {
         for (int j = 0; j < RT; j++) {
             const int gc = n0 + tx + 16 * j;
             if (gc >= g.N) continue;
+            if (part) {
+                part[(((long long)sl * nb + bz) * g.M + gr) * g.N + gc] = acc[i][j];
+                continue;
+            }
             double* cp = C + (long long)gr * g.crs + (long long)gc * g.ccs;
             *cp = (g.beta != 0.0) ? fma(g.alpha, acc[i][j], g.beta * *cp) : g.alpha * acc[i][j];
         }
+    }
+}
+
+// C[b][r][c] = alpha * sum_s part[s][b][r][c] + beta * C, slices in order
+__global__ void k_gemm_red(GemmB g, int ns, const double* part) {
+    const long long nb = (long long)g.nb1 * g.nb2;
+    const long long per = (long long)g.M * g.N, tot = per * nb;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int s = 0; s < ns; s++) acc += part[(long long)s * tot + e];
+        const int bz = (int)(e / per);
+        const long long rc = e - (long long)bz * per;
+        const int gr = (int)(rc / g.N), gc = (int)(rc - (long long)gr * g.N);
+        const int b1 = bz % g.nb1, b2 = bz / g.nb1;
+        double* cp = g.C + b1 * g.cb1 + b2 * g.cb2 + (long long)gr * g.crs + (long long)gc * g.ccs;
+        *cp = (g.beta != 0.0) ? fma(g.alpha, acc, g.beta * *cp) : g.alpha * acc;
     }
 }
 
@@ -113,16 +142,43 @@ int gemm(ptt_ctx* c, const GemmB& g) {
     const bool big = g.M >= 48 && g.N >= 48;
     const int TM = big ? 64 : 32;
     dim3 grid((g.M + TM - 1) / TM, (g.N + TM - 1) / TM, 1);
-    for (long long z0 = 0; z0 < nb; z0 += 65535) {
-        grid.z = (unsigned)((nb - z0) < 65535 ? (nb - z0) : 65535);
-        ptt_time_begin(c, PTT_TIME_GEMM);
+    // split K when the tiles alone cannot fill the GPU and K is long
+    const long long tiles = (long long)grid.x * grid.y * nb;
+    int ns = 1, kper = g.K;
+    if (tiles < 2 * 148 && g.K >= 512) {
+        long long want = (2 * 148 + tiles - 1) / tiles;
+        const long long kmax = (g.K + 255) / 256;
+        ns = (int)(want < kmax ? want : kmax);
+        if (ns > 64) ns = 64;
+        kper = (g.K + ns - 1) / ns;
+        kper = (kper + 15) / 16 * 16;
+        ns = (g.K + kper - 1) / kper;
+    }
+    double* part = nullptr;
+    if (ns > 1) {
+        const size_t need = sizeof(double) * (size_t)ns * (size_t)nb * (size_t)g.M * (size_t)g.N;
+        int rc = ptt_ws3_reserve(c, need);
+        if (rc) return rc;
+        part = (double*)c->ws3;
+    }
+    const long long nz = nb * ns;
+    ptt_time_begin(c, PTT_TIME_GEMM);
+    for (long long z0 = 0; z0 < nz; z0 += 65535) {
+        grid.z = (unsigned)((nz - z0) < 65535 ? (nz - z0) : 65535);
         if (big)
-            k_gemm_b<64><<<grid, 256, 0, c->stream>>>(g, (int)z0);
+            k_gemm_b<64><<<grid, 256, 0, c->stream>>>(g, z0, kper, part);
         else
-            k_gemm_b<32><<<grid, 256, 0, c->stream>>>(g, (int)z0);
-        ptt_time_end(c, PTT_TIME_GEMM);
+            k_gemm_b<32><<<grid, 256, 0, c->stream>>>(g, z0, kper, part);
         PTT_LAUNCHED(c);
     }
+    if (part) {
+        const long long tot = (long long)g.M * g.N * nb;
+        long long nbk = (tot + 255) / 256;
+        if (nbk > 1184) nbk = 1184;
+        k_gemm_red<<<(int)nbk, 256, 0, c->stream>>>(g, ns, part);
+        PTT_LAUNCHED(c);
+    }
+    ptt_time_end(c, PTT_TIME_GEMM);
     return PTT_OK;
 }
 
@@ -312,8 +368,18 @@ static int sketch_round(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* 
         if ((rc = gemm(c, g))) return rc;
         int rr[2] = {r, Lp};
         if ((rc = ptt_set_ranks_async(z, k, rr, 2))) return rc;
-        if ((rc = ptt_round_phases(z, 0.0, NULL, 4, k))) return rc;
-        if ((rc = ptt_pull_desc(z))) return rc;
+        {
+            // QR of core k: ranks known here (no read-back); the QR swaps
+            // core k with its second buffer, mirrored in the host shadow
+            int rk[PTT_MAX_DIM + 1];
+            for (int i = 0; i <= d; i++) rk[i] = 1;  // only core k is factored
+            rk[k] = r;
+            rk[k + 1] = Lp;
+            if ((rc = ptt_round_phases_rk(z, rk, 0.0, NULL, 4, k))) return rc;
+            double* t = z->hd.core[k];
+            z->hd.core[k] = z->hd.alt[k];
+            z->hd.alt[k] = t;
+        }
         const int q = r * nk < Lp ? r * nk : Lp;
         // M' = Q^T Z   (q x Rp)
         g = GemmB{z->hd.core[k], (long long)r * nk, 1, 0, 0,
@@ -330,7 +396,7 @@ static int sketch_round(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* 
     if ((rc = ptt_set_ranks_async(z, 0, zr, d + 1))) return rc;
     if (used)
         for (int k = 0; k <= d; k++) used[k] = L[k];
-    return ptt_round_phases(z, tol, maxrank, 2, 0);
+    return ptt_round_phases_rk(z, zr, tol, maxrank, 2, 0);
 }
 
 extern "C" int ptt_round_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* ell, unsigned long long seed,

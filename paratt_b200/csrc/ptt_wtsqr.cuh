@@ -1,0 +1,741 @@
+// Warp-level TSQR for unfoldings with at most 32 columns (included by
+// ptt_round.cu inside its anonymous namespace, after the block-level kernels).
+//
+// One warp owns one 32-row leaf of the m x c unfolding; lane l owns column l
+// of the leaf tile, held in registers.  A Householder step then needs no
+// barrier: the pivot lane's column norm and vector are broadcast with
+// shuffles and every lane updates its own column.  The reflector loops are
+// unrolled over the 32 rows, so every register index is a compile-time
+// constant.
+//
+// Tree: leaves p = 0..W-1 (W = ceil(m / 32)) sit at heap slots P-1+p,
+// P = next_pow2(W).  A node whose right subtree holds no leaf passes the left
+// child's R up unchanged.  Otherwise the warp that arrives second (atomic
+// ticket, nobody waits) combines [R_left; R_right] -- always left on top, so
+// the result does not depend on which warp arrived first -- with Householder
+// steps on the two triangles; the vectors replace R_right in its slot.  The
+// last leaf may be short (h < 32 rows); it is never the upper triangle of a
+// combination, and with m < c the single leaf gives a q = m row trapezoid.
+//
+// Pivot rows are always real rows of the unfolding (as in LAPACK), so Q has
+// orthonormal columns also for rank-deficient unfoldings.
+//
+// Q is not formed while sweeping: k_wapply forms Q*B for all bonds of a sweep
+// in one launch.  Each warp walks from the root to its leaf applying the node
+// reflectors to B (c x qB, one column per lane), then its leaf's reflectors,
+// and writes its 32 rows of Q*B.
+#pragma once
+
+namespace wt {
+
+constexpr int WPB = 4;  // warps per block
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int SLOT = 32 * 32;
+constexpr int PMAX = 4096;  // leaves per bond (m <= 131072)
+
+// Per-bond tree records.  Bond (core) k's region starts at ws + k * stride;
+// offsets are in doubles within a region; counters of bond k at cnt + k * Pcap.
+struct WP {
+    long long o_R;   // (2 Pcap - 1) slots, R or vectors, row-major 32 x 32
+    long long o_tl;  // leaf taus, Pcap x 32
+    long long o_tn;  // node taus, Pcap x 32
+    long long stride;
+    int Pcap;
+    int* cnt;        // zero between launches; reset by the combining warp
+};
+
+__host__ __device__ __forceinline__ int pow2_ge(int v) {
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+// Rows [r0, r0 + h) x columns [0, c) of the view into X (lane = column),
+// zero elsewhere.  Column-major views are read along rows and transposed
+// through the warp's shared tile so every load is coalesced.
+__device__ __forceinline__ void w_load(const double* p, long long rs, long long cs, int r0, int h, int c,
+                                       double (&X)[32], double* sh) {
+    const int lane = threadIdx.x & 31;
+    if (rs == 1) {
+        // lane = row: all column loads in flight at once, then transpose
+#pragma unroll
+        for (int l = 0; l < 32; l++) X[l] = (l < c && lane < h) ? p[(long long)(r0 + lane) + (long long)l * cs] : 0.0;
+#pragma unroll
+        for (int l = 0; l < 32; l++) sh[lane * 33 + l] = X[l];
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < 32; t++) X[t] = lane < c ? sh[t * 33 + lane] : 0.0;
+        __syncwarp();
+    } else {
+#pragma unroll
+        for (int t = 0; t < 32; t++)
+            X[t] = (t < h && lane < c) ? p[(long long)(r0 + t) * rs + (long long)lane * cs] : 0.0;
+    }
+}
+
+// Rows [r0, r0 + h) x columns [0, nc) of X (lane = column) into the view.
+__device__ __forceinline__ void w_store(double* p, long long rs, long long cs, int r0, int h, int nc,
+                                        const double (&X)[32], double* sh) {
+    const int lane = threadIdx.x & 31;
+    if (rs == 1) {
+#pragma unroll
+        for (int t = 0; t < 32; t++) sh[t * 33 + lane] = X[t];
+        __syncwarp();
+        if (lane < h)
+#pragma unroll 8
+            for (int l = 0; l < nc; l++) p[(long long)(r0 + lane) + (long long)l * cs] = sh[lane * 33 + l];
+        __syncwarp();
+    } else {
+        if (lane < nc)
+#pragma unroll
+            for (int t = 0; t < 32; t++)
+                if (t < h) p[(long long)(r0 + t) * rs + (long long)lane * cs] = X[t];
+    }
+}
+
+#ifdef WT_ROLLED
+// Rolled forms: the reflector loop is not unrolled (small code); the pivot
+// row is picked and written back by selects over the compile-time rows.
+__device__ __forceinline__ double w_geqrt(double (&X)[32], int c, int h) {
+    const int lane = threadIdx.x & 31;
+    const int nr = c < h ? c : h;
+    double mytau = 0.0;
+#pragma unroll 1
+    for (int j = 0; j < nr; j++) {
+        double s0 = 0.0, s1 = 0.0, xj = 0.0;
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+            const double x = X[t];
+            if (t == j) xj = x;
+            const double y = t > j ? x : 0.0;
+            if (t & 1)
+                s0 = fma(y, y, s0);
+            else
+                s1 = fma(y, y, s1);
+        }
+        const double alpha = __shfl_sync(FULL, xj, j);
+        const double s2 = __shfl_sync(FULL, s0 + s1, j);
+        double beta, tau, sc;
+        hh_params(alpha, s2, &beta, &tau, &sc);
+        double V[32];
+        double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+            const double sv = __shfl_sync(FULL, X[t], j);
+            V[t] = t > j ? sv * sc : 0.0;
+            if (t & 1)
+                d0 = fma(V[t], X[t], d0);
+            else
+                d1 = fma(V[t], X[t], d1);
+        }
+        const double w = tau * (xj + (d0 + d1));
+        const bool upd = lane > j, piv = lane == j;
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+            const double x = X[t];
+            double y = upd ? fma(-w, V[t], x) : ((piv && t > j) ? V[t] : x);
+            if (t == j) y = upd ? x - w : (piv ? beta : x);
+            X[t] = y;
+        }
+        if (piv) mytau = tau;
+    }
+    return mytau;
+}
+
+__device__ __forceinline__ double w_ttqrt(double (&T)[32], double (&B)[32], int c) {
+    const int lane = threadIdx.x & 31;
+    double mytau = 0.0;
+#pragma unroll 1
+    for (int j = 0; j < c; j++) {
+        double s0 = 0.0, s1 = 0.0, tj = 0.0;
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+            if (t == j) tj = T[t];
+            const double y = t <= j ? B[t] : 0.0;
+            if (t & 1)
+                s0 = fma(y, y, s0);
+            else
+                s1 = fma(y, y, s1);
+        }
+        const double alpha = __shfl_sync(FULL, tj, j);
+        const double s2 = __shfl_sync(FULL, s0 + s1, j);
+        double beta, tau, sc;
+        hh_params(alpha, s2, &beta, &tau, &sc);
+        double V[32];
+        double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+            const double sv = __shfl_sync(FULL, B[t], j);
+            V[t] = t <= j ? sv * sc : 0.0;
+            if (t & 1)
+                d0 = fma(V[t], B[t], d0);
+            else
+                d1 = fma(V[t], B[t], d1);
+        }
+        const double w = tau * (tj + (d0 + d1));
+        const bool upd = lane > j, piv = lane == j;
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+            const double b = B[t];
+            B[t] = upd ? fma(-w, V[t], b) : ((piv && t <= j) ? V[t] : b);
+            if (t == j) T[t] = upd ? T[t] - w : (piv ? beta : T[t]);
+        }
+        if (piv) mytau = tau;
+    }
+    return mytau;
+}
+#else
+// Householder QR of the h x c tile X (lane = column, rows >= h are zero).
+// On exit rows t <= lane of X hold R and rows t > lane the vector of
+// reflector `lane` (unit diagonal implied); returns that reflector's tau.
+__device__ __forceinline__ double w_geqrt(double (&X)[32], int c, int h) {
+    const int lane = threadIdx.x & 31;
+    const int nr = c < h ? c : h;
+    double mytau = 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+        if (j >= nr) continue;
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int t = j + 1; t < 32; t++) {
+            if ((t - j) & 1)
+                s0 = fma(X[t], X[t], s0);
+            else
+                s1 = fma(X[t], X[t], s1);
+        }
+        const double alpha = __shfl_sync(FULL, X[j], j);
+        const double s2 = __shfl_sync(FULL, s0 + s1, j);
+        double beta, tau, sc;
+        hh_params(alpha, s2, &beta, &tau, &sc);
+        double V[32];
+        double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+        for (int t = j + 1; t < 32; t++) {
+            V[t] = __shfl_sync(FULL, X[t], j) * sc;
+            if ((t - j) & 1)
+                d0 = fma(V[t], X[t], d0);
+            else
+                d1 = fma(V[t], X[t], d1);
+        }
+        const double w = tau * (X[j] + (d0 + d1));
+        if (lane > j) {
+            X[j] -= w;
+#pragma unroll
+            for (int t = j + 1; t < 32; t++) X[t] = fma(-w, V[t], X[t]);
+        } else if (lane == j) {
+            X[j] = beta;
+#pragma unroll
+            for (int t = j + 1; t < 32; t++) X[t] = V[t];
+            mytau = tau;
+        }
+    }
+    return mytau;
+}
+
+// [T; B] with T, B upper triangular (lane = column): eliminate B into T.
+// On exit T is the R of the pair and rows t <= lane of B hold the vector of
+// reflector `lane` (its top part is e_lane); returns that reflector's tau.
+__device__ __forceinline__ double w_ttqrt(double (&T)[32], double (&B)[32], int c) {
+    const int lane = threadIdx.x & 31;
+    double mytau = 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+        if (j >= c) continue;
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int t = 0; t <= j; t++) {
+            if (t & 1)
+                s0 = fma(B[t], B[t], s0);
+            else
+                s1 = fma(B[t], B[t], s1);
+        }
+        const double alpha = __shfl_sync(FULL, T[j], j);
+        const double s2 = __shfl_sync(FULL, s0 + s1, j);
+        double beta, tau, sc;
+        hh_params(alpha, s2, &beta, &tau, &sc);
+        double V[32];
+        double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+        for (int t = 0; t <= j; t++) {
+            V[t] = __shfl_sync(FULL, B[t], j) * sc;
+            if (t & 1)
+                d0 = fma(V[t], B[t], d0);
+            else
+                d1 = fma(V[t], B[t], d1);
+        }
+        const double w = tau * (T[j] + (d0 + d1));
+        if (lane > j) {
+            T[j] -= w;
+#pragma unroll
+            for (int t = 0; t <= j; t++) B[t] = fma(-w, V[t], B[t]);
+        } else if (lane == j) {
+            T[j] = beta;
+#pragma unroll
+            for (int t = 0; t <= j; t++) B[t] = V[t];
+            mytau = tau;
+        }
+    }
+    return mytau;
+}
+
+#endif  // WT_ROLLED
+
+// Factor the unfolding (mode) of core k: leaf reflectors in place, taus and
+// tree records in the bond's region wsb, R at slot 0, Info (m, c, q).
+// A block holds FPB leaves; the lowest LB = log2(FPB) tree levels are
+// combined inside the block through shared memory, the levels above by the
+// warp 0 of each block through the global slots (last arriver combines).
+#ifndef WT_FLB
+#define WT_FLB 3
+#endif
+constexpr int FLB = WT_FLB;       // tree levels combined inside a block
+constexpr int FPB = 1 << FLB;     // warps (leaves) per factor block
+
+__host__ __device__ constexpr size_t wfactor_smem() { return sizeof(double) * FPB * 32 * 33; }
+
+__global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, int mode, Plan pl, WP wp,
+                                                      double* wsb, int* status) {
+    extern __shared__ double fsm[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int p = blockIdx.x * FPB + wid;
+    const View A = make_view(D, k, mode, false);
+    const int m = A.m, c = A.c;
+    Info* info = (Info*)(wsb + pl.o_info_d);
+    const int W = (m + 31) >> 5;
+    const int P = pow2_ge(W);
+    if (c > 32 || c < 1 || m < 1 || P > wp.Pcap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            info->status = PTT_ERR_CAPACITY;
+            PTT_STATUS_SET(status, PTT_ERR_CAPACITY);
+        }
+        return;  // uniform over the block
+    }
+    if (blockIdx.x * FPB >= W) return;  // uniform over the block
+    if (pl.work && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(pl.work, 16.0 * (double)m * (double)c);
+    double* sw = fsm + wid * (32 * 33);
+    const bool valid = p < W;
+    const int r0 = p * 32;
+    const int h = valid ? ((m - r0) < 32 ? (m - r0) : 32) : 0;
+    double* Rs = wsb + wp.o_R;
+    double X[32];
+    if (valid) {
+        w_load(A.p, A.rs, A.cs, r0, h, c, X, sw);
+        const double tl = w_geqrt(X, c, h);
+        w_store(A.p, A.rs, A.cs, r0, h, c, X, sw);
+        wsb[wp.o_tl + p * 32 + lane] = tl;
+#pragma unroll
+        for (int t = 0; t < 32; t++)
+            if (t > lane) X[t] = 0.0;
+    }
+    // in-block levels: the left child's warp combines with its right sibling
+    int lb = 0;
+    while ((1 << lb) < P && lb < FLB) lb++;
+    for (int lvl = 0; lvl < lb; lvl++) {
+        const int span = 1 << lvl;
+        const int mask = (2 << lvl) - 1;
+        __syncthreads();
+        if (valid && (wid & mask) == span) {
+#pragma unroll
+            for (int t = 0; t < 32; t++) sw[t * 32 + lane] = X[t];
+        }
+        __syncthreads();
+        if (valid && (wid & mask) == 0 && p + span < W) {
+            const double* Rr = fsm + (wid + span) * (32 * 33);
+            double B[32];
+#pragma unroll
+            for (int t = 0; t < 32; t++) B[t] = Rr[t * 32 + lane];
+            const double tn = w_ttqrt(X, B, c);
+            const int node = ((P + p) >> (lvl + 1)) - 1;
+            double* Vo = Rs + (long long)(2 * node + 2) * SLOT;
+#pragma unroll
+            for (int t = 0; t < 32; t++) Vo[t * 32 + lane] = B[t];
+            wsb[wp.o_tn + node * 32 + lane] = tn;
+        }
+    }
+    if (wid != 0) return;
+    // global levels
+    int* cnt = wp.cnt + (long long)k * wp.Pcap;
+    int slot = ((P + p) >> lb) - 1, lvl = lb;
+    while (slot > 0) {
+        const int node = (slot - 1) >> 1;
+        const int span = 1 << lvl;
+        const int base = (p >> (lvl + 1)) << (lvl + 1);
+        if (base + span >= W) {  // empty right subtree: pass R up
+            slot = node;
+            lvl++;
+            continue;
+        }
+        double* Ro = Rs + (long long)slot * SLOT;
+#pragma unroll
+        for (int t = 0; t < 32; t++) Ro[t * 32 + lane] = X[t];
+        __threadfence();
+        int old = 0;
+        if (lane == 0) old = atomicAdd(cnt + node, 1);
+        old = __shfl_sync(FULL, old, 0);
+        if (old == 0) return;  // the sibling's warp combines
+        __threadfence();
+        if (lane == 0) cnt[node] = 0;
+        const double* Rl = Rs + (long long)(2 * node + 1) * SLOT;
+        double* Rr = Rs + (long long)(2 * node + 2) * SLOT;
+        double B[32];
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+            X[t] = __ldcg(Rl + t * 32 + lane);
+            B[t] = __ldcg(Rr + t * 32 + lane);
+        }
+        const double tn = w_ttqrt(X, B, c);
+#pragma unroll
+        for (int t = 0; t < 32; t++) Rr[t * 32 + lane] = B[t];
+        wsb[wp.o_tn + node * 32 + lane] = tn;
+        slot = node;
+        lvl++;
+    }
+#pragma unroll
+    for (int t = 0; t < 32; t++) Rs[t * 32 + lane] = X[t];
+    if (lane == 0) {
+        info->m = m;
+        info->c = c;
+        info->q = m < c ? m : c;
+        info->rank = 0;
+        info->status = 0;
+    }
+}
+
+// out = Q * B for bonds (cores) k = k0 .. k0 + gridDim.y - 1 of one sweep,
+// with the sizes recorded by k_wfactor (the descriptor's ranks have moved on).
+//   LEFT:    B = I_q;                       out (m x q, column-major) -> alt[k]
+//   RIGHT_T: B = V_r (Bn, row-major 32 x KC); out(row, col) -> alt[k][row * rank + col]
+__global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, int mode, Plan pl, WP wp, double* ws) {
+    __shared__ double sh[WPB][32 * 33];
+    __shared__ double stau[WPB][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int k = k0 + blockIdx.y;
+    double* wsb = ws + (long long)k * wp.stride;
+    const Info* info = (const Info*)(wsb + pl.o_info_d);
+    if (info->status) return;
+    const int m = info->m, c = info->c, q = info->q;
+    const int qB = (mode == LEFT) ? q : info->rank;
+    const int W = (m + 31) >> 5, P = pow2_ge(W);
+    const int p = blockIdx.x * WPB + wid;
+    if (p >= W) return;
+    double* sw = sh[wid];
+    volatile double* vs = sw;  // re-read in the updates instead of holding 32 values
+    double* st = stau[wid];
+    const double* Rs = wsb + wp.o_R;
+    double X[32];
+    if (mode == LEFT) {
+#pragma unroll
+        for (int t = 0; t < 32; t++) X[t] = (t == lane && lane < q) ? 1.0 : 0.0;
+    } else {
+        const double* Bn = wsb + pl.o_Bn;
+#pragma unroll
+        for (int t = 0; t < 32; t++) X[t] = lane < qB ? Bn[(long long)t * pl.KC + lane] : 0.0;
+    }
+    // root to leaf
+    int s = 0, base = 0;
+    for (int half = P >> 1; half >= 1; half >>= 1) {
+        if (base + half >= W) {  // pass-through node
+            s = 2 * s + 1;
+            continue;
+        }
+        const bool right = p >= base + half;
+        const double* V = Rs + (long long)(2 * s + 2) * SLOT;  // vector j: rows t <= j of column j
+#pragma unroll 4
+        for (int t = 0; t < 32; t++) sw[t * 33 + lane] = V[t * 32 + lane];
+        st[lane] = wsb[wp.o_tn + s * 32 + lane];
+        __syncwarp();
+        double Bt[32];
+#pragma unroll
+        for (int t = 0; t < 32; t++) Bt[t] = 0.0;
+#ifdef WT_ROLLED
+#pragma unroll 1
+        for (int j = c - 1; j >= 0; j--) {
+            const double tau = st[j];
+            double d0 = 0.0, d1 = 0.0, xj = 0.0;
+#pragma unroll
+            for (int t = 0; t < 32; t++) {
+                if (t == j) xj = X[t];
+                const double vv = t <= j ? sw[t * 33 + j] : 0.0;
+                if (t & 1)
+                    d0 = fma(vv, Bt[t], d0);
+                else
+                    d1 = fma(vv, Bt[t], d1);
+            }
+            const double w = tau * (xj + (d0 + d1));
+#pragma unroll
+            for (int t = 0; t < 32; t++) {
+                if (t == j) X[t] = xj - w;
+                if (t <= j) Bt[t] = fma(-w, vs[t * 33 + j], Bt[t]);
+            }
+        }
+#else
+#pragma unroll
+        for (int j = 31; j >= 0; j--) {
+            if (j >= c) continue;
+            const double tau = st[j];
+            double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+            for (int t = 0; t <= j; t++) {
+                if (t & 1)
+                    d0 = fma(sw[t * 33 + j], Bt[t], d0);
+                else
+                    d1 = fma(sw[t * 33 + j], Bt[t], d1);
+            }
+            const double w = tau * (X[j] + (d0 + d1));
+            X[j] -= w;
+#pragma unroll
+            for (int t = 0; t <= j; t++) Bt[t] = fma(-w, vs[t * 33 + j], Bt[t]);
+        }
+#endif
+        __syncwarp();
+        if (right) {
+#pragma unroll
+            for (int t = 0; t < 32; t++) X[t] = Bt[t];
+            base += half;
+            s = 2 * s + 2;
+        } else {
+            s = 2 * s + 1;
+        }
+    }
+    // leaf: reflectors stored in place in core k
+    const double* Ap = D->core[k];
+    const long long ars = (mode == LEFT) ? 1 : c, acs = (mode == LEFT) ? m : 1;
+    const int r0 = p * 32;
+    const int h = (m - r0) < 32 ? (m - r0) : 32;
+    if (mode == LEFT) {
+#pragma unroll 8
+        for (int j = 0; j < c; j++) sw[lane * 33 + j] = lane < h ? Ap[(long long)(r0 + lane) + (long long)j * acs] : 0.0;
+    } else {
+#pragma unroll 4
+        for (int t = 0; t < 32; t++) sw[t * 33 + lane] = (t < h && lane < c) ? Ap[(long long)(r0 + t) * ars + lane] : 0.0;
+    }
+    st[lane] = wsb[wp.o_tl + p * 32 + lane];
+    __syncwarp();
+    const int nr = c < h ? c : h;
+#ifdef WT_ROLLED
+#pragma unroll 1
+    for (int j = nr - 1; j >= 0; j--) {
+        const double tau = st[j];
+        double d0 = 0.0, d1 = 0.0, xj = 0.0;
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+            if (t == j) xj = X[t];
+            const double vv = t > j ? sw[t * 33 + j] : 0.0;
+            if (t & 1)
+                d0 = fma(vv, X[t], d0);
+            else
+                d1 = fma(vv, X[t], d1);
+        }
+        const double w = tau * (xj + (d0 + d1));
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+            if (t == j) X[t] = xj - w;
+            if (t > j) X[t] = fma(-w, vs[t * 33 + j], X[t]);
+        }
+    }
+#else
+#pragma unroll
+    for (int j = 31; j >= 0; j--) {
+        if (j >= nr) continue;
+        const double tau = st[j];
+        double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+        for (int t = j + 1; t < 32; t++) {
+            if ((t - j) & 1)
+                d0 = fma(sw[t * 33 + j], X[t], d0);
+            else
+                d1 = fma(sw[t * 33 + j], X[t], d1);
+        }
+        const double w = tau * (X[j] + (d0 + d1));
+        X[j] -= w;
+#pragma unroll
+        for (int t = j + 1; t < 32; t++) X[t] = fma(-w, vs[t * 33 + j], X[t]);
+    }
+#endif
+    __syncwarp();
+    double* out = D->alt[k];
+    if (mode == LEFT)
+        w_store(out, 1, m, r0, h, qB, X, sw);
+    else
+        w_store(out, qB, 1, r0, h, qB, X, sw);
+}
+
+// One-sided Jacobi SVD of L = R^T (c x q, c <= 32) by one warp: lane j owns
+// column j of L (row j of the root R) and column j of V.  Pairs follow the
+// same circle ordering, tolerance, tracked norms and sweep limit as
+// k_svd_jacobi; both lanes of a pair form the same dot product in the same
+// order, so they take the same rotation.  Writes the same records (Info,
+// per-bond stats, sig/order, U_r S_r) and V_r into Bn directly, so no
+// rotation log or replay is needed.
+__global__ void __launch_bounds__(32) k_wsvd(Plan pl, double* ws, double delta, int maxr, int bond, int* status) {
+    __shared__ double sL[32 * 33];
+    __shared__ double sV[32 * 33];
+    __shared__ double s_sig[32];
+    __shared__ int s_ord[32];
+    __shared__ int s_rank;
+    const int lane = threadIdx.x;
+    Info* info = pl.info;
+    if (info->status) return;
+    const int c = info->c, q = info->q;
+    const int qq = q + (q & 1);
+    const double* R = ws + pl.o_Rn;
+    double a[32], v[32], b[32];
+#pragma unroll
+    for (int t = 0; t < 32; t++) {
+        a[t] = (lane < q && t < c) ? __ldcg(R + lane * 32 + t) : 0.0;
+        v[t] = (t == lane && lane < q) ? 1.0 : 0.0;
+    }
+    const double tol = (double)(c < 16 ? 16 : c) * 2.220446049250313e-16;
+    int sweeps = 0;
+    bool conv = (qq < 2);
+    for (int sw = 0; sw < MAXSW && !conv; sw++) {
+        double n0 = 0.0, n1 = 0.0;
+#pragma unroll
+        for (int t = 0; t < 32; t += 2) {
+            n0 = fma(a[t], a[t], n0);
+            n1 = fma(a[t + 1], a[t + 1], n1);
+        }
+        double nrm = n0 + n1;
+        int rot = 0;
+        for (int rd = 0; rd < qq - 1; rd++) {
+            int pos = 0;
+            if (lane > 0) {
+                const int e = (lane - 1 - rd) % (qq - 1);
+                pos = 1 + (e < 0 ? e + qq - 1 : e);
+            }
+            const bool act = lane < qq;
+            const int src = act ? circle_col(qq - 1 - pos, rd, qq) : lane;
+            const bool first = pos < qq / 2;
+            double g0 = 0.0, g1 = 0.0;
+#pragma unroll
+            for (int t = 0; t < 32; t += 2) {
+                b[t] = __shfl_sync(FULL, a[t], src);
+                b[t + 1] = __shfl_sync(FULL, a[t + 1], src);
+                g0 = fma(a[t], b[t], g0);
+                g1 = fma(a[t + 1], b[t + 1], g1);
+            }
+            const double ga = g0 + g1;
+            const double nb = __shfl_sync(FULL, nrm, src);
+            const double al = first ? nrm : nb, be = first ? nb : nrm;
+            const bool doit = act && ga != 0.0 && fabs(ga) > tol * sqrt(al * be);
+            double cs = 1.0, sn = 0.0;
+            if (doit) {
+                const double dd = be - al, g2 = 2.0 * ga;
+                const double tn = g2 * __drcp_rn(dd + copysign(sqrt(fma(dd, dd, g2 * g2)), dd));
+                cs = rsqrt(fma(tn, tn, 1.0));
+                sn = cs * tn;
+                if (first) {
+#pragma unroll
+                    for (int t = 0; t < 32; t++) a[t] = cs * a[t] - sn * b[t];
+                    nrm = al - tn * ga;
+                } else {
+#pragma unroll
+                    for (int t = 0; t < 32; t++) a[t] = sn * b[t] + cs * a[t];
+                    nrm = be + tn * ga;
+                }
+                rot = 1;
+            }
+#pragma unroll
+            for (int t = 0; t < 32; t++) {
+                const double vb = __shfl_sync(FULL, v[t], src);
+                if (doit) v[t] = first ? cs * v[t] - sn * vb : sn * vb + cs * v[t];
+            }
+        }
+        if (__any_sync(FULL, rot))
+            sweeps = sw + 1;
+        else
+            conv = true;
+    }
+    if (!conv && lane == 0) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
+    double n0 = 0.0, n1 = 0.0;
+#pragma unroll
+    for (int t = 0; t < 32; t += 2) {
+        n0 = fma(a[t], a[t], n0);
+        n1 = fma(a[t + 1], a[t + 1], n1);
+    }
+    const double sg = lane < q ? sqrt(n0 + n1) : -1.0;
+    int pos = 0;
+    for (int i = 0; i < 32; i++) {
+        const double si = __shfl_sync(FULL, sg, i);
+        if (i < qq) pos += (si > sg) || (si == sg && i < lane);
+    }
+    s_sig[lane] = sg;
+    if (lane < qq) s_ord[pos] = lane;
+#pragma unroll
+    for (int t = 0; t < 32; t++) {
+        sL[lane * 33 + t] = a[t];
+        sV[lane * 33 + t] = v[t];
+    }
+    __syncwarp();
+    double* sig_out = ws + pl.o_sig;
+    if (lane == 0) {
+        const double s0 = q > 0 ? s_sig[s_ord[0]] : 0.0;
+        // numerical rank kept by LAPACK dgesvdq(JOBA='A'): sqrt(N)*eps*s0
+        const double thr = sqrt((double)q) * 1.1102230246251565e-16 * s0;
+        int nsv = q > 0 ? 1 : 0;
+        while (nsv < q && s_sig[s_ord[nsv]] >= thr) nsv++;
+        if (!(s0 == s0)) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
+        // tail-sum rule, pattac.c:468-481
+        double ssum = 0.0;
+        int rank = nsv;
+        for (int j = nsv - 1; j >= 0; j--) {
+            const double sj = s_sig[s_ord[j]];
+            ssum += sj * sj;
+            if (sqrt(ssum) < delta)
+                rank = j;
+            else
+                break;
+        }
+        if (rank > q) rank = q;
+        if (rank > maxr) rank = maxr;
+        if (rank < 1) rank = 1;
+        info->rank = rank;
+        info->nsv = nsv;
+        info->sweeps = sweeps;
+        double tail = 0.0;
+        for (int j = rank; j < q; j++) tail += s_sig[s_ord[j]] * s_sig[s_ord[j]];
+        info->tail = tail;
+        if (pl.stats) {
+            double* st = pl.stats + (long long)bond * PTT_STAT_LEN;
+            st[0] = rank;
+            st[1] = nsv;
+            st[2] = sweeps;
+            st[3] = q;
+            st[4] = c;
+            st[5] = tail;
+            st[6] = delta;
+            st[7] = 0.0;
+            for (int j = 0; j < PTT_STAT_NSIG; j++) st[8 + j] = j < q ? s_sig[s_ord[j]] : 0.0;
+        }
+        s_rank = rank;
+    }
+    __syncwarp();
+    const int rank = s_rank;
+    sig_out[lane] = 0.0;
+    ((int*)(sig_out + 32))[lane] = lane < qq ? s_ord[lane] : 0;
+    __syncwarp();
+    if (lane < q) sig_out[pos] = sg;
+    // U_r S_r (c x rank, column-major ld 32) and V_r (q x rank, row-major, ld KC)
+    double* US = ws + pl.o_US;
+    double* Bn = ws + pl.o_Bn;
+    for (int bb = 0; bb < 32; bb++) {
+        const int j = s_ord[bb < qq ? bb : 0];
+        US[bb * 32 + lane] = (bb < rank && lane < c) ? sL[j * 33 + lane] : 0.0;
+    }
+    for (int row = 0; row < 32; row++) {
+        const int j = s_ord[lane < qq ? lane : 0];
+        Bn[(long long)row * pl.KC + lane] = (row < q && lane < rank) ? sV[j * 33 + row] : 0.0;
+    }
+}
+
+// swap core and alt of cores [k0, k1) unless an error was recorded
+__global__ void k_wswap(DevDesc* D, int k0, int k1, const int* status) {
+    if (*status) return;
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        double* t = D->core[k];
+        D->core[k] = D->alt[k];
+        D->alt[k] = t;
+    }
+}
+
+}  // namespace wt

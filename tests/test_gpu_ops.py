@@ -58,6 +58,25 @@ def test_hadamard_bit_exact(ctx, dims, ranks):
     _same(Z.get(), O.hadamard(x, y))
 
 
+@pytest.mark.parametrize("dims,ranks", SHAPES)
+def test_square_sym(ctx, dims, ranks):
+    """x (.) x at ranks r(r+1)/2 is the same tensor as the formal square."""
+    x = O.random_tt(dims, ranks, 5)
+    X = P.TT.from_cores(ctx, x)
+    Z = P.TT(ctx, dims, [1] * (len(dims) + 1))
+    P.square_sym(X, Z)
+    z = Z.get()
+    assert [c.shape[0] for c in z] + [1] == [r * (r + 1) // 2 for r in ranks]
+    ref = O.full(O.hadamard(x, x))
+    np.testing.assert_allclose(O.full(z), ref, rtol=0, atol=1e-13 * np.abs(ref).max())
+    # the rounded square matches the rounded formal square
+    tol = 1e-10 * O.norm(x) ** 2
+    Z.round(tol)
+    zr = O.round_tt(O.hadamard(x, x), tol, 10**6)
+    assert [c.shape[0] for c in Z.get()] == [c.shape[0] for c in zr]
+    np.testing.assert_allclose(O.full(Z.get()), O.full(zr), rtol=0, atol=1e-11 * np.abs(ref).max())
+
+
 def test_scale_and_diag(ctx):
     dims, ranks = SHAPES[0]
     x = O.random_tt(dims, ranks, 5)
