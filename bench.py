@@ -1,19 +1,32 @@
 #!/usr/bin/env python3
 """Benchmark: reaction-Burgers step-truncation RK2 steps/s at d=40, n=256,
-rank-max 64, tol 1e-8 (config 4 of the benchmark plan), one trajectory per
-GPU (replicas; the step has no data-parallel exchange).
+rank-max 64, tol 1e-8 x ||u0||_RMS, dt 1e-3, 3-Gaussian initial condition
+(config 4 of the benchmark plan), one trajectory per GPU (replicas; the step
+has no data-parallel exchange).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One JSON line on rank 0.  `value` is steps/s over all GPUs with the state
-resident in HBM (CUDA events on the library's stream, L2 flushed before every
-step, flush outside the events); `e2e` is the same metric through the
-reference-facing C API (pattac_rxn_burgers_midpoint_st on host cores, pinned),
-host<->device copies inside the timed region; `roofline` is the dominant
-kernel class (TSQR factorisation tree) timed launch by launch with events
-during the timed steps; `cpu_baseline` is the reference's own C
-(oracle/_ref/libparatt_ref.so) on this host, extrapolated from a bounded
-per-bond sample of the same roundings.
+One JSON line on rank 0.  After W plain warm-up steps from the initial
+condition, the same state is advanced K steps by
+
+  * the learned-sketch method (`value`): before each step the MLP proposes
+    per-bond sketch ranks from the previous step's spectra, every rounding
+    goes through a Gaussian sketch of those ranks with the deterministic
+    truncation as judge and fallback (paratt_b200.learned.LearnedStepper);
+  * the plain method (`plain`): every rounding is the deterministic FP64
+    TSQR + Jacobi-SVD truncation (ptt_rxn_burgers_rk2_step).
+
+Both run with the state resident in HBM, timed by CUDA events on the
+library's stream around each step, L2 flushed before every step (outside
+the events).  `err_vs_plain` is the relative L2 difference between one
+learned and one plain step from the same state; `fallback_rate` the share of
+sketch roundings the judge sent back to the deterministic path.  `e2e` is the
+learned method with the state on the host (page-locked): upload, step,
+download every step, timed by the host clock.  `roofline` is the dominant
+kernel class (TSQR factorisation) timed launch by launch with events during
+the learned steps.  `cpu_baseline` / `--impl reference` time the reference's
+own C (oracle/_ref/libparatt_ref.so: paratt_truncate, pattacHadamard,
+attac_tt_axpby) composing the same RK2 step on this host's cores.
 """
 from __future__ import annotations
 
@@ -32,7 +45,6 @@ sys.path.insert(0, ROOT)
 
 METRIC = "RK steps/s d=40,n=256: learned-sketch vs plain rounding, 1 B200, err≤1e-8"
 CFG = dict(d=40, n=256, maxrank=64, tol=1e-8, dt=1e-3, ngauss=3, seed=3)
-REF_RANK = 20  # representative state rank for the reference's extrapolation
 
 
 def peaks():
@@ -94,37 +106,26 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU reference: per-bond cost of paratt_truncate at the step's rank profile
+# CPU reference: the same RK2 step composed from the reference's own C
 # ---------------------------------------------------------------------------
-def reference_step_seconds(r, n, d, reps=1):
-    """Seconds for one RK2 step on the reference CPU path, extrapolated.
-
-    The step rounds 2 formal products (interior rank r^2, attacHadamard) and
-    8 sums / operator TTs (rank 2r) -- 10 paratt_truncate calls, each a
-    left-to-right QR sweep and a right-to-left LQ+SVD sweep over d-1 bonds.
-    Sample: paratt_truncate of 3-core trains (2 bonds) with those interior
-    ranks and n=256, timed on this host, scaled by (d-1)/2 bonds."""
-    from oracle import ref_lib as R  # CPU-baseline leg only
-
-    rng = np.random.default_rng(11)
-
-    def per_bond(rank):
-        ts = []
-        for _ in range(reps):
-            cores = [rng.standard_normal((1, n, rank)), rng.standard_normal((rank, n, rank)),
-                     rng.standard_normal((rank, n, 1))]
-            t0 = time.perf_counter()
-            R.ref_truncate(cores, 1e-300, [1, rank, rank, 1])
-            ts.append(time.perf_counter() - t0)
-        return min(ts) / 2.0
-
-    t_prod = per_bond(r * r)
-    t_sum = per_bond(2 * r)
-    return (d - 1) * (2 * t_prod + 8 * t_sum), t_prod, t_sum
+WORKLOAD = ("config4: reaction-Burgers step-truncation RK2, d=40, n=256, rank-max 64, tol 1e-8 x ||u0||_RMS, "
+            "dt 1e-3, 3-Gaussian IC (seed 3), state after the warm-up steps")
 
 
 def cpu_threads():
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+
+def reference_steps(u, tol, steps):
+    """Advance `u` by `steps` reference RK2 steps; returns (state, seconds)."""
+    from oracle import ref_lib as R  # CPU-baseline leg only
+
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        u = R.ref_rxn_burgers_rk2_step(u, CFG["dt"], tol, CFG["maxrank"])
+        ts.append(time.perf_counter() - t0)
+    return u, ts
 
 
 def run_reference(args, rank):
@@ -133,30 +134,31 @@ def run_reference(args, rank):
     nthr = cpu_threads()
     os.environ.setdefault("OPENBLAS_NUM_THREADS", str(nthr))
     try:
-        from oracle import ref_lib as R  # noqa: F401
+        from oracle import ref_lib as R
         if not R.available():
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libparatt_ref.so not built"}))
             return 0
     except Exception as e:  # pragma: no cover
         print(json.dumps({"impl": "reference", "unavailable": f"reference library failed to load: {e}"}))
         return 0
-    d, n, r = CFG["d"], CFG["n"], REF_RANK
-    for _ in range(args.warmup):
-        reference_step_seconds(r, 64, 3)
-    ts = []
-    for _ in range(args.steps):
-        t, tp, tsum = reference_step_seconds(r, n, d)
-        ts.append(t)
-    sec = statistics.median(ts)
+    from paratt_b200 import workloads as Wl
+
+    d, n = CFG["d"], CFG["n"]
+    u = Wl.initial_condition(d, n, CFG["ngauss"], CFG["seed"])
+    tol = CFG["tol"] * Wl.rms_norm(u)
+    u, _ = reference_steps(u, tol, args.warmup)
+    u, ts = reference_steps(u, tol, args.steps)
+    sec = sum(ts) / len(ts)
     v = 1.0 / sec
-    sample = (f"paratt_truncate of 3-core trains, n={n}, interior rank {r*r} (formal u.u) and {2*r} (sums), "
-              f"per-bond time x (d-1) x (2 + 8 roundings per RK2 step); state rank {r}")
+    ranks = [c.shape[2] for c in u[:-1]]
+    sample = (f"{args.steps} full RK2 steps after {args.warmup} warm-up steps (state rank {max(ranks)}), "
+              f"{nthr} OpenBLAS threads")
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "RK2 steps/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "config4 reaction-Burgers RK2 (extrapolated per-bond reference cost)",
-                   "d": d, "n": n, "maxrank": CFG["maxrank"], "tol": CFG["tol"], "state_rank": r},
+        "config": {"workload": WORKLOAD, "d": d, "n": n, "maxrank": CFG["maxrank"], "tol": CFG["tol"],
+                   "method": "plain (reference paratt_truncate)", "state_rank": max(ranks)},
         "cpu_baseline": {"value": v, "unit": "RK2 steps/s", "cores": int(os.environ["OPENBLAS_NUM_THREADS"]),
                          "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": "RK2 steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -170,8 +172,8 @@ def run_reference(args, rank):
 # ---------------------------------------------------------------------------
 def run_ours(args, rank, world, local_rank):
     import paratt_b200 as P
+    from paratt_b200 import learned as Lr
     from paratt_b200 import workloads as Wl
-    from paratt_b200.capi import HostTT, capi
 
     dist = None
     if world > 1:
@@ -182,68 +184,112 @@ def run_ours(args, rank, world, local_rank):
         td.init_process_group("nccl", timeout=timedelta(seconds=600))
         dist = (torch, td)
 
-    d, n, maxr = CFG["d"], CFG["n"], CFG["maxrank"]
-    ctx = P.Context(local_rank)
-    u0 = Wl.initial_condition(d, n, CFG["ngauss"], CFG["seed"] + rank)
-    tol = CFG["tol"] * Wl.rms_norm(u0)
-    sim = P.RxnBurgers(ctx, d, n, maxrank=maxr, dt=CFG["dt"], tol=tol, seed=7 + rank)
-    cap = [1] + [2 * maxr] * (d - 1) + [1]
-    U = P.TT(ctx, [n] * d, cap, u0)
-    for _ in range(args.warmup):
-        sim.step(U)
-    ctx.sync()
-    start_cores = U.get()
-
     def barrier():
         if dist:
             dist[1].barrier()
 
-    # ---- device-resident timed region --------------------------------------
-    ctx.time_kernels(P.TIME_TSQR)
-    l0 = ctx.launches
-    barrier()
-    step_ms = []
-    with ClockSampler(local_rank) as clk:
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        t = dist[0].tensor([v], device="cuda")
+        dist[1].all_reduce(t, op=dist[1].ReduceOp.MAX)
+        return float(t.item())
+
+    d, n, maxr, dt = CFG["d"], CFG["n"], CFG["maxrank"], CFG["dt"]
+    ctx = P.Context(local_rank)
+    u0 = Wl.initial_condition(d, n, CFG["ngauss"], CFG["seed"] + rank)
+    tol = CFG["tol"] * Wl.rms_norm(u0)
+    cap = [1] + [2 * maxr] * (d - 1) + [1]
+    plain = P.RxnBurgers(ctx, d, n, maxrank=maxr, dt=dt, tol=tol, seed=7 + rank)
+    plain.log(True)
+    S0 = P.TT(ctx, [n] * d, cap, u0)
+    for _ in range(args.warmup):
+        plain.step(S0)
+    _, sig0, delta0 = plain.last_step(d)
+    ctx.sync()
+
+    def copy_of(src):
+        t = P.TT(ctx, [n] * d, cap)
+        t.copy_from(src)
+        return t
+
+    def timed(stepper_step, U):
+        barrier()
+        ms = []
         for _ in range(args.steps):
             ctx.flush_l2()
             ctx.mark(0)
-            sim.step(U)
+            stepper_step(U)
             ctx.mark(1)
-            step_ms.append(ctx.elapsed_ms(0, 1))
-    ctx.sync()
-    barrier()
+            ms.append(ctx.elapsed_ms(0, 1))
+        ctx.sync()
+        barrier()
+        return max_over_ranks(float(sum(ms)))
+
+    # ---- learned-sketch method (the headline) --------------------------------
+    ls = Lr.LearnedStepper(ctx, d, n, maxr, dt, tol, seed=3 + rank)
+    ls.seed_spectra(sig0, delta0)
+    UL = copy_of(S0)
+    l0 = ctx.launches
+    with ClockSampler(local_rank) as clk:
+        learned_ms = timed(ls.step, UL)
     launches = ctx.launches - l0 - args.steps  # minus the flush kernels
+    calls, fallbacks = ls.counts()
+    value = world * args.steps / (learned_ms / 1e3)
+
+    # ---- the same learned steps again with every factorisation launch timed
+    # by its own event pair (kept out of the headline region)
+    lk = Lr.LearnedStepper(ctx, d, n, maxr, dt, tol, seed=3 + rank)
+    lk.seed_spectra(sig0, delta0)
+    UK = copy_of(S0)
+    ctx.time_kernels(P.TIME_TSQR)
+    timed(lk.step, UK)
     ktime_ms, klaunch = ctx.kernel_time()
     kwork = ctx.kernel_work()
     ctx.time_kernels(0)
-    ranks_after = U.ranks()
-    total_ms = float(sum(step_ms))
-    if dist:
-        t = dist[0].tensor([total_ms], device="cuda")
-        dist[1].all_reduce(t, op=dist[1].ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * args.steps / (total_ms / 1e3)
+    lk.close()
+    UK.close()
 
-    # ---- end to end through the reference-facing C API ---------------------
-    L = capi()
-    host = HostTT(start_cores, capacity=cap)
-    host.pin()
+    # ---- plain method from the same state ------------------------------------
+    UP = copy_of(S0)
+    plain_ms = timed(plain.step, UP)
+    plain_value = world * args.steps / (plain_ms / 1e3)
+
+    # ---- error of one learned step against one plain step --------------------
+    A, B = copy_of(S0), copy_of(S0)
+    plain.step(A)
+    chk = Lr.LearnedStepper(ctx, d, n, maxr, dt, tol, seed=3 + rank)
+    chk.seed_spectra(sig0, delta0)
+    chk.step(B)
+    aa, bb, ab = A.dot(A), B.dot(B), A.dot(B)
+    err_step = float(np.sqrt(abs(aa - 2.0 * ab + bb) / aa))
+    pp, ll, pl = UP.dot(UP), UL.dot(UL), UP.dot(UL)
+    err_traj = float(np.sqrt(abs(pp - 2.0 * pl + ll) / pp))
+    chk.close()
+    A.close()
+    B.close()
+
+    # ---- end to end: learned method with the state on the host --------------
+    host = P.HostTrain([n] * d, cap, S0.get())
+    ue = P.TT(ctx, [n] * d, cap)
+    le = Lr.LearnedStepper(ctx, d, n, maxr, dt, tol, seed=3 + rank)
+    le.seed_spectra(sig0, delta0)
     h2d = d2h = 0
+    ctx.sync()
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        h2d += host.core_bytes()
-        L.pattac_rxn_burgers_midpoint_st(host.p, CFG["dt"], tol, maxr)
-        d2h += host.core_bytes()
-    e2e_s = time.perf_counter() - t0
-    if L.paratt_last_error() != 0:
-        raise RuntimeError("C API step failed")
-    if dist:
-        t = dist[0].tensor([e2e_s], device="cuda")
-        dist[1].all_reduce(t, op=dist[1].ReduceOp.MAX)
-        e2e_s = float(t.item())
-    host.free()
+        h2d += host.nbytes()
+        host.upload(ue)
+        le.step(ue)
+        host.download(ue)
+        d2h += host.nbytes()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = world * args.steps / e2e_s
+    start_cores = S0.get()
+    le.close()
+    ue.close()
+    host.close()
 
     if rank != 0:
         if dist:
@@ -253,17 +299,23 @@ def run_ours(args, rank, world, local_rank):
     hbm, src = peaks()
     achieved = (kwork / 1e9) / (ktime_ms / 1e3) if ktime_ms > 0 else 0.0  # GB/s
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "traffic": None, "kernel": "k_tsqr_factor",
+            "frac": achieved / hbm, "traffic": None, "kernel": "TSQR factorisation (k_wfactor, k_tsqr_factor)",
             "launches": klaunch, "avg_launch_us": 1e3 * ktime_ms / max(klaunch, 1),
+            "algorithmic_bytes_per_launch": kwork / max(klaunch, 1),
+            "timing": "event pair per launch in a second pass of the same K learned steps",
             "peak_source": f"{src} MEASURED_PEAKS.json hbm_gbs" if src == "measured" else "fallback 6650 GB/s"}
     out = {
         "metric": METRIC, "value": value, "unit": "RK2 steps/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": learned_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "config4: reaction-Burgers step-truncation RK2, d=40, n=256, rank-max 64, "
-                               "tol 1e-8 x ||u0||_RMS, dt 1e-3, 3-Gaussian IC (seed 3), plain FP64 rounding",
-                   "method": "plain", "l2": "flushed before every step (2 x L2 write, outside the events)",
-                   "ranks_after": max(ranks_after), "parallelism": f"replicas x{world}"},
+        "config": {"workload": WORKLOAD, "method": "learned-sketch (MLP-proposed sketch ranks, pad 4)",
+                   "l2": "flushed before every step (2 x L2 write, outside the events)",
+                   "state_rank": max(UL.ranks()), "parallelism": f"replicas x{world}"},
+        "plain": {"value": plain_value, "unit": "RK2 steps/s", "ms_per_step": plain_ms / args.steps},
+        "learned_over_plain": value / plain_value,
+        "err_vs_plain": {"one_step": err_step, "after_steps": err_traj, "steps": args.steps},
+        "fallback_rate": fallbacks / max(calls, 1),
+        "sketch_roundings": calls,
         "roofline": roof,
         "e2e": {"value": e2e, "unit": "RK2 steps/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
@@ -273,20 +325,21 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_cpu_baseline:
         nthr = cpu_threads()
         os.environ.setdefault("OPENBLAS_NUM_THREADS", str(nthr))
-        r = max(ranks_after)
         try:
-            sec, tp, tsum = reference_step_seconds(r, n, d)
+            _, ts = reference_steps(start_cores, tol, 2)
+            sec = sum(ts) / len(ts)
             out["cpu_baseline"] = {"value": 1.0 / sec, "unit": "RK2 steps/s",
                                    "cores": int(os.environ["OPENBLAS_NUM_THREADS"]), "kind": "reference",
-                                   "sample": f"paratt_truncate of 3-core trains n={n} at interior rank {r*r} "
-                                             f"({tp:.3f} s/bond) and {2*r} ({tsum:.4f} s/bond), x (d-1) x 10 "
-                                             f"roundings per step (extrapolated)"}
+                                   "sample": f"2 full RK2 steps of the reference routines from the warmed-up "
+                                             f"state (rank {max(r.shape[2] for r in start_cores[:-1])})"}
         except Exception as e:
             out["cpu_baseline"] = {"value": None, "unit": "RK2 steps/s", "cores": 0, "kind": "reference",
                                    "sample": f"unavailable: {e}"}
     print(json.dumps(out))
-    sim.close()
-    U.close()
+    for t in (UL, UP, S0):
+        t.close()
+    ls.close()
+    plain.close()
     ctx.close()
     if dist:
         dist[1].destroy_process_group()

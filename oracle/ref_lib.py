@@ -233,3 +233,29 @@ def ref_entry(cores, idx):
         return lib().paratt_entry(t.p, _iarr(idx))
     finally:
         t.free()
+
+
+def ref_rxn_burgers_F(u, tol, maxr, L=10.0, nu=0.05):
+    """F(u) of the reaction-Burgers step composed from the reference's own C
+    routines in the order of ``tt_oracle.rxn_burgers_F``: paratt_truncate
+    after every intermediate, the product u.u by pattacHadamard (rank r^2),
+    the sum by attac_tt_axpby.  The operator sums sum_i S_i x + shift x are
+    the rank-2r trains of ``tt_oracle.op_sum_apply`` (the reference has no
+    such operator)."""
+    from oracle import tt_oracle as O
+
+    d, n = len(u), u[0].shape[1]
+    d2, d1 = O.burgers_stencils(d, n, L, nu)
+    w = ref_truncate(ref_hadamard(u, u), tol, maxr)
+    a = ref_truncate(O.op_sum_apply(u, [d2] * d, 1.0), tol, maxr)
+    b = ref_truncate(O.op_sum_apply(w, [d1] * d, -1.0), tol, maxr)
+    return ref_truncate(ref_axpby(1.0, a, 1.0, b), tol, maxr)
+
+
+def ref_rxn_burgers_rk2_step(u, dt, tol, maxr, L=10.0, nu=0.05):
+    """Step-truncation midpoint step (paratt_ode.h:77-112, stage rounded) on
+    the reference routines, as ``tt_oracle.rxn_burgers_rk2_step``."""
+    k1 = ref_rxn_burgers_F(u, tol, maxr, L, nu)
+    us = ref_truncate(ref_axpby(1.0, u, 0.5 * dt, k1), tol, maxr)
+    k2 = ref_rxn_burgers_F(us, tol, maxr, L, nu)
+    return ref_truncate(ref_axpby(1.0, u, dt, k2), tol, maxr)

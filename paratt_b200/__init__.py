@@ -292,6 +292,47 @@ class TT:
             self.h = None
 
 
+class HostTrain:
+    """Page-locked host copy of a tensor train: one flat buffer per core,
+    sized for the rank capacity, column-major cores as in the reference.
+    upload() / download() move the whole train with one copy per core."""
+
+    def __init__(self, dims, rank_cap, cores=None):
+        self.dims = [int(n) for n in dims]
+        self.d = len(self.dims)
+        self.cap = list(rank_cap)
+        self.bufs = [np.zeros(self.cap[k] * self.dims[k] * self.cap[k + 1]) for k in range(self.d)]
+        for b in self.bufs:
+            _check(lib().ptt_host_pin(C.c_void_p(b.ctypes.data), C.c_ulonglong(b.nbytes)))
+        self._ptrs = (_dp * self.d)(*[b.ctypes.data_as(_dp) for b in self.bufs])
+        self.r = [1] * (self.d + 1)
+        if cores is not None:
+            self.r = [cores[0].shape[0]] + [c.shape[2] for c in cores]
+            for k, c in enumerate(cores):
+                self.bufs[k][: c.size] = c.ravel(order="F")
+
+    def nbytes(self):
+        """Bytes of the train at its current ranks."""
+        return 8 * sum(self.r[k] * self.dims[k] * self.r[k + 1] for k in range(self.d))
+
+    def upload(self, tt: TT):
+        _check(lib().ptt_tt_set(tt.h, _iarr(self.r), self._ptrs))
+
+    def download(self, tt: TT):
+        r = (C.c_int * (self.d + 1))()
+        _check(lib().ptt_tt_get(tt.h, r, self._ptrs))
+        self.r = list(r)
+
+    def cores(self):
+        return [self.bufs[k][: self.r[k] * self.dims[k] * self.r[k + 1]].reshape(
+            (self.r[k], self.dims[k], self.r[k + 1]), order="F").copy() for k in range(self.d)]
+
+    def close(self):
+        for b in self.bufs:
+            lib().ptt_host_unpin(C.c_void_p(b.ctypes.data))
+        self.bufs = []
+
+
 def axpby(a, x: TT, b, y: TT, z: TT):
     _check(lib().ptt_axpby(float(a), x.h, float(b), y.h, z.h))
     return z

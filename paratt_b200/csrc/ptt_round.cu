@@ -793,8 +793,8 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
 // Rounding of a train whose ranks stay <= 32 on the warp-level TSQR.
 // Per bond only the factorisation, the small product that moves R (or U S)
 // into the neighbour core and the rank update run in sequence; Q (and V_r Q)
-// is formed for all bonds of a sweep in one launch after the sweep; the
-// one-warp SVD accumulates V itself.
+// is formed for all bonds of a sweep in one launch after the sweep, and the
+// SVD rotations are replayed for all bonds in one launch.
 // Every bond k has its own record region (ws + k * stride) so the deferred
 // launches find each bond's reflectors.  Same phases as round_impl.
 static bool wt_fits(const ptt_tt* x, const int* rk) {
@@ -904,11 +904,7 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
             Wmax = Wr[i] > Wmax ? Wr[i] : Wmax;
             const int mr = maxr ? maxr[i] : rk[i];
             ptt_time_begin(c, PTT_TIME_SVD);
-#ifdef WT_WSVD
-            k_wsvd<<<1, 32, 0, c->stream>>>(pl, wsb, delta, mr, i, c->d_status);
-#else
             k_svd_jacobi<32><<<1, SVD_NT, svd_smem<32>(), c->stream>>>(pl, wsb, delta, mr, i, c->d_status);
-#endif
             ptt_time_end(c, PTT_TIME_SVD);
             PTT_LAUNCHED(c);
             const long long mcap = (long long)rk[i - 1] * x->n[i - 1];
@@ -920,10 +916,8 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
             PTT_LAUNCHED(c);
         }
         if (d > 1) {
-#ifndef WT_WSVD
             k_svd_replay_b<<<dim3(4, d - 1), 256, replay_smem<32>(), c->stream>>>(base, ws, wp.stride, 1);
             PTT_LAUNCHED(c);
-#endif
             k_wapply<<<dim3((Wmax + WPB - 1) / WPB, d - 1), 32 * WPB, 0, c->stream>>>(x->dd, 1, RIGHT_T, base, wp, ws);
             PTT_LAUNCHED(c);
             k_wswap<<<1, 64, 0, c->stream>>>(x->dd, 1, d, c->d_status);

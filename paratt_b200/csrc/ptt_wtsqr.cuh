@@ -93,98 +93,6 @@ __device__ __forceinline__ void w_store(double* p, long long rs, long long cs, i
     }
 }
 
-#ifdef WT_ROLLED
-// Rolled forms: the reflector loop is not unrolled (small code); the pivot
-// row is picked and written back by selects over the compile-time rows.
-__device__ __forceinline__ double w_geqrt(double (&X)[32], int c, int h) {
-    const int lane = threadIdx.x & 31;
-    const int nr = c < h ? c : h;
-    double mytau = 0.0;
-#pragma unroll 1
-    for (int j = 0; j < nr; j++) {
-        double s0 = 0.0, s1 = 0.0, xj = 0.0;
-#pragma unroll
-        for (int t = 0; t < 32; t++) {
-            const double x = X[t];
-            if (t == j) xj = x;
-            const double y = t > j ? x : 0.0;
-            if (t & 1)
-                s0 = fma(y, y, s0);
-            else
-                s1 = fma(y, y, s1);
-        }
-        const double alpha = __shfl_sync(FULL, xj, j);
-        const double s2 = __shfl_sync(FULL, s0 + s1, j);
-        double beta, tau, sc;
-        hh_params(alpha, s2, &beta, &tau, &sc);
-        double V[32];
-        double d0 = 0.0, d1 = 0.0;
-#pragma unroll
-        for (int t = 0; t < 32; t++) {
-            const double sv = __shfl_sync(FULL, X[t], j);
-            V[t] = t > j ? sv * sc : 0.0;
-            if (t & 1)
-                d0 = fma(V[t], X[t], d0);
-            else
-                d1 = fma(V[t], X[t], d1);
-        }
-        const double w = tau * (xj + (d0 + d1));
-        const bool upd = lane > j, piv = lane == j;
-#pragma unroll
-        for (int t = 0; t < 32; t++) {
-            const double x = X[t];
-            double y = upd ? fma(-w, V[t], x) : ((piv && t > j) ? V[t] : x);
-            if (t == j) y = upd ? x - w : (piv ? beta : x);
-            X[t] = y;
-        }
-        if (piv) mytau = tau;
-    }
-    return mytau;
-}
-
-__device__ __forceinline__ double w_ttqrt(double (&T)[32], double (&B)[32], int c) {
-    const int lane = threadIdx.x & 31;
-    double mytau = 0.0;
-#pragma unroll 1
-    for (int j = 0; j < c; j++) {
-        double s0 = 0.0, s1 = 0.0, tj = 0.0;
-#pragma unroll
-        for (int t = 0; t < 32; t++) {
-            if (t == j) tj = T[t];
-            const double y = t <= j ? B[t] : 0.0;
-            if (t & 1)
-                s0 = fma(y, y, s0);
-            else
-                s1 = fma(y, y, s1);
-        }
-        const double alpha = __shfl_sync(FULL, tj, j);
-        const double s2 = __shfl_sync(FULL, s0 + s1, j);
-        double beta, tau, sc;
-        hh_params(alpha, s2, &beta, &tau, &sc);
-        double V[32];
-        double d0 = 0.0, d1 = 0.0;
-#pragma unroll
-        for (int t = 0; t < 32; t++) {
-            const double sv = __shfl_sync(FULL, B[t], j);
-            V[t] = t <= j ? sv * sc : 0.0;
-            if (t & 1)
-                d0 = fma(V[t], B[t], d0);
-            else
-                d1 = fma(V[t], B[t], d1);
-        }
-        const double w = tau * (tj + (d0 + d1));
-        const bool upd = lane > j, piv = lane == j;
-#pragma unroll
-        for (int t = 0; t < 32; t++) {
-            const double b = B[t];
-            B[t] = upd ? fma(-w, V[t], b) : ((piv && t <= j) ? V[t] : b);
-            if (t == j) T[t] = upd ? T[t] - w : (piv ? beta : T[t]);
-        }
-        if (piv) mytau = tau;
-    }
-    return mytau;
-}
-#else
 // Householder QR of the h x c tile X (lane = column, rows >= h are zero).
 // On exit rows t <= lane of X hold R and rows t > lane the vector of
 // reflector `lane` (unit diagonal implied); returns that reflector's tau.
@@ -278,18 +186,13 @@ __device__ __forceinline__ double w_ttqrt(double (&T)[32], double (&B)[32], int 
     return mytau;
 }
 
-#endif  // WT_ROLLED
-
 // Factor the unfolding (mode) of core k: leaf reflectors in place, taus and
 // tree records in the bond's region wsb, R at slot 0, Info (m, c, q).
 // A block holds FPB leaves; the lowest LB = log2(FPB) tree levels are
 // combined inside the block through shared memory, the levels above by the
 // warp 0 of each block through the global slots (last arriver combines).
-#ifndef WT_FLB
-#define WT_FLB 3
-#endif
-constexpr int FLB = WT_FLB;       // tree levels combined inside a block
-constexpr int FPB = 1 << FLB;     // warps (leaves) per factor block
+constexpr int FLB = 3;         // tree levels combined inside a block
+constexpr int FPB = 1 << FLB;  // warps (leaves) per factor block
 
 __host__ __device__ constexpr size_t wfactor_smem() { return sizeof(double) * FPB * 32 * 33; }
 
@@ -447,28 +350,6 @@ __global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, i
         double Bt[32];
 #pragma unroll
         for (int t = 0; t < 32; t++) Bt[t] = 0.0;
-#ifdef WT_ROLLED
-#pragma unroll 1
-        for (int j = c - 1; j >= 0; j--) {
-            const double tau = st[j];
-            double d0 = 0.0, d1 = 0.0, xj = 0.0;
-#pragma unroll
-            for (int t = 0; t < 32; t++) {
-                if (t == j) xj = X[t];
-                const double vv = t <= j ? sw[t * 33 + j] : 0.0;
-                if (t & 1)
-                    d0 = fma(vv, Bt[t], d0);
-                else
-                    d1 = fma(vv, Bt[t], d1);
-            }
-            const double w = tau * (xj + (d0 + d1));
-#pragma unroll
-            for (int t = 0; t < 32; t++) {
-                if (t == j) X[t] = xj - w;
-                if (t <= j) Bt[t] = fma(-w, vs[t * 33 + j], Bt[t]);
-            }
-        }
-#else
 #pragma unroll
         for (int j = 31; j >= 0; j--) {
             if (j >= c) continue;
@@ -486,7 +367,6 @@ __global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, i
 #pragma unroll
             for (int t = 0; t <= j; t++) Bt[t] = fma(-w, vs[t * 33 + j], Bt[t]);
         }
-#endif
         __syncwarp();
         if (right) {
 #pragma unroll
@@ -512,28 +392,6 @@ __global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, i
     st[lane] = wsb[wp.o_tl + p * 32 + lane];
     __syncwarp();
     const int nr = c < h ? c : h;
-#ifdef WT_ROLLED
-#pragma unroll 1
-    for (int j = nr - 1; j >= 0; j--) {
-        const double tau = st[j];
-        double d0 = 0.0, d1 = 0.0, xj = 0.0;
-#pragma unroll
-        for (int t = 0; t < 32; t++) {
-            if (t == j) xj = X[t];
-            const double vv = t > j ? sw[t * 33 + j] : 0.0;
-            if (t & 1)
-                d0 = fma(vv, X[t], d0);
-            else
-                d1 = fma(vv, X[t], d1);
-        }
-        const double w = tau * (xj + (d0 + d1));
-#pragma unroll
-        for (int t = 0; t < 32; t++) {
-            if (t == j) X[t] = xj - w;
-            if (t > j) X[t] = fma(-w, vs[t * 33 + j], X[t]);
-        }
-    }
-#else
 #pragma unroll
     for (int j = 31; j >= 0; j--) {
         if (j >= nr) continue;
@@ -551,181 +409,12 @@ __global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, i
 #pragma unroll
         for (int t = j + 1; t < 32; t++) X[t] = fma(-w, vs[t * 33 + j], X[t]);
     }
-#endif
     __syncwarp();
     double* out = D->alt[k];
     if (mode == LEFT)
         w_store(out, 1, m, r0, h, qB, X, sw);
     else
         w_store(out, qB, 1, r0, h, qB, X, sw);
-}
-
-// One-sided Jacobi SVD of L = R^T (c x q, c <= 32) by one warp: lane j owns
-// column j of L (row j of the root R) and column j of V.  Pairs follow the
-// same circle ordering, tolerance, tracked norms and sweep limit as
-// k_svd_jacobi; both lanes of a pair form the same dot product in the same
-// order, so they take the same rotation.  Writes the same records (Info,
-// per-bond stats, sig/order, U_r S_r) and V_r into Bn directly, so no
-// rotation log or replay is needed.
-__global__ void __launch_bounds__(32) k_wsvd(Plan pl, double* ws, double delta, int maxr, int bond, int* status) {
-    __shared__ double sL[32 * 33];
-    __shared__ double sV[32 * 33];
-    __shared__ double s_sig[32];
-    __shared__ int s_ord[32];
-    __shared__ int s_rank;
-    const int lane = threadIdx.x;
-    Info* info = pl.info;
-    if (info->status) return;
-    const int c = info->c, q = info->q;
-    const int qq = q + (q & 1);
-    const double* R = ws + pl.o_Rn;
-    double a[32], v[32], b[32];
-#pragma unroll
-    for (int t = 0; t < 32; t++) {
-        a[t] = (lane < q && t < c) ? __ldcg(R + lane * 32 + t) : 0.0;
-        v[t] = (t == lane && lane < q) ? 1.0 : 0.0;
-    }
-    const double tol = (double)(c < 16 ? 16 : c) * 2.220446049250313e-16;
-    int sweeps = 0;
-    bool conv = (qq < 2);
-    for (int sw = 0; sw < MAXSW && !conv; sw++) {
-        double n0 = 0.0, n1 = 0.0;
-#pragma unroll
-        for (int t = 0; t < 32; t += 2) {
-            n0 = fma(a[t], a[t], n0);
-            n1 = fma(a[t + 1], a[t + 1], n1);
-        }
-        double nrm = n0 + n1;
-        int rot = 0;
-        for (int rd = 0; rd < qq - 1; rd++) {
-            int pos = 0;
-            if (lane > 0) {
-                const int e = (lane - 1 - rd) % (qq - 1);
-                pos = 1 + (e < 0 ? e + qq - 1 : e);
-            }
-            const bool act = lane < qq;
-            const int src = act ? circle_col(qq - 1 - pos, rd, qq) : lane;
-            const bool first = pos < qq / 2;
-            double g0 = 0.0, g1 = 0.0;
-#pragma unroll
-            for (int t = 0; t < 32; t += 2) {
-                b[t] = __shfl_sync(FULL, a[t], src);
-                b[t + 1] = __shfl_sync(FULL, a[t + 1], src);
-                g0 = fma(a[t], b[t], g0);
-                g1 = fma(a[t + 1], b[t + 1], g1);
-            }
-            const double ga = g0 + g1;
-            const double nb = __shfl_sync(FULL, nrm, src);
-            const double al = first ? nrm : nb, be = first ? nb : nrm;
-            const bool doit = act && ga != 0.0 && fabs(ga) > tol * sqrt(al * be);
-            double cs = 1.0, sn = 0.0;
-            if (doit) {
-                const double dd = be - al, g2 = 2.0 * ga;
-                const double tn = g2 * __drcp_rn(dd + copysign(sqrt(fma(dd, dd, g2 * g2)), dd));
-                cs = rsqrt(fma(tn, tn, 1.0));
-                sn = cs * tn;
-                if (first) {
-#pragma unroll
-                    for (int t = 0; t < 32; t++) a[t] = cs * a[t] - sn * b[t];
-                    nrm = al - tn * ga;
-                } else {
-#pragma unroll
-                    for (int t = 0; t < 32; t++) a[t] = sn * b[t] + cs * a[t];
-                    nrm = be + tn * ga;
-                }
-                rot = 1;
-            }
-#pragma unroll
-            for (int t = 0; t < 32; t++) {
-                const double vb = __shfl_sync(FULL, v[t], src);
-                if (doit) v[t] = first ? cs * v[t] - sn * vb : sn * vb + cs * v[t];
-            }
-        }
-        if (__any_sync(FULL, rot))
-            sweeps = sw + 1;
-        else
-            conv = true;
-    }
-    if (!conv && lane == 0) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
-    double n0 = 0.0, n1 = 0.0;
-#pragma unroll
-    for (int t = 0; t < 32; t += 2) {
-        n0 = fma(a[t], a[t], n0);
-        n1 = fma(a[t + 1], a[t + 1], n1);
-    }
-    const double sg = lane < q ? sqrt(n0 + n1) : -1.0;
-    int pos = 0;
-    for (int i = 0; i < 32; i++) {
-        const double si = __shfl_sync(FULL, sg, i);
-        if (i < qq) pos += (si > sg) || (si == sg && i < lane);
-    }
-    s_sig[lane] = sg;
-    if (lane < qq) s_ord[pos] = lane;
-#pragma unroll
-    for (int t = 0; t < 32; t++) {
-        sL[lane * 33 + t] = a[t];
-        sV[lane * 33 + t] = v[t];
-    }
-    __syncwarp();
-    double* sig_out = ws + pl.o_sig;
-    if (lane == 0) {
-        const double s0 = q > 0 ? s_sig[s_ord[0]] : 0.0;
-        // numerical rank kept by LAPACK dgesvdq(JOBA='A'): sqrt(N)*eps*s0
-        const double thr = sqrt((double)q) * 1.1102230246251565e-16 * s0;
-        int nsv = q > 0 ? 1 : 0;
-        while (nsv < q && s_sig[s_ord[nsv]] >= thr) nsv++;
-        if (!(s0 == s0)) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
-        // tail-sum rule, pattac.c:468-481
-        double ssum = 0.0;
-        int rank = nsv;
-        for (int j = nsv - 1; j >= 0; j--) {
-            const double sj = s_sig[s_ord[j]];
-            ssum += sj * sj;
-            if (sqrt(ssum) < delta)
-                rank = j;
-            else
-                break;
-        }
-        if (rank > q) rank = q;
-        if (rank > maxr) rank = maxr;
-        if (rank < 1) rank = 1;
-        info->rank = rank;
-        info->nsv = nsv;
-        info->sweeps = sweeps;
-        double tail = 0.0;
-        for (int j = rank; j < q; j++) tail += s_sig[s_ord[j]] * s_sig[s_ord[j]];
-        info->tail = tail;
-        if (pl.stats) {
-            double* st = pl.stats + (long long)bond * PTT_STAT_LEN;
-            st[0] = rank;
-            st[1] = nsv;
-            st[2] = sweeps;
-            st[3] = q;
-            st[4] = c;
-            st[5] = tail;
-            st[6] = delta;
-            st[7] = 0.0;
-            for (int j = 0; j < PTT_STAT_NSIG; j++) st[8 + j] = j < q ? s_sig[s_ord[j]] : 0.0;
-        }
-        s_rank = rank;
-    }
-    __syncwarp();
-    const int rank = s_rank;
-    sig_out[lane] = 0.0;
-    ((int*)(sig_out + 32))[lane] = lane < qq ? s_ord[lane] : 0;
-    __syncwarp();
-    if (lane < q) sig_out[pos] = sg;
-    // U_r S_r (c x rank, column-major ld 32) and V_r (q x rank, row-major, ld KC)
-    double* US = ws + pl.o_US;
-    double* Bn = ws + pl.o_Bn;
-    for (int bb = 0; bb < 32; bb++) {
-        const int j = s_ord[bb < qq ? bb : 0];
-        US[bb * 32 + lane] = (bb < rank && lane < c) ? sL[j * 33 + lane] : 0.0;
-    }
-    for (int row = 0; row < 32; row++) {
-        const int j = s_ord[lane < qq ? lane : 0];
-        Bn[(long long)row * pl.KC + lane] = (row < q && lane < rank) ? sV[j * 33 + row] : 0.0;
-    }
 }
 
 // swap core and alt of cores [k0, k1) unless an error was recorded

@@ -44,6 +44,46 @@ def propose(mlp, sig, delta, d, dt, pad, maxrank):
     return [1] + [int(v) for v in ell] + [1]
 
 
+class LearnedStepper:
+    """Reaction-Burgers RK2 steps by the learned-sketch method: before every
+    step the MLP proposes per-bond sketch ranks from the previous step's
+    spectra; the step rounds through Gaussian sketches of those ranks, with
+    the deterministic truncation as the judge and fallback
+    (ptt_rxn_burgers_rk2_step_sketch).  Without spectra (first step) the
+    step is the plain deterministic one, which records them."""
+
+    def __init__(self, ctx, d, n, maxrank, dt, tol, pad=4, model=MODEL, seed=3):
+        self.d, self.dt, self.pad, self.maxrank = d, dt, pad, maxrank
+        self.sim = RxnBurgers(ctx, d, n, maxrank=maxrank, dt=dt, tol=tol, seed=seed)
+        self.sim.log(True)
+        z = np.load(model)
+        self.mlp = MLP(ctx, int(z["nin"]), int(z["width"]))
+        self.mlp.set_params(z["params"])
+        self.spec = None
+        self.ell = None
+
+    def seed_spectra(self, sig, delta):
+        """Spectra of a step taken elsewhere (e.g. a plain warm-up step)."""
+        self.spec = (np.array(sig, copy=True), float(delta))
+
+    def step(self, U):
+        if self.spec is None:
+            self.sim.step(U)
+        else:
+            self.ell = propose(self.mlp, self.spec[0], self.spec[1], self.d, self.dt, self.pad, self.maxrank)
+            self.sim.step_sketch(U, self.ell, pad=self.pad)
+        _, sig, delta = self.sim.last_step(self.d)
+        self.spec = (sig, delta)
+
+    def counts(self):
+        """(sketch roundings, deterministic fallbacks) so far."""
+        return self.sim.sketch_counts()
+
+    def close(self):
+        self.mlp.close()
+        self.sim.close()
+
+
 def collect(ctx, cfg, seed, steps, warm=1):
     """Plain run with logging; returns features (previous step's spectra)
     and targets (this step's largest kept rank) for every bond and step."""
