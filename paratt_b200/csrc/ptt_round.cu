@@ -814,7 +814,9 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
     if (rc) return rc;
     static bool wattr = false;
     if (!wattr) {
-        PTT_CUDA(cudaFuncSetAttribute(k_wfactor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wfactor_smem()));
+        PTT_CUDA(cudaFuncSetAttribute(k_wfactor<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wfactor_smem()));
+        PTT_CUDA(cudaFuncSetAttribute(k_wfactor<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wfactor_smem()));
+        PTT_CUDA(cudaFuncSetAttribute(k_wfactor<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wfactor_smem()));
         wattr = true;
     }
     int Wl[PTT_MAX_DIM], Wr[PTT_MAX_DIM], Pcap = 1;
@@ -854,11 +856,32 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
         pl.info = (Info*)(*wsb + base.o_info_d);
         return pl;
     };
+    // column bound of the unrolled Householder loops: the bond's rank bound
+    auto cbound = [](int cols) { return cols <= 16 ? 16 : (cols <= 24 ? 24 : 32); };
     auto factor = [&](int i, int mode, int W, const Plan& pl, double* wsb) -> int {
+        const int cb = cbound(mode == LEFT ? rk[i + 1] : rk[i]);
+        const dim3 g((W + FPB - 1) / FPB), b(32 * FPB);
+        const size_t sm = wfactor_smem();
         ptt_time_begin(c, PTT_TIME_TSQR);
-        k_wfactor<<<(W + FPB - 1) / FPB, 32 * FPB, wfactor_smem(), c->stream>>>(x->dd, i, mode, pl, wp, wsb,
-                                                                                c->d_status);
+        if (cb == 16)
+            k_wfactor<16><<<g, b, sm, c->stream>>>(x->dd, i, mode, pl, wp, wsb, c->d_status);
+        else if (cb == 24)
+            k_wfactor<24><<<g, b, sm, c->stream>>>(x->dd, i, mode, pl, wp, wsb, c->d_status);
+        else
+            k_wfactor<32><<<g, b, sm, c->stream>>>(x->dd, i, mode, pl, wp, wsb, c->d_status);
         ptt_time_end(c, PTT_TIME_TSQR);
+        PTT_LAUNCHED(c);
+        return PTT_OK;
+    };
+    auto apply = [&](int k0, int nb, int mode, int Wmax, int cmax) -> int {
+        const int cb = cbound(cmax);
+        const dim3 g((Wmax + WPB - 1) / WPB, nb), b(32 * WPB);
+        if (cb == 16)
+            k_wapply<16><<<g, b, 0, c->stream>>>(x->dd, k0, mode, base, wp, ws);
+        else if (cb == 24)
+            k_wapply<24><<<g, b, 0, c->stream>>>(x->dd, k0, mode, base, wp, ws);
+        else
+            k_wapply<32><<<g, b, 0, c->stream>>>(x->dd, k0, mode, base, wp, ws);
         PTT_LAUNCHED(c);
         return PTT_OK;
     };
@@ -867,15 +890,15 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
         double* wsb;
         Plan pl = bond(i, &wsb);
         if ((rc = factor(i, LEFT, Wl[i], pl, wsb))) return rc;
-        k_wapply<<<dim3((Wl[i] + WPB - 1) / WPB, 1), 32 * WPB, 0, c->stream>>>(x->dd, i, LEFT, base, wp, ws);
-        PTT_LAUNCHED(c);
+        if ((rc = apply(i, 1, LEFT, Wl[i], rk[i + 1]))) return rc;
         k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i, -1, &pl.info->q, pl.info);
         PTT_LAUNCHED(c);
         return PTT_OK;
     }
     if (phases & 1) {
-        int Wmax = 1;
+        int Wmax = 1, cmax = 1;
         for (int i = 0; i < d - 1; i++) {
+            cmax = rk[i + 1] > cmax ? rk[i + 1] : cmax;
             double* wsb;
             Plan pl = bond(i, &wsb);
             if ((rc = factor(i, LEFT, Wl[i], pl, wsb))) return rc;
@@ -889,15 +912,15 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
             PTT_LAUNCHED(c);
         }
         if (d > 1) {
-            k_wapply<<<dim3((Wmax + WPB - 1) / WPB, d - 1), 32 * WPB, 0, c->stream>>>(x->dd, 0, LEFT, base, wp, ws);
-            PTT_LAUNCHED(c);
+            if ((rc = apply(0, d - 1, LEFT, Wmax, cmax))) return rc;
             k_wswap<<<1, 64, 0, c->stream>>>(x->dd, 0, d - 1, c->d_status);
             PTT_LAUNCHED(c);
         }
     }
     if (phases & 2) {
-        int Wmax = 1;
+        int Wmax = 1, cmax = 1;
         for (int i = d - 1; i >= 1; i--) {
+            cmax = rk[i] > cmax ? rk[i] : cmax;
             double* wsb;
             Plan pl = bond(i, &wsb);
             if ((rc = factor(i, RIGHT_T, Wr[i], pl, wsb))) return rc;
@@ -918,8 +941,7 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
         if (d > 1) {
             k_svd_replay_b<<<dim3(4, d - 1), 256, replay_smem<32>(), c->stream>>>(base, ws, wp.stride, 1);
             PTT_LAUNCHED(c);
-            k_wapply<<<dim3((Wmax + WPB - 1) / WPB, d - 1), 32 * WPB, 0, c->stream>>>(x->dd, 1, RIGHT_T, base, wp, ws);
-            PTT_LAUNCHED(c);
+            if ((rc = apply(1, d - 1, RIGHT_T, Wmax, cmax))) return rc;
             k_wswap<<<1, 64, 0, c->stream>>>(x->dd, 1, d, c->d_status);
             PTT_LAUNCHED(c);
         }

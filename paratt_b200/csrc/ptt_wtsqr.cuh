@@ -96,12 +96,13 @@ __device__ __forceinline__ void w_store(double* p, long long rs, long long cs, i
 // Householder QR of the h x c tile X (lane = column, rows >= h are zero).
 // On exit rows t <= lane of X hold R and rows t > lane the vector of
 // reflector `lane` (unit diagonal implied); returns that reflector's tau.
+template <int CB>
 __device__ __forceinline__ double w_geqrt(double (&X)[32], int c, int h) {
     const int lane = threadIdx.x & 31;
     const int nr = c < h ? c : h;
     double mytau = 0.0;
 #pragma unroll
-    for (int j = 0; j < 32; j++) {
+    for (int j = 0; j < CB; j++) {
         if (j >= nr) continue;
         double s0 = 0.0, s1 = 0.0;
 #pragma unroll
@@ -143,11 +144,12 @@ __device__ __forceinline__ double w_geqrt(double (&X)[32], int c, int h) {
 // [T; B] with T, B upper triangular (lane = column): eliminate B into T.
 // On exit T is the R of the pair and rows t <= lane of B hold the vector of
 // reflector `lane` (its top part is e_lane); returns that reflector's tau.
+template <int CB>
 __device__ __forceinline__ double w_ttqrt(double (&T)[32], double (&B)[32], int c) {
     const int lane = threadIdx.x & 31;
     double mytau = 0.0;
 #pragma unroll
-    for (int j = 0; j < 32; j++) {
+    for (int j = 0; j < CB; j++) {
         if (j >= c) continue;
         double s0 = 0.0, s1 = 0.0;
 #pragma unroll
@@ -196,6 +198,7 @@ constexpr int FPB = 1 << FLB;  // warps (leaves) per factor block
 
 __host__ __device__ constexpr size_t wfactor_smem() { return sizeof(double) * FPB * 32 * 33; }
 
+template <int CB>
 __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, int mode, Plan pl, WP wp,
                                                       double* wsb, int* status) {
     extern __shared__ double fsm[];
@@ -206,7 +209,7 @@ __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, i
     Info* info = (Info*)(wsb + pl.o_info_d);
     const int W = (m + 31) >> 5;
     const int P = pow2_ge(W);
-    if (c > 32 || c < 1 || m < 1 || P > wp.Pcap) {
+    if (c > CB || c < 1 || m < 1 || P > wp.Pcap) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             info->status = PTT_ERR_CAPACITY;
             PTT_STATUS_SET(status, PTT_ERR_CAPACITY);
@@ -223,7 +226,7 @@ __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, i
     double X[32];
     if (valid) {
         w_load(A.p, A.rs, A.cs, r0, h, c, X, sw);
-        const double tl = w_geqrt(X, c, h);
+        const double tl = w_geqrt<CB>(X, c, h);
         w_store(A.p, A.rs, A.cs, r0, h, c, X, sw);
         wsb[wp.o_tl + p * 32 + lane] = tl;
 #pragma unroll
@@ -246,12 +249,12 @@ __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, i
             const double* Rr = fsm + (wid + span) * (32 * 33);
             double B[32];
 #pragma unroll
-            for (int t = 0; t < 32; t++) B[t] = Rr[t * 32 + lane];
-            const double tn = w_ttqrt(X, B, c);
+            for (int t = 0; t < 32; t++) B[t] = t < CB ? Rr[t * 32 + lane] : 0.0;
+            const double tn = w_ttqrt<CB>(X, B, c);
             const int node = ((P + p) >> (lvl + 1)) - 1;
             double* Vo = Rs + (long long)(2 * node + 2) * SLOT;
 #pragma unroll
-            for (int t = 0; t < 32; t++) Vo[t * 32 + lane] = B[t];
+            for (int t = 0; t < CB; t++) Vo[t * 32 + lane] = B[t];
             wsb[wp.o_tn + node * 32 + lane] = tn;
         }
     }
@@ -270,7 +273,7 @@ __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, i
         }
         double* Ro = Rs + (long long)slot * SLOT;
 #pragma unroll
-        for (int t = 0; t < 32; t++) Ro[t * 32 + lane] = X[t];
+        for (int t = 0; t < CB; t++) Ro[t * 32 + lane] = X[t];
         __threadfence();
         int old = 0;
         if (lane == 0) old = atomicAdd(cnt + node, 1);
@@ -283,18 +286,18 @@ __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, i
         double B[32];
 #pragma unroll
         for (int t = 0; t < 32; t++) {
-            X[t] = __ldcg(Rl + t * 32 + lane);
-            B[t] = __ldcg(Rr + t * 32 + lane);
+            X[t] = t < CB ? __ldcg(Rl + t * 32 + lane) : 0.0;
+            B[t] = t < CB ? __ldcg(Rr + t * 32 + lane) : 0.0;
         }
-        const double tn = w_ttqrt(X, B, c);
+        const double tn = w_ttqrt<CB>(X, B, c);
 #pragma unroll
-        for (int t = 0; t < 32; t++) Rr[t * 32 + lane] = B[t];
+        for (int t = 0; t < CB; t++) Rr[t * 32 + lane] = B[t];
         wsb[wp.o_tn + node * 32 + lane] = tn;
         slot = node;
         lvl++;
     }
 #pragma unroll
-    for (int t = 0; t < 32; t++) Rs[t * 32 + lane] = X[t];
+    for (int t = 0; t < 32; t++) Rs[t * 32 + lane] = t < CB ? X[t] : 0.0;
     if (lane == 0) {
         info->m = m;
         info->c = c;
@@ -308,6 +311,7 @@ __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, i
 // with the sizes recorded by k_wfactor (the descriptor's ranks have moved on).
 //   LEFT:    B = I_q;                       out (m x q, column-major) -> alt[k]
 //   RIGHT_T: B = V_r (Bn, row-major 32 x KC); out(row, col) -> alt[k][row * rank + col]
+template <int CB>
 __global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, int mode, Plan pl, WP wp, double* ws) {
     __shared__ double sh[WPB][32 * 33];
     __shared__ double stau[WPB][32];
@@ -320,7 +324,7 @@ __global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, i
     const int qB = (mode == LEFT) ? q : info->rank;
     const int W = (m + 31) >> 5, P = pow2_ge(W);
     const int p = blockIdx.x * WPB + wid;
-    if (p >= W) return;
+    if (p >= W || c > CB) return;  // c <= CB: the factorisation used the same bound
     double* sw = sh[wid];
     volatile double* vs = sw;  // re-read in the updates instead of holding 32 values
     double* st = stau[wid];
@@ -351,7 +355,7 @@ __global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, i
 #pragma unroll
         for (int t = 0; t < 32; t++) Bt[t] = 0.0;
 #pragma unroll
-        for (int j = 31; j >= 0; j--) {
+        for (int j = CB - 1; j >= 0; j--) {
             if (j >= c) continue;
             const double tau = st[j];
             double d0 = 0.0, d1 = 0.0;
@@ -393,7 +397,7 @@ __global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, i
     __syncwarp();
     const int nr = c < h ? c : h;
 #pragma unroll
-    for (int j = 31; j >= 0; j--) {
+    for (int j = CB - 1; j >= 0; j--) {
         if (j >= nr) continue;
         const double tau = st[j];
         double d0 = 0.0, d1 = 0.0;
