@@ -96,6 +96,9 @@ __device__ __forceinline__ void w_store(double* p, long long rs, long long cs, i
 // Householder QR of the h x c tile X (lane = column, rows >= h are zero).
 // On exit rows t <= lane of X hold R and rows t > lane the vector of
 // reflector `lane` (unit diagonal implied); returns that reflector's tau.
+// Each step forms the dot products with the unscaled pivot column x (v = [1;
+// sc x]), so they run while the reflector's scalars are computed:
+//   w = tau (X_j + sc x.X),  X_j -= w,  X_t -= (w sc) x_t.
 template <int CB>
 __device__ __forceinline__ double w_geqrt(double (&X)[32], int c, int h) {
     const int lane = threadIdx.x & 31;
@@ -104,37 +107,28 @@ __device__ __forceinline__ double w_geqrt(double (&X)[32], int c, int h) {
 #pragma unroll
     for (int j = 0; j < CB; j++) {
         if (j >= nr) continue;
-        double s0 = 0.0, s1 = 0.0;
+        double s[4] = {0.0, 0.0, 0.0, 0.0}, dd[4] = {0.0, 0.0, 0.0, 0.0};
+        double xr[32];
 #pragma unroll
         for (int t = j + 1; t < 32; t++) {
-            if ((t - j) & 1)
-                s0 = fma(X[t], X[t], s0);
-            else
-                s1 = fma(X[t], X[t], s1);
+            xr[t] = __shfl_sync(FULL, X[t], j);
+            s[t & 3] = fma(X[t], X[t], s[t & 3]);
+            dd[t & 3] = fma(xr[t], X[t], dd[t & 3]);
         }
         const double alpha = __shfl_sync(FULL, X[j], j);
-        const double s2 = __shfl_sync(FULL, s0 + s1, j);
+        const double s2 = __shfl_sync(FULL, (s[0] + s[1]) + (s[2] + s[3]), j);
         double beta, tau, sc;
         hh_params(alpha, s2, &beta, &tau, &sc);
-        double V[32];
-        double d0 = 0.0, d1 = 0.0;
-#pragma unroll
-        for (int t = j + 1; t < 32; t++) {
-            V[t] = __shfl_sync(FULL, X[t], j) * sc;
-            if ((t - j) & 1)
-                d0 = fma(V[t], X[t], d0);
-            else
-                d1 = fma(V[t], X[t], d1);
-        }
-        const double w = tau * (X[j] + (d0 + d1));
+        const double w = tau * fma(sc, (dd[0] + dd[1]) + (dd[2] + dd[3]), X[j]);
         if (lane > j) {
+            const double ws = w * sc;
             X[j] -= w;
 #pragma unroll
-            for (int t = j + 1; t < 32; t++) X[t] = fma(-w, V[t], X[t]);
+            for (int t = j + 1; t < 32; t++) X[t] = fma(-ws, xr[t], X[t]);
         } else if (lane == j) {
             X[j] = beta;
 #pragma unroll
-            for (int t = j + 1; t < 32; t++) X[t] = V[t];
+            for (int t = j + 1; t < 32; t++) X[t] = sc * xr[t];
             mytau = tau;
         }
     }
@@ -144,6 +138,7 @@ __device__ __forceinline__ double w_geqrt(double (&X)[32], int c, int h) {
 // [T; B] with T, B upper triangular (lane = column): eliminate B into T.
 // On exit T is the R of the pair and rows t <= lane of B hold the vector of
 // reflector `lane` (its top part is e_lane); returns that reflector's tau.
+// Same step structure as w_geqrt.
 template <int CB>
 __device__ __forceinline__ double w_ttqrt(double (&T)[32], double (&B)[32], int c) {
     const int lane = threadIdx.x & 31;
@@ -151,37 +146,28 @@ __device__ __forceinline__ double w_ttqrt(double (&T)[32], double (&B)[32], int 
 #pragma unroll
     for (int j = 0; j < CB; j++) {
         if (j >= c) continue;
-        double s0 = 0.0, s1 = 0.0;
+        double s[4] = {0.0, 0.0, 0.0, 0.0}, dd[4] = {0.0, 0.0, 0.0, 0.0};
+        double xr[32];
 #pragma unroll
         for (int t = 0; t <= j; t++) {
-            if (t & 1)
-                s0 = fma(B[t], B[t], s0);
-            else
-                s1 = fma(B[t], B[t], s1);
+            xr[t] = __shfl_sync(FULL, B[t], j);
+            s[t & 3] = fma(B[t], B[t], s[t & 3]);
+            dd[t & 3] = fma(xr[t], B[t], dd[t & 3]);
         }
         const double alpha = __shfl_sync(FULL, T[j], j);
-        const double s2 = __shfl_sync(FULL, s0 + s1, j);
+        const double s2 = __shfl_sync(FULL, (s[0] + s[1]) + (s[2] + s[3]), j);
         double beta, tau, sc;
         hh_params(alpha, s2, &beta, &tau, &sc);
-        double V[32];
-        double d0 = 0.0, d1 = 0.0;
-#pragma unroll
-        for (int t = 0; t <= j; t++) {
-            V[t] = __shfl_sync(FULL, B[t], j) * sc;
-            if (t & 1)
-                d0 = fma(V[t], B[t], d0);
-            else
-                d1 = fma(V[t], B[t], d1);
-        }
-        const double w = tau * (T[j] + (d0 + d1));
+        const double w = tau * fma(sc, (dd[0] + dd[1]) + (dd[2] + dd[3]), T[j]);
         if (lane > j) {
+            const double ws = w * sc;
             T[j] -= w;
 #pragma unroll
-            for (int t = 0; t <= j; t++) B[t] = fma(-w, V[t], B[t]);
+            for (int t = 0; t <= j; t++) B[t] = fma(-ws, xr[t], B[t]);
         } else if (lane == j) {
             T[j] = beta;
 #pragma unroll
-            for (int t = 0; t <= j; t++) B[t] = V[t];
+            for (int t = 0; t <= j; t++) B[t] = sc * xr[t];
             mytau = tau;
         }
     }
