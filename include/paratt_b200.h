@@ -148,6 +148,15 @@ PTT_API int ptt_round_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, cons
 PTT_API int ptt_round_sketch(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* ell,
                              unsigned long long seed, double tol, const int* maxrank, int pad, int* accepted);
 
+/* Round count independent trains (distinct, one context), train i with
+ * tol[i] and rank caps maxrank[i] (d_i + 1 ints, or maxrank == NULL / a NULL
+ * entry for no cap): the same result as ptt_round on each.  The trains are
+ * rounded concurrently on up to `lanes` worker streams (<= 16) of the
+ * context; reads every train's ranks once (synchronises) and returns with
+ * the context's stream ordered after all of them.  No counterpart in the
+ * reference. */
+PTT_API int ptt_round_batch(ptt_tt* const* xs, int count, const double* tol, const int* const* maxrank, int lanes);
+
 /* ---- reaction-Burgers step-truncation RK2 ------------------------------- */
 typedef struct {
     double dt;        /* time step                                            */

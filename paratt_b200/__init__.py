@@ -65,6 +65,7 @@ _SIGS = {
     "ptt_axpby": (_i, [_d, _p, _d, _p, _p]),
     "ptt_hadamard": (_i, [_p, _p, _p]),
     "ptt_square_sym": (_i, [_p, _p]),
+    "ptt_round_batch": (_i, [C.POINTER(_p), _i, _dp, C.POINTER(_ip), _i]),
     "ptt_scale": (_i, [_d, _p]),
     "ptt_mult_diag": (_i, [_p, _i, _dp]),
     "ptt_stencil": (_i, [_p, _i, _dp, _i]),
@@ -341,6 +342,27 @@ def axpby(a, x: TT, b, y: TT, z: TT):
 def hadamard(x: TT, y: TT, z: TT):
     _check(lib().ptt_hadamard(x.h, y.h, z.h))
     return z
+
+
+def round_batch(tts, tols, maxranks=None, lanes=8):
+    """Round independent trains concurrently (ptt_round_batch); maxranks is
+    None or one entry per train (None, an int or d+1 ints)."""
+    n = len(tts)
+    hs = (_p * n)(*[t.h for t in tts])
+    tv = np.ascontiguousarray(tols, dtype=np.float64)
+    mr = None
+    keep = []
+    if maxranks is not None:
+        mr = (_ip * n)()
+        for i, (t, m) in enumerate(zip(tts, maxranks)):
+            if m is None:
+                mr[i] = _ip()
+                continue
+            a = _iarr(m if hasattr(m, "__len__") else [m] * (t.d + 1))
+            keep.append(a)
+            mr[i] = C.cast(a, _ip)
+    _check(lib().ptt_round_batch(hs, n, tv.ctypes.data_as(_dp), mr, int(lanes)))
+    return tts
 
 
 def square_sym(x: TT, z: TT):

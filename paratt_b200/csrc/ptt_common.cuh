@@ -26,6 +26,8 @@ struct DevDesc {
 // Device status word codes (mirrors PTT_ERR_*).
 #define PTT_STATUS_SET(st, code) atomicCAS((st), 0, (code))
 
+#define PTT_MAX_LANES 16
+
 struct ptt_ctx {
     int device;
     cudaStream_t stream;
@@ -59,6 +61,11 @@ struct ptt_ctx {
     int ones_n;
     void* flush;                  // L2 flush buffer
     size_t flush_bytes;
+    // worker contexts of batched calls (own stream and workspaces, the
+    // parent's status word)
+    struct ptt_ctx* lanes[PTT_MAX_LANES];
+    int nlanes;
+    int shared_status;            // d_status belongs to the parent context
 };
 
 // Event pair around a launch of kind `kind` when that class is being timed.

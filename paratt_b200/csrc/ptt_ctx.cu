@@ -84,7 +84,8 @@ extern "C" void ptt_ctx_destroy(ptt_ctx* c) {
     cudaFree(c->ws3);
     cudaFree(c->d_ones);
     cudaFree(c->d_counters);
-    cudaFree(c->d_status);
+    for (int i = 0; i < c->nlanes; i++) ptt_ctx_destroy(c->lanes[i]);
+    if (!c->shared_status) cudaFree(c->d_status);
     cudaFree(c->d_scalars);
     cudaFree(c->d_stats);
     cudaFree(c->d_work);
@@ -443,7 +444,7 @@ extern "C" int ptt_tt_set(ptt_tt* t, const int* ranks, const double* const* core
     if (rc) return rc;
     for (int k = 0; k < t->d; k++) {
         size_t cnt = (size_t)ranks[k] * t->n[k] * ranks[k + 1];
-        PTT_CUDA(cudaMemcpyAsync(t->hd.core[k], cores[k], cnt * sizeof(double), cudaMemcpyHostToDevice,
+        PTT_CUDA(cudaMemcpyAsync(t->hd.core[k], cores[k], cnt * sizeof(double), cudaMemcpyDefault,
                                  t->ctx->stream));
     }
     for (int k = 0; k <= t->d; k++) t->hd.r[k] = ranks[k];
@@ -471,7 +472,7 @@ extern "C" int ptt_tt_get(ptt_tt* t, int* ranks, double* const* cores) {
     if (cores) {
         for (int k = 0; k < t->d; k++) {
             size_t cnt = (size_t)t->hd.r[k] * t->n[k] * t->hd.r[k + 1];
-            PTT_CUDA(cudaMemcpyAsync(cores[k], t->hd.core[k], cnt * sizeof(double), cudaMemcpyDeviceToHost,
+            PTT_CUDA(cudaMemcpyAsync(cores[k], t->hd.core[k], cnt * sizeof(double), cudaMemcpyDefault,
                                      t->ctx->stream));
         }
         PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
