@@ -346,6 +346,138 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# batched rounding (--workload batch): 64 independent trains
+# ---------------------------------------------------------------------------
+def run_batch(args, rank, world, local_rank):
+    """64 trains of uneven d/n/r (workloads.batch_shapes), each rounded to
+    tol 1e-8 x its RMS norm with rank cap floor(r_k/2): ptt_round_batch
+    (concurrent worker streams) against the one-train-at-a-time loop, both
+    from fresh copies of the same inputs every repetition; device time by
+    events on the context stream (rank read-backs included)."""
+    import paratt_b200 as P
+    from paratt_b200 import workloads as Wl
+
+    if rank != 0:
+        return 0
+    ctx = P.Context(local_rank)
+    orig = Wl.batch_trains(ctx, 64, 4)
+    tts = [t for t, _ in orig]
+    caps = [sh[3] for _, sh in orig]
+    tols = [1e-8 * t.norm() for t in tts]
+    work = []
+    for t, (d, n, r, cap) in orig:
+        w = P.TT(ctx, [n] * d, r)
+        work.append(w)
+    elems = sum(sum(r[k] * n * r[k + 1] for k in range(d)) for _, (d, n, r, _) in orig)
+
+    def fresh():
+        for w, t in zip(work, tts):
+            w.copy_from(t)
+        ctx.sync()
+
+    def timed(fn):
+        fresh()
+        ctx.mark(0)
+        fn()
+        ctx.mark(1)
+        ctx.sync()
+        return ctx.elapsed_ms(0, 1)
+
+    def loop():
+        for w, tol, cap in zip(work, tols, caps):
+            w.round(tol, cap)
+
+    lanes = 8
+    t_loop, t_batch = [], []
+    for i in range(args.warmup + args.steps):
+        a = timed(loop)
+        ranks_loop = [w.ranks() for w in work]
+        b = timed(lambda: P.round_batch(work, tols, caps, lanes=lanes))
+        ranks_batch = [w.ranks() for w in work]
+        if i >= args.warmup:
+            t_loop.append(a)
+            t_batch.append(b)
+    same = ranks_loop == ranks_batch
+    tb, tl = statistics.median(t_batch), statistics.median(t_loop)
+    out = {
+        "metric": "batched TT rounding: 64 trains (d 10-40, n 32-512, r 8-96), roundings/s", "value": 64e3 / tb,
+        "unit": "roundings/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": tb,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batched rounding of 64 independent trains (seed 4), tol 1e-8 x ||X||_RMS, "
+                               "rank cap floor(r/2); left-orthonormal cores, bond spectra 2^-j",
+                   "lanes": lanes, "input_gb": elems * 8 / 1e9},
+        "loop": {"value": 64e3 / tl, "unit": "roundings/s", "ms": tl},
+        "batch_over_loop": tl / tb,
+        "same_ranks_as_loop": bool(same),
+    }
+    print(json.dumps(out))
+    for t in tts + work:
+        t.close()
+    ctx.close()
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# single rounding (--workload round): x + y of two rank-32 trains -> rank 32
+# ---------------------------------------------------------------------------
+def run_round(args, rank, world, local_rank):
+    """d=40, n=256: z = x + y of two seeded random trains of interior rank
+    32 (entries N(0, 1/(n r)) -- std 1/sqrt(n r)), rounded to tol 1e-10 x
+    ||z||_RMS with rank cap 32, plain FP64.  Device time by events on the
+    context stream, L2 flushed before each rounding; roofline against the
+    algorithmic bytes 8 sum_k (3 R_k n R_{k+1} + r_k n r_{k+1})."""
+    import paratt_b200 as P
+
+    if rank != 0:
+        return 0
+    d, n, r = 40, 256, 32
+    ctx = P.Context(local_rank)
+    sd = 1.0 / np.sqrt(n * r)
+
+    def rnd(seed):
+        rng = np.random.default_rng(seed)
+        rr = [1] + [r] * (d - 1) + [1]
+        return [rng.standard_normal((rr[k], n, rr[k + 1])) * sd for k in range(d)]
+
+    X = P.TT.from_cores(ctx, rnd(1))
+    Y = P.TT.from_cores(ctx, rnd(2))
+    cap = [1] + [2 * r] * (d - 1) + [1]
+    Z = P.TT(ctx, [n] * d, cap)
+    P.axpby(1.0, X, 1.0, Y, Z)
+    tol = 1e-10 * Z.norm()
+    W = P.TT(ctx, [n] * d, cap)
+    ts = []
+    for i in range(args.warmup + args.steps):
+        W.copy_from(Z)
+        ctx.flush_l2()
+        ctx.mark(0)
+        W.round(tol, r)
+        ctx.mark(1)
+        ctx.sync()
+        if i >= args.warmup:
+            ts.append(ctx.elapsed_ms(0, 1))
+    rk_in, rk_out = Z.ranks(), W.ranks()
+    alg = 8.0 * sum(3 * rk_in[k] * n * rk_in[k + 1] + rk_out[k] * n * rk_out[k + 1] for k in range(d))
+    t = statistics.median(ts)
+    hbm, src = peaks()
+    out = {
+        "metric": "TT rounding d=40, n=256, ranks 64 -> 32 (plain FP64), roundings/s", "value": 1e3 / t,
+        "unit": "roundings/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "round(x + y), x, y seeded rank-32 trains, N(0, 1/(n r)) entries, tol 1e-10 x "
+                               "||z||_RMS, rank cap 32", "ranks_out": max(rk_out), "l2": "flushed before each"},
+        "roofline": {"bound": "hbm", "achieved": alg / (t / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": alg / (t / 1e3) / 1e9 / hbm, "traffic": None, "algorithmic_bytes": alg,
+                     "peak_source": src},
+    }
+    print(json.dumps(out))
+    for t_ in (X, Y, Z, W):
+        t_.close()
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -353,12 +485,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="rk2", choices=["rk2", "batch", "round"],
+                    help="rk2: the headline reaction-Burgers steps; batch: 64 independent roundings; "
+                         "round: one rank-64 -> 32 rounding")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.workload == "batch":
+        return run_batch(args, rank, world, local_rank)
+    if args.workload == "round":
+        return run_round(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 
 

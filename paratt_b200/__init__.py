@@ -143,6 +143,7 @@ class Context:
     """One device + stream + workspace (ptt_ctx)."""
 
     def __init__(self, device: int = 0):
+        self.device = int(device)
         self.h = lib().ptt_ctx_create(device)
         if not self.h:
             _check(lib().ptt_last_error() or PTT_ERR_CUDA)
@@ -225,6 +226,12 @@ class TT:
         bufs = [np.ascontiguousarray(c.ravel(order="F"), dtype=np.float64) for c in cores]
         ptrs = (_dp * self.d)(*[b.ctypes.data_as(_dp) for b in bufs])
         _check(lib().ptt_tt_set(self.h, _iarr(ranks), ptrs))
+
+    def set_device(self, ranks, ptrs):
+        """Set the cores from device (or any CUDA-addressable) memory: ptrs[k]
+        is the address of core k, ranks[k] x n_k x ranks[k+1] column-major."""
+        arr = (_dp * self.d)(*[C.cast(C.c_void_p(int(p)), _dp) for p in ptrs])
+        _check(lib().ptt_tt_set(self.h, _iarr(ranks), arr))
 
     def ranks(self):
         r = (C.c_int * (self.d + 1))()

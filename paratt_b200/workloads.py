@@ -59,3 +59,52 @@ def rms_norm(cores):
         t = np.einsum("ik,kjd->ijd", a, c)
         a = np.einsum("ijb,ijd->bd", c, t) / c.shape[1]
     return float(np.sqrt(max(a[0, 0], 0.0)))
+
+
+def batch_shapes(count=64, seed=4):
+    """Shapes of the batched-rounding workload: per train d ~ U{10..40},
+    one mode size n ~ U{32, 64, 128, 256, 512}, interior ranks r_k ~
+    U{8..96} clamped to r_{k-1} n and n r_{k+1} (a valid TT), rank cap
+    floor(r_k / 2) per bond."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        d = int(rng.integers(10, 41))
+        n = int(rng.choice([32, 64, 128, 256, 512]))
+        r = [1] + [int(v) for v in rng.integers(8, 97, size=d - 1)] + [1]
+        for k in range(1, d):  # left-to-right, then right-to-left clamp
+            r[k] = min(r[k], r[k - 1] * n)
+        for k in range(d - 1, 0, -1):
+            r[k] = min(r[k], r[k + 1] * n)
+        cap = [1] + [max(1, v // 2) for v in r[1:-1]] + [1]
+        out.append((d, n, r, cap))
+    return out
+
+
+def batch_trains(ctx, count=64, seed=4):
+    """The batched-rounding workload as device trains: left-orthonormal
+    random cores (QR of a Gaussian matrix) whose bond column j is scaled by
+    2^-j, so every bond's spectrum decays as 2^-j.  Generated on the GPU
+    with torch (input preparation only).  Returns [(TT, shape)]."""
+    import torch
+
+    from . import TT
+
+    dev = torch.device("cuda", ctx.device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    trains = []
+    for d, n, r, cap in batch_shapes(count, seed):
+        T = TT(ctx, [n] * d, r)
+        cores = []
+        for k in range(d):
+            a = torch.randn(r[k] * n, r[k + 1], dtype=torch.float64, device=dev, generator=g)
+            q, _ = torch.linalg.qr(a)
+            if k < d - 1:
+                q = q * torch.pow(2.0, -torch.arange(r[k + 1], dtype=torch.float64, device=dev))
+            # (r_k n) x r_{k+1} column-major == the core's layout
+            cores.append(q.t().contiguous().t())
+        T.set_device(r, [c.data_ptr() for c in cores])
+        torch.cuda.synchronize(dev)
+        trains.append((T, (d, n, r, cap)))
+    return trains
