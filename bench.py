@@ -478,6 +478,42 @@ def run_round(args, rank, world, local_rank):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# one step for profilers (--one-step plain|learned)
+# ---------------------------------------------------------------------------
+def run_one_step(args, local_rank):
+    """W plain warm-up steps, then exactly one step of the chosen method;
+    prints the number of kernel launches before that step (the value for
+    `ncu -s`)."""
+    import paratt_b200 as P
+    from paratt_b200 import learned as Lr
+    from paratt_b200 import workloads as Wl
+
+    d, n, maxr, dt = CFG["d"], CFG["n"], CFG["maxrank"], CFG["dt"]
+    ctx = P.Context(local_rank)
+    u0 = Wl.initial_condition(d, n, CFG["ngauss"], CFG["seed"])
+    tol = CFG["tol"] * Wl.rms_norm(u0)
+    plain = P.RxnBurgers(ctx, d, n, maxrank=maxr, dt=dt, tol=tol, seed=7)
+    plain.log(True)
+    U = P.TT(ctx, [n] * d, [1] + [2 * maxr] * (d - 1) + [1], u0)
+    for _ in range(args.warmup):
+        plain.step(U)
+    step = plain.step
+    if args.one_step == "learned":
+        ls = Lr.LearnedStepper(ctx, d, n, maxr, dt, tol, seed=3)
+        _, sig, delta = plain.last_step(d)
+        ls.seed_spectra(sig, delta)
+        ls.step(U)  # first learned step: the MLP and sketch workspaces warm up
+        step = ls.step
+    ctx.sync()
+    print(f"launches before the measured step: {ctx.launches}", flush=True)
+    step(U)
+    ctx.sync()
+    print(f"launches in the step: {ctx.launches}", flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -485,6 +521,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--one-step", choices=["plain", "learned"], default=None,
+                    help="profiling aid: W warm-up steps, then one step; prints the launch index to skip to")
     ap.add_argument("--workload", default="rk2", choices=["rk2", "batch", "round"],
                     help="rk2: the headline reaction-Burgers steps; batch: 64 independent roundings; "
                          "round: one rank-64 -> 32 rounding")
@@ -494,6 +532,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.one_step:
+        return run_one_step(args, local_rank)
     if args.workload == "batch":
         return run_batch(args, rank, world, local_rank)
     if args.workload == "round":

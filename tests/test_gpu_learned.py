@@ -77,3 +77,60 @@ def test_sketch_step_close_to_plain(ctx):
     assert calls > 0
     plain.close()
     sk.close()
+
+
+def test_learned_ranks_gain_over_fixed_sketch(ctx):
+    """What the trained network buys: from a config-4 state (d=40, n=256,
+    rank cap 64), one sketch step with the MLP's per-bond ranks against the
+    same step with the rank a sketch needs without a model (cap + pad on
+    every bond).  Both must be accepted by the deterministic judge and agree
+    to the tolerance; the learned ranks are far smaller and the step faster."""
+    import time
+
+    from paratt_b200 import learned as Lr
+    from paratt_b200 import workloads as W
+
+    d, n, maxr, dt, pad = 40, 256, 64, 1e-3, 4
+    u0 = W.initial_condition(d, n, 3, 3)
+    tol = 1e-8 * W.rms_norm(u0)
+    cap = [1] + [2 * maxr] * (d - 1) + [1]
+    plain = P.RxnBurgers(ctx, d, n, maxrank=maxr, dt=dt, tol=tol)
+    plain.log(True)
+    U = P.TT(ctx, [n] * d, cap, u0)
+    for _ in range(3):
+        plain.step(U)
+    _, sig, delta = plain.last_step(d)
+    fixed = [1] + [maxr + pad] * (d - 1) + [1]
+    ls = Lr.LearnedStepper(ctx, d, n, maxr, dt, tol, pad=pad, seed=3)
+    fx = P.RxnBurgers(ctx, d, n, maxrank=maxr, dt=dt, tol=tol, seed=3)
+    A, B = P.TT(ctx, [n] * d, cap), P.TT(ctx, [n] * d, cap)
+
+    def run(step, X):
+        X.copy_from(U)
+        ctx.sync()
+        t0 = time.perf_counter()
+        step(X)
+        ctx.sync()
+        return time.perf_counter() - t0
+
+    run(lambda X: fx.step_sketch(X, fixed, pad=pad), B)  # warm both paths
+    ls.seed_spectra(sig, delta)
+    run(ls.step, A)
+    tf = min(run(lambda X: fx.step_sketch(X, fixed, pad=pad), B) for _ in range(2))
+    tl = []
+    for _ in range(2):
+        ls.seed_spectra(sig, delta)
+        tl.append(run(ls.step, A))
+    tl = min(tl)
+    ell = ls.ell
+    assert ls.counts()[1] == 0 and fx.sketch_counts()[1] == 0  # no fallback
+    a, b = A.get(), B.get()
+    assert O.ranks_of(a) == O.ranks_of(b)
+    assert O.rel_diff_exact(a, b) <= 1e-7
+    assert sum(ell[1:-1]) < 0.5 * sum(fixed[1:-1])
+    assert tl < 0.85 * tf, (tl, tf)
+    for t in (A, B, U):
+        t.close()
+    ls.close()
+    fx.close()
+    plain.close()
