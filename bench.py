@@ -261,10 +261,18 @@ def run_ours(args, rank, world, local_rank):
     chk = Lr.LearnedStepper(ctx, d, n, maxr, dt, tol, seed=3 + rank)
     chk.seed_spectra(sig0, delta0)
     chk.step(B)
-    aa, bb, ab = A.dot(A), B.dot(B), A.dot(B)
-    err_step = float(np.sqrt(abs(aa - 2.0 * ab + bb) / aa))
-    pp, ll, pl = UP.dot(UP), UL.dot(UL), UP.dot(UL)
-    err_traj = float(np.sqrt(abs(pp - 2.0 * pl + ll) / pp))
+    def rel_diff(X, Y):
+        # ||X - Y|| / ||Y||: the difference formed as a train and orthogonalised
+        # (zero-tolerance rounding) before its norm, so nothing cancels
+        D = P.TT(ctx, [n] * d, [1] * (d + 1))  # grown to the exact sum ranks
+        P.axpby(1.0, X, -1.0, Y, D)
+        D.round(0.0)
+        v = D.norm() / Y.norm()
+        D.close()
+        return float(v)
+
+    err_step = rel_diff(B, A)
+    err_traj = rel_diff(UL, UP)
     chk.close()
     A.close()
     B.close()

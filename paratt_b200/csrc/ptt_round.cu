@@ -347,7 +347,13 @@ __global__ void __launch_bounds__(SVD_NT) k_svd_jacobi(Plan pl, double* ws, doub
             s2 += x * x;
         }
         s2 = gsum8(s2, gm);
-        if (p == 0) s_sig[j] = (j < q) ? sqrt(s2) : -1.0;
+        // a NaN (corrupt input) would break the strict order below and leave
+        // order slots unset; it sorts last and is reported instead
+        if (p == 0) {
+            const bool nan = !(s2 == s2);
+            if (nan && j < q) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
+            s_sig[j] = (j < q && !nan) ? sqrt(s2) : -1.0;
+        }
     }
     __syncthreads();
     for (int j = tid; j < qq; j += SVD_NT) {
