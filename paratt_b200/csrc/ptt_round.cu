@@ -237,15 +237,21 @@ __device__ __forceinline__ int circle_col(int pos, int round, int qq) {
     return pos == 0 ? 0 : 1 + (pos - 1 + round) % (qq - 1);
 }
 
-constexpr int SVD_NT = 512;
+// threads of the SVD block: 8 lanes for each of the (CT+2)/2 column pairs
+// of a round, rounded to a power of two (idle threads only slow the barriers)
+template <int CT>
+__host__ __device__ constexpr int svd_nt() {
+    return CT <= 32 ? 128 : (CT <= 64 ? 256 : 512);
+}
 
 // One-sided Jacobi on the columns of L (c rows, q columns).  Each column pair
 // is handled by 8 lanes (rows p + 8v), 64 pairs per pass, so one circle-order
 // round is a single pass for q <= 128.  Column norms are tracked through the
 // rotations (a_p' = a_p - t a_pq ...) and recomputed at the start of a sweep.
 template <int CT>
-__global__ void __launch_bounds__(SVD_NT) k_svd_jacobi(Plan pl, double* ws, double delta, int maxr, int bond,
+__global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws, double delta, int maxr, int bond,
                                                        int* status) {
+    constexpr int SVD_NT = svd_nt<CT>();
     extern __shared__ double sm[];
     constexpr int S = CT + 1;
     constexpr int NG = CT / 8;
@@ -775,7 +781,7 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
         if ((rc = launch_factor<CT>(c, x, i, RIGHT_T, pl, ws))) return rc;
         const int mr = maxr ? maxr[i] : rk[i];
         ptt_time_begin(c, PTT_TIME_SVD);
-        k_svd_jacobi<CT><<<1, SVD_NT, svd_smem<CT>(), c->stream>>>(pl, ws, delta, mr, i, c->d_status);
+        k_svd_jacobi<CT><<<1, svd_nt<CT>(), svd_smem<CT>(), c->stream>>>(pl, ws, delta, mr, i, c->d_status);
         ptt_time_end(c, PTT_TIME_SVD);
         PTT_LAUNCHED(c);
         k_svd_replay<<<(CT + 7) / 8, 256, replay_smem<CT>(), c->stream>>>(pl, ws);
@@ -933,7 +939,7 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
             Wmax = Wr[i] > Wmax ? Wr[i] : Wmax;
             const int mr = maxr ? maxr[i] : rk[i];
             ptt_time_begin(c, PTT_TIME_SVD);
-            k_svd_jacobi<32><<<1, SVD_NT, svd_smem<32>(), c->stream>>>(pl, wsb, delta, mr, i, c->d_status);
+            k_svd_jacobi<32><<<1, svd_nt<32>(), svd_smem<32>(), c->stream>>>(pl, wsb, delta, mr, i, c->d_status);
             ptt_time_end(c, PTT_TIME_SVD);
             PTT_LAUNCHED(c);
             const long long mcap = (long long)rk[i - 1] * x->n[i - 1];
