@@ -22,7 +22,7 @@ import time
 
 import numpy as np
 
-from . import STAT_NSIG, MLP, Context, RxnBurgers, TT
+from . import STAT_NSIG, MLP, Context, RxnBurgers, TT, axpby
 from . import workloads as W
 
 NIN = STAT_NSIG + 2
@@ -118,14 +118,80 @@ def train(mlp, X, T, epochs=300, lr=3e-3, batch=512, seed=0):
     return losses
 
 
+def rel_diff(ctx, X, Y):
+    """||X - Y|| / ||Y|| with the difference formed as a train and
+    orthogonalised (zero-tolerance rounding) before its norm, so nothing
+    cancels."""
+    D = TT(ctx, X.dims, [1] * (X.d + 1))
+    axpby(1.0, X, -1.0, Y, D)
+    D.round(0.0)
+    v = D.norm() / Y.norm()
+    D.close()
+    return float(v)
+
+
+def evaluate(ctx, cfg, steps, every=50, pad=4, model=MODEL):
+    """Learned and plain trajectories from the same initial condition, side
+    by side: time per step of each, sketch roundings and fallbacks, largest
+    proposed sketch rank, state rank, and the relative difference of the two
+    states every `every` steps.  Returns a summary dict."""
+    d, n, maxr, dt = cfg["d"], cfg["n"], cfg["maxrank"], cfg["dt"]
+    u0 = W.initial_condition(d, n, cfg["ngauss"], cfg["seed"])
+    tol = cfg["tol"] * W.rms_norm(u0)
+    cap = [1] + [2 * maxr] * (d - 1) + [1]
+    plain = RxnBurgers(ctx, d, n, maxrank=maxr, dt=dt, tol=tol, seed=7)
+    ls = LearnedStepper(ctx, d, n, maxr, dt, tol, pad=pad, model=model, seed=3)
+    UP = TT(ctx, [n] * d, cap, u0)
+    UL = TT(ctx, [n] * d, cap, u0)
+    tp = tl = 0.0
+    ell_max, rank_max, diffs = 0, 0, []
+    for s in range(steps):
+        ctx.sync()
+        t0 = time.perf_counter()
+        plain.step(UP)
+        ctx.sync()
+        t1 = time.perf_counter()
+        ls.step(UL)
+        ctx.sync()
+        t2 = time.perf_counter()
+        tp += t1 - t0
+        tl += t2 - t1
+        if ls.ell is not None:
+            ell_max = max(ell_max, max(ls.ell))
+        rank_max = max(rank_max, max(UL.ranks()))
+        if (s + 1) % every == 0 or s == steps - 1:
+            diffs.append((s + 1, rel_diff(ctx, UL, UP)))
+    calls, fb = ls.counts()
+    out = {"steps": steps, "plain_ms_per_step": 1e3 * tp / steps, "learned_ms_per_step": 1e3 * tl / steps,
+           "learned_over_plain": tp / tl, "sketch_roundings": calls, "fallbacks": fb,
+           "fallback_rate": fb / max(calls, 1), "max_sketch_rank": ell_max, "max_state_rank": rank_max,
+           "rel_diff_vs_plain": diffs}
+    for t in (UP, UL):
+        t.close()
+    ls.close()
+    plain.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=MODEL)
     ap.add_argument("--seeds", type=int, nargs="*", default=[10, 11, 12, 13])
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--epochs", type=int, default=300)
+    ap.add_argument("--evaluate", default=None, choices=["c2", "c4"],
+                    help="instead of training: run the learned and plain methods side by side on a "
+                         "configuration for --steps steps and print a JSON summary")
     args = ap.parse_args()
     ctx = Context(0)
+    if args.evaluate:
+        import json
+
+        res = evaluate(ctx, W.CONFIGS[args.evaluate], args.steps)
+        res["config"] = args.evaluate
+        print(json.dumps(res), flush=True)
+        ctx.close()
+        return
     cfg = dict(W.CONFIGS["c2"])
     t0 = time.time()
     Xs, Ts = [], []
