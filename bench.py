@@ -205,7 +205,7 @@ def run_ours(args, rank, world, local_rank):
     S0 = P.TT(ctx, [n] * d, cap, u0)
     for _ in range(args.warmup):
         plain.step(S0)
-    _, sig0, delta0 = plain.last_step(d)
+    spec0 = Lr.kind_spectra(plain, d)
     ctx.sync()
 
     def copy_of(src):
@@ -228,7 +228,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- learned-sketch method (the headline) --------------------------------
     ls = Lr.LearnedStepper(ctx, d, n, maxr, dt, tol, seed=3 + rank)
-    ls.seed_spectra(sig0, delta0)
+    ls.seed_from(spec0)
     UL = copy_of(S0)
     l0 = ctx.launches
     with ClockSampler(local_rank) as clk:
@@ -240,7 +240,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- the same learned steps again with every factorisation launch timed
     # by its own event pair (kept out of the headline region)
     lk = Lr.LearnedStepper(ctx, d, n, maxr, dt, tol, seed=3 + rank)
-    lk.seed_spectra(sig0, delta0)
+    lk.seed_from(spec0)
     UK = copy_of(S0)
     ctx.time_kernels(P.TIME_TSQR)
     timed(lk.step, UK)
@@ -259,7 +259,7 @@ def run_ours(args, rank, world, local_rank):
     A, B = copy_of(S0), copy_of(S0)
     plain.step(A)
     chk = Lr.LearnedStepper(ctx, d, n, maxr, dt, tol, seed=3 + rank)
-    chk.seed_spectra(sig0, delta0)
+    chk.seed_from(spec0)
     chk.step(B)
     def rel_diff(X, Y):
         # ||X - Y|| / ||Y||: the difference formed as a train and orthogonalised
@@ -281,7 +281,7 @@ def run_ours(args, rank, world, local_rank):
     host = P.HostTrain([n] * d, cap, S0.get())
     ue = P.TT(ctx, [n] * d, cap)
     le = Lr.LearnedStepper(ctx, d, n, maxr, dt, tol, seed=3 + rank)
-    le.seed_spectra(sig0, delta0)
+    le.seed_from(spec0)
     h2d = d2h = 0
     ctx.sync()
     barrier()
@@ -509,8 +509,7 @@ def run_one_step(args, local_rank):
     step = plain.step
     if args.one_step == "learned":
         ls = Lr.LearnedStepper(ctx, d, n, maxr, dt, tol, seed=3)
-        _, sig, delta = plain.last_step(d)
-        ls.seed_spectra(sig, delta)
+        ls.seed_from(plain)
         ls.step(U)  # first learned step: the MLP and sketch workspaces warm up
         step = ls.step
     ctx.sync()

@@ -183,12 +183,26 @@ PTT_API int ptt_rxn_burgers_rk2_step(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_pa
  * ptt_round_sketch (margin `pad`) is redone deterministically. */
 PTT_API int ptt_rxn_burgers_rk2_step_sketch(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int* ell,
                                             int pad);
+/* Rounding kinds of a step: the product u.u, the field F, the two stage
+ * roundings (u_s and u+). */
+#define PTT_RXN_KIND_PRODUCT 0
+#define PTT_RXN_KIND_FIELD 1
+#define PTT_RXN_KIND_STAGE 2
+#define PTT_RXN_KINDS 3
+/* The sketch step with sketch ranks per kind: ell holds PTT_RXN_KINDS blocks
+ * of d+1 entries, block t for the roundings of kind t. */
+PTT_API int ptt_rxn_burgers_rk2_step_sketch_kinds(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p,
+                                                  const int* ell, int pad);
 PTT_API int ptt_rxn_ws_sketch_counts(const ptt_rxn_ws* ws, long long* calls, long long* fallbacks);
 /* Logging (reads each rounding's statistics back): per step the largest kept
  * rank of every bond over the step's roundings, and the top PTT_STAT_NSIG
  * singular values of every bond of the last rounding with its threshold. */
 PTT_API int ptt_rxn_ws_log(ptt_rxn_ws* ws, int on);
 PTT_API int ptt_rxn_ws_last_step(const ptt_rxn_ws* ws, int* ranks, double* sig, double* delta);
+/* The same restricted to the roundings of one kind (PTT_RXN_KIND_*): their
+ * largest kept rank per bond in the last step, and the spectra and threshold
+ * of the last rounding of that kind. */
+PTT_API int ptt_rxn_ws_last_step_kind(const ptt_rxn_ws* ws, int kind, int* ranks, double* sig, double* delta);
 
 /* ---- sketch-rank proposer: MLP nin -> width -> width -> 1 (ReLU), BF16
  * weights, FP32 accumulation, trained with hand-written kernels (Adam) ---- */

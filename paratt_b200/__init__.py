@@ -23,6 +23,9 @@ LIB_PATH = os.path.join(_HERE, "libparatt_b200.so")
 TIME_TSQR, TIME_SVD, TIME_GEMM = 1, 2, 3
 STAT_NSIG = 16
 STAT_LEN = 8 + STAT_NSIG
+# rounding kinds of the reaction-Burgers step (PTT_RXN_KIND_*)
+KIND_PRODUCT, KIND_FIELD, KIND_STAGE = 0, 1, 2
+KINDS = 3
 
 PTT_OK, PTT_ERR_ARG, PTT_ERR_CUDA, PTT_ERR_CAPACITY, PTT_ERR_NUMERIC, PTT_ERR_NOGPU, PTT_ERR_TIMEOUT = range(7)
 
@@ -94,6 +97,8 @@ _SIGS = {
     "ptt_rxn_ws_sketch_counts": (_i, [_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "ptt_rxn_ws_log": (_i, [_p, _i]),
     "ptt_rxn_ws_last_step": (_i, [_p, _ip, _dp, _dp]),
+    "ptt_rxn_ws_last_step_kind": (_i, [_p, _i, _ip, _dp, _dp]),
+    "ptt_rxn_burgers_rk2_step_sketch_kinds": (_i, [_p, _p, _p, _ip, _i]),
     "ptt_mlp_create": (_p, [_p, _i, _i, C.c_ulonglong]),
     "ptt_mlp_destroy": (None, [_p]),
     "ptt_mlp_num_params": (C.c_longlong, [_p]),
@@ -414,6 +419,12 @@ class RxnBurgers:
         _check(lib().ptt_rxn_burgers_rk2_step_sketch(u.h, self.h, C.byref(self.p), e, int(pad)))
         return u
 
+    def step_sketch_kinds(self, u: TT, ell, pad=4):
+        """ell: KINDS x (d+1) sketch ranks, row t for the roundings of kind t."""
+        e = _iarr(np.asarray(ell, dtype=np.int64).ravel())
+        _check(lib().ptt_rxn_burgers_rk2_step_sketch_kinds(u.h, self.h, C.byref(self.p), e, int(pad)))
+        return u
+
     def sketch_counts(self):
         c, f = C.c_longlong(), C.c_longlong()
         _check(lib().ptt_rxn_ws_sketch_counts(self.h, C.byref(c), C.byref(f)))
@@ -429,6 +440,14 @@ class RxnBurgers:
         sig = np.zeros((d + 1, STAT_NSIG))
         dl = C.c_double()
         _check(lib().ptt_rxn_ws_last_step(self.h, r, sig.ctypes.data_as(_dp), C.byref(dl)))
+        return list(r), sig, dl.value
+
+    def last_step_kind(self, kind, d):
+        """last_step restricted to the roundings of one kind (KIND_*)."""
+        r = (C.c_int * (d + 1))()
+        sig = np.zeros((d + 1, STAT_NSIG))
+        dl = C.c_double()
+        _check(lib().ptt_rxn_ws_last_step_kind(self.h, int(kind), r, sig.ctypes.data_as(_dp), C.byref(dl)))
         return list(r), sig, dl.value
 
     def counts(self):

@@ -48,7 +48,13 @@ struct ptt_rxn_ws {
     double sig[(PTT_MAX_DIM + 1) * PTT_STAT_NSIG];   /* top spectra of the last rounding */
     double delta;                                     /* its per-bond threshold */
     double stats[(PTT_MAX_DIM + 1) * PTT_STAT_LEN];
+    /* the same per rounding kind (PTT_RXN_KIND_*) */
+    int kind_rank[PTT_RXN_KINDS][PTT_MAX_DIM + 1];
+    double kind_sig[PTT_RXN_KINDS][(PTT_MAX_DIM + 1) * PTT_STAT_NSIG];
+    double kind_delta[PTT_RXN_KINDS];
 };
+
+#define KIND_NONE (-1) /* intermediate roundings of the plain F (a, b): step maximum only */
 
 #define FORMAL_MAX 128
 
@@ -118,9 +124,18 @@ int ptt_rxn_ws_last_step(const ptt_rxn_ws* ws, int* ranks, double* sig, double* 
     return PTT_OK;
 }
 
-/* After a rounding: fold its per-bond ranks into the step maximum and keep
- * its spectra (logging mode only: reads the statistics back). */
-static int logged(ptt_rxn_ws* ws, int rc) {
+int ptt_rxn_ws_last_step_kind(const ptt_rxn_ws* ws, int kind, int* ranks, double* sig, double* delta) {
+    if (!ws || kind < 0 || kind >= PTT_RXN_KINDS) return PTT_ERR_ARG;
+    if (ranks) memcpy(ranks, ws->kind_rank[kind], sizeof(int) * (ws->d + 1));
+    if (sig) memcpy(sig, ws->kind_sig[kind], sizeof(double) * (ws->d + 1) * PTT_STAT_NSIG);
+    if (delta) *delta = ws->kind_delta[kind];
+    return PTT_OK;
+}
+
+/* After a rounding of the given kind: fold its per-bond ranks into the step
+ * maximum (and the kind's maximum) and keep its spectra (logging mode only:
+ * reads the statistics back). */
+static int logged_kind(ptt_rxn_ws* ws, int rc, int kind) {
     if (rc || !ws->log) return rc;
     const int d = ws->d;
     if ((rc = ptt_round_stats(ws->ctx, d, ws->stats))) return rc;
@@ -130,12 +145,20 @@ static int logged(ptt_rxn_ws* ws, int rc) {
         if (r > ws->step_rank[k]) ws->step_rank[k] = r;
         memcpy(ws->sig + (size_t)k * PTT_STAT_NSIG, st + 8, sizeof(double) * PTT_STAT_NSIG);
         ws->delta = st[6];
+        if (kind >= 0) {
+            if (r > ws->kind_rank[kind][k]) ws->kind_rank[kind][k] = r;
+            memcpy(ws->kind_sig[kind] + (size_t)k * PTT_STAT_NSIG, st + 8, sizeof(double) * PTT_STAT_NSIG);
+            ws->kind_delta[kind] = st[6];
+        }
     }
     return PTT_OK;
 }
 
 static void step_begin(ptt_rxn_ws* ws) {
-    for (int k = 0; k <= ws->d; k++) ws->step_rank[k] = 0;
+    for (int k = 0; k <= ws->d; k++) {
+        ws->step_rank[k] = 0;
+        for (int t = 0; t < PTT_RXN_KINDS; t++) ws->kind_rank[t][k] = 0;
+    }
 }
 
 static void stencils(const ptt_rxn_params* p, int d, int n, double* d2, double* d1) {
@@ -166,12 +189,12 @@ static int product(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int
     if (!ell_sketch && rmax * (rmax + 1) / 2 <= FORMAL_MAX) {
         if ((rc = ptt_square_sym(u, ws->w))) return rc;
         ws->hadamard_formal++;
-        return logged(ws, ptt_round(ws->w, p->tol, mr));
+        return logged_kind(ws, ptt_round(ws->w, p->tol, mr), PTT_RXN_KIND_PRODUCT);
     }
     int ell[PTT_MAX_DIM + 1];
     for (int k = 0; k <= d; k++) ell[k] = ell_sketch ? ell_sketch[k] : p->maxrank + p->sketch_pad;
     ws->hadamard_sketch++;
-    return logged(ws, ptt_round_hadamard(u, u, ws->w, ell, p->seed, p->tol, mr));
+    return logged_kind(ws, ptt_round_hadamard(u, u, ws->w, ell, p->seed, p->tol, mr), PTT_RXN_KIND_PRODUCT);
 }
 
 int ptt_rxn_burgers_F(ptt_tt* u, ptt_tt* F, ptt_rxn_ws* ws, const ptt_rxn_params* p) {
@@ -183,11 +206,11 @@ int ptt_rxn_burgers_F(ptt_tt* u, ptt_tt* F, ptt_rxn_ws* ws, const ptt_rxn_params
     stencils(p, d, n[0], d2, d1);
     if ((rc = product(u, ws, p, mr, NULL))) return rc;
     if ((rc = ptt_op_sum(u, d2, 3, 1.0, ws->a))) return rc;
-    if ((rc = logged(ws, ptt_round(ws->a, p->tol, mr)))) return rc;
+    if ((rc = logged_kind(ws, ptt_round(ws->a, p->tol, mr), KIND_NONE))) return rc;
     if ((rc = ptt_op_sum(ws->w, d1, 3, -1.0, ws->b))) return rc;
-    if ((rc = logged(ws, ptt_round(ws->b, p->tol, mr)))) return rc;
+    if ((rc = logged_kind(ws, ptt_round(ws->b, p->tol, mr), KIND_NONE))) return rc;
     if ((rc = ptt_axpby(1.0, ws->a, 1.0, ws->b, F))) return rc;
-    return logged(ws, ptt_round(F, p->tol, mr));
+    return logged_kind(ws, ptt_round(F, p->tol, mr), PTT_RXN_KIND_FIELD);
 }
 
 int ptt_rxn_burgers_rk2_step(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p) {
@@ -198,10 +221,10 @@ int ptt_rxn_burgers_rk2_step(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p)
     step_begin(ws);
     if ((rc = ptt_rxn_burgers_F(u, ws->k, ws, p))) return rc;
     if ((rc = ptt_axpby(1.0, u, 0.5 * p->dt, ws->k, ws->us))) return rc;
-    if ((rc = logged(ws, ptt_round(ws->us, p->tol, mr)))) return rc;
+    if ((rc = logged_kind(ws, ptt_round(ws->us, p->tol, mr), PTT_RXN_KIND_STAGE))) return rc;
     if ((rc = ptt_rxn_burgers_F(ws->us, ws->k, ws, p))) return rc;
     if ((rc = ptt_axpby(1.0, u, p->dt, ws->k, u))) return rc;
-    return logged(ws, ptt_round(u, p->tol, mr));
+    return logged_kind(ws, ptt_round(u, p->tol, mr), PTT_RXN_KIND_STAGE);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -215,16 +238,17 @@ static int sketch_or_round(ptt_tt* src, ptt_tt* dst, ptt_rxn_ws* ws, const ptt_r
                            const int* ell, int pad, unsigned long long salt) {
     int ok = 0, rc;
     ws->sketch_calls++;
-    rc = logged(ws, ptt_round_sketch(src, NULL, dst, ell, p->seed ^ salt, p->tol, mr, pad, &ok));
+    rc = logged_kind(ws, ptt_round_sketch(src, NULL, dst, ell, p->seed ^ salt, p->tol, mr, pad, &ok),
+                     PTT_RXN_KIND_STAGE);
     if (rc) return rc;
     if (ok) return PTT_OK;
     ws->sketch_fallbacks++;
-    if ((rc = logged(ws, ptt_round(src, p->tol, mr)))) return rc;
+    if ((rc = logged_kind(ws, ptt_round(src, p->tol, mr), PTT_RXN_KIND_STAGE))) return rc;
     return ptt_tt_copy(dst, src);
 }
 
-static int F_sketch(ptt_tt* u, ptt_tt* F, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int* ell, int pad,
-                    unsigned long long salt) {
+static int F_sketch(ptt_tt* u, ptt_tt* F, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int* ell_prod,
+                    const int* ell_field, int pad, unsigned long long salt) {
     int rc, d, n[PTT_MAX_DIM], mr[PTT_MAX_DIM + 1];
     if ((rc = shape(u, &d, n))) return rc;
     for (int k = 0; k <= d; k++) mr[k] = p->maxrank;
@@ -237,7 +261,8 @@ static int F_sketch(ptt_tt* u, ptt_tt* F, ptt_rxn_ws* ws, const ptt_rxn_params* 
         for (int k = 0; k <= d; k++) full[k] = r[k] * r[k];
         ws->sketch_calls++;
         ws->hadamard_sketch++;
-        rc = logged(ws, ptt_round_sketch(u, u, ws->w, ell, p->seed ^ (salt * 7 + 1), p->tol, mr, pad, &ok));
+        rc = logged_kind(ws, ptt_round_sketch(u, u, ws->w, ell_prod, p->seed ^ (salt * 7 + 1), p->tol, mr, pad, &ok),
+                         PTT_RXN_KIND_PRODUCT);
         if (rc) return rc;
         if (!ok) {
             ws->sketch_fallbacks++;
@@ -250,27 +275,41 @@ static int F_sketch(ptt_tt* u, ptt_tt* F, ptt_rxn_ws* ws, const ptt_rxn_params* 
     if ((rc = ptt_axpby(1.0, ws->a, 1.0, ws->b, ws->s))) return rc;
     int ok = 0;
     ws->sketch_calls++;
-    rc = logged(ws, ptt_round_sketch(ws->s, NULL, F, ell, p->seed ^ (salt * 7 + 2), p->tol, mr, pad, &ok));
+    rc = logged_kind(ws, ptt_round_sketch(ws->s, NULL, F, ell_field, p->seed ^ (salt * 7 + 2), p->tol, mr, pad, &ok),
+                     PTT_RXN_KIND_FIELD);
     if (rc) return rc;
     if (ok) return PTT_OK;
     /* fallback: the deterministic composition T(T(a) + T(b)) */
     ws->sketch_fallbacks++;
-    if ((rc = logged(ws, ptt_round(ws->a, p->tol, mr)))) return rc;
-    if ((rc = logged(ws, ptt_round(ws->b, p->tol, mr)))) return rc;
+    if ((rc = logged_kind(ws, ptt_round(ws->a, p->tol, mr), KIND_NONE))) return rc;
+    if ((rc = logged_kind(ws, ptt_round(ws->b, p->tol, mr), KIND_NONE))) return rc;
     if ((rc = ptt_axpby(1.0, ws->a, 1.0, ws->b, F))) return rc;
-    return logged(ws, ptt_round(F, p->tol, mr));
+    return logged_kind(ws, ptt_round(F, p->tol, mr), PTT_RXN_KIND_FIELD);
 }
 
-int ptt_rxn_burgers_rk2_step_sketch(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int* ell, int pad) {
+int ptt_rxn_burgers_rk2_step_sketch_kinds(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int* ell,
+                                          int pad) {
     int rc, d, mr[PTT_MAX_DIM + 1];
     if (!u || !ws || !p || !ell) return PTT_ERR_ARG;
     if ((rc = ptt_tt_shape(u, &d, NULL, NULL))) return rc;
     for (int k = 0; k <= d; k++) mr[k] = p->maxrank;
+    const int* ep = ell + (size_t)PTT_RXN_KIND_PRODUCT * (d + 1);
+    const int* ef = ell + (size_t)PTT_RXN_KIND_FIELD * (d + 1);
+    const int* es = ell + (size_t)PTT_RXN_KIND_STAGE * (d + 1);
     step_begin(ws);
-    if ((rc = F_sketch(u, ws->k, ws, p, ell, pad, 1))) return rc;
+    if ((rc = F_sketch(u, ws->k, ws, p, ep, ef, pad, 1))) return rc;
     if ((rc = ptt_axpby(1.0, u, 0.5 * p->dt, ws->k, ws->t))) return rc;
-    if ((rc = sketch_or_round(ws->t, ws->us, ws, p, mr, ell, pad, 3))) return rc;
-    if ((rc = F_sketch(ws->us, ws->k, ws, p, ell, pad, 4))) return rc;
+    if ((rc = sketch_or_round(ws->t, ws->us, ws, p, mr, es, pad, 3))) return rc;
+    if ((rc = F_sketch(ws->us, ws->k, ws, p, ep, ef, pad, 4))) return rc;
     if ((rc = ptt_axpby(1.0, u, p->dt, ws->k, ws->t))) return rc;
-    return sketch_or_round(ws->t, u, ws, p, mr, ell, pad, 5);
+    return sketch_or_round(ws->t, u, ws, p, mr, es, pad, 5);
+}
+
+int ptt_rxn_burgers_rk2_step_sketch(ptt_tt* u, ptt_rxn_ws* ws, const ptt_rxn_params* p, const int* ell, int pad) {
+    int d, rc;
+    if (!u || !ws || !p || !ell) return PTT_ERR_ARG;
+    if ((rc = ptt_tt_shape(u, &d, NULL, NULL))) return rc;
+    int all[PTT_RXN_KINDS * (PTT_MAX_DIM + 1)];
+    for (int t = 0; t < PTT_RXN_KINDS; t++) memcpy(all + (size_t)t * (d + 1), ell, sizeof(int) * (d + 1));
+    return ptt_rxn_burgers_rk2_step_sketch_kinds(u, ws, p, all, pad);
 }
