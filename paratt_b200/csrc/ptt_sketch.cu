@@ -308,6 +308,23 @@ static int sketch_round(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* 
         const int Lk = L[k], Lp = L[k + 1], nk = n[k];
         const int rxk = rx[k], ryk = ry[k], rxp = rx[k + 1], ryp = ry[k + 1];
         GemmB g;
+        if (!y) {
+            // x alone (the partner is the ones train): A_j = W_{k+1} G_j^T
+            // stored with row index j + n jx, so that
+            // W_k[ix, c] = sum_{j, jx} x[ix, j, jx] A_j[jx, c] is one GEMM
+            // with K = n r_{k+1} over the core's right unfolding
+            g = GemmB{ws + oW[k + 1], 1, Rp, 0, 0,
+                      ws + oG[k], (long long)Lk * nk, 1, Lk, 0,
+                      ws + oA, nk, (long long)nk * Rp, 1, 0,
+                      (int)Rp, Lk, Lp, nk, 1, 1.0, 0.0};
+            if ((rc = gemm(c, g))) return rc;
+            g = GemmB{xc[k], 1, rxk, 0, 0,
+                      ws + oA, 1, (long long)nk * Rp, 0, 0,
+                      ws + oW[k], 1, R[k], 0, 0,
+                      rxk, Lk, (int)(nk * Rp), 1, 1, 1.0, 0.0};
+            if ((rc = gemm(c, g))) return rc;
+            continue;
+        }
         // A_j = W_{k+1} G_j^T   (Rp x Lk), j < n
         g = GemmB{ws + oW[k + 1], 1, Rp, 0, 0,
                   ws + oG[k], (long long)Lk * nk, 1, Lk, 0,
@@ -341,19 +358,28 @@ static int sketch_round(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* 
         const long long Rp = R[k + 1];
         const int nk = n[k], rxk = rx[k], ryk = ry[k], rxp = rx[k + 1], ryp = ry[k + 1];
         GemmB g;
-        // P[ix][q][c] = sum_ky M[c, ky + ryk ix] y_right[ky, q]
-        g = GemmB{M, 1, r, (long long)r * ryk, 0,
-                  yc[k], 1, ryk, 0, 0,
-                  ws + oP, 1, r, (long long)r * nk * ryp, 0,
-                  r, nk * ryp, ryk, rxk, 1, 1.0, 0.0};
-        if ((rc = gemm(c, g))) return rc;
-        // Z[c + r j, ly + ryp jx] = sum_ix P[ix][j + n ly][c] x[ix, j, jx]
         double* Zp = (k == d - 1) ? z->hd.core[k] : ws + oZ;
-        g = GemmB{ws + oP, 1, (long long)r * nk * ryp, r, (long long)r * nk,
-                  xc[k], 1, (long long)rxk * nk, rxk, 0,
-                  Zp, 1, (long long)r * nk * ryp, r, (long long)r * nk,
-                  r, rxp, rxk, nk, ryp, 1.0, 0.0};
-        if ((rc = gemm(c, g))) return rc;
+        if (!y) {
+            // x alone: Z = M x_k, (r x r_k) times the core's right unfolding
+            g = GemmB{M, 1, r, 0, 0,
+                      xc[k], 1, rxk, 0, 0,
+                      Zp, 1, r, 0, 0,
+                      r, nk * rxp, rxk, 1, 1, 1.0, 0.0};
+            if ((rc = gemm(c, g))) return rc;
+        } else {
+            // P[ix][q][c] = sum_ky M[c, ky + ryk ix] y_right[ky, q]
+            g = GemmB{M, 1, r, (long long)r * ryk, 0,
+                      yc[k], 1, ryk, 0, 0,
+                      ws + oP, 1, r, (long long)r * nk * ryp, 0,
+                      r, nk * ryp, ryk, rxk, 1, 1.0, 0.0};
+            if ((rc = gemm(c, g))) return rc;
+            // Z[c + r j, ly + ryp jx] = sum_ix P[ix][j + n ly][c] x[ix, j, jx]
+            g = GemmB{ws + oP, 1, (long long)r * nk * ryp, r, (long long)r * nk,
+                      xc[k], 1, (long long)rxk * nk, rxk, 0,
+                      Zp, 1, (long long)r * nk * ryp, r, (long long)r * nk,
+                      r, rxp, rxk, nk, ryp, 1.0, 0.0};
+            if ((rc = gemm(c, g))) return rc;
+        }
         if (k == d - 1) {
             zr[k] = r;
             zr[d] = 1;
