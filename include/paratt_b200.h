@@ -72,6 +72,14 @@ PTT_API int ptt_ctx_kernel_time(ptt_ctx* ctx, double* ms, long long* count);
 /* Algorithmic work of the timed launches: bytes for PTT_TIME_TSQR (16 m c
  * per factorisation of an m x c unfolding), flops for PTT_TIME_GEMM. */
 PTT_API int ptt_ctx_kernel_work(ptt_ctx* ctx, double* work);
+/* Replay roundings from CUDA graphs (no counterpart in the reference): with
+ * on != 0, each rounding's launch sequence is captured once per distinct
+ * (train, ranks, threshold, workspace) and replayed from then on; results are
+ * identical.  Off by default; bypassed while kernels are timed and inside a
+ * capture the caller makes.  The cache holds device pointers: a train
+ * destroyed and recreated at the same address reuses its graph, which is
+ * correct because the graph reads the descriptor at run time. */
+PTT_API int ptt_ctx_graphs(ptt_ctx* ctx, int on);
 /* Overwrite a device buffer of twice the L2 size on the context's stream. */
 PTT_API int ptt_ctx_flush_l2(ptt_ctx* ctx);
 /* Page-lock / release host memory for fast transfers (cudaHostRegister). */

@@ -79,6 +79,7 @@ _SIGS = {
     "ptt_op_sum": (_i, [_p, _dp, _i, _d, _p]),
     "ptt_ctx_mark": (_i, [_p, _i]),
     "ptt_ctx_fixed_plans": (_i, [_p, _i]),
+    "ptt_ctx_graphs": (_i, [_p, _i]),
     "ptt_ctx_elapsed": (_i, [_p, _i, _i, _dp]),
     "ptt_ctx_time_kernels": (_i, [_p, _i]),
     "ptt_ctx_kernel_time": (_i, [_p, _dp, C.POINTER(C.c_longlong)]),
@@ -166,6 +167,10 @@ class Context:
     def fixed_plans(self, on=True):
         """Size rounding plans by capacity (no rank read-back) when on."""
         _check(lib().ptt_ctx_fixed_plans(self.h, 1 if on else 0))
+
+    def graphs(self, on=True):
+        """Replay roundings from cached CUDA graphs when on (same results)."""
+        _check(lib().ptt_ctx_graphs(self.h, 1 if on else 0))
 
     def mark(self, slot):
         _check(lib().ptt_ctx_mark(self.h, slot))

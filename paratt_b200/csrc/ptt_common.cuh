@@ -1,5 +1,6 @@
 // Internal definitions shared by the paratt_b200 CUDA sources.
 #pragma once
+#include <functional>
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -66,6 +67,9 @@ struct ptt_ctx {
     struct ptt_ctx* lanes[PTT_MAX_LANES];
     int nlanes;
     int shared_status;            // d_status belongs to the parent context
+    // captured launch sequences (ptt_graph_run): on/off and the cache
+    int graphs;
+    void* graph_cache;
 };
 
 // Event pair around a launch of kind `kind` when that class is being timed.
@@ -117,6 +121,13 @@ int ptt_swap(ptt_tt* t, int k0, int k1);
 // Rounding stages (ptt_round.cu): phases 1 = orthogonalise, 2 = truncate
 // (input left-orthogonal), 4 = QR of core `only` alone.
 int ptt_round_phases(ptt_tt* x, double tol, const int* maxrank, int phases, int only);
+// Run issue() (kernel launches on c->stream only: no allocation, no
+// synchronisation) directly, or -- with graphs on and no kernel timing --
+// through a CUDA graph cached under `key`, which must hold every value the
+// launches bake in (pointers, sizes, scalars): captured on the first call,
+// replayed afterwards.
+int ptt_graph_run(ptt_ctx* c, const void* key, size_t keylen, const std::function<int()>& issue);
+void ptt_graph_clear(ptt_ctx* c);
 int ptt_round_phases_rk(ptt_tt* x, const int* rk, double tol, const int* maxrank, int phases, int only);
 double ptt_round_threshold(const ptt_tt* x, double tol);
 

@@ -6,6 +6,9 @@
 // out-of-place kernels.  Actual ranks are kept on the device (DevDesc).
 #include "ptt_common.cuh"
 
+#include <string>
+#include <unordered_map>
+
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -74,11 +77,75 @@ extern "C" ptt_ctx* ptt_ctx_create(int device) {
     return c;
 }
 
+// ---------------------------------------------------------------------------
+// graph cache
+// ---------------------------------------------------------------------------
+namespace {
+struct GraphEntry {
+    cudaGraphExec_t exec;
+    long long kernels;  // kernel launches the graph holds
+};
+struct GraphCache {
+    std::unordered_map<std::string, GraphEntry> map;
+};
+constexpr size_t GRAPH_CACHE_MAX = 512;
+}  // namespace
+
+void ptt_graph_clear(ptt_ctx* c) {
+    GraphCache* g = (GraphCache*)c->graph_cache;
+    if (!g) return;
+    for (auto& e : g->map) cudaGraphExecDestroy(e.second.exec);
+    g->map.clear();
+}
+
+int ptt_graph_run(ptt_ctx* c, const void* key, size_t keylen, const std::function<int()>& issue) {
+    if (!c->graphs || c->tkind) return issue();
+    // inside a capture the caller makes, the launches join the caller's graph
+    cudaStreamCaptureStatus cs;
+    PTT_CUDA(cudaStreamIsCapturing(c->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return issue();
+    GraphCache* g = (GraphCache*)c->graph_cache;
+    if (!g) c->graph_cache = g = new GraphCache();
+    std::string k((const char*)key, keylen);
+    auto it = g->map.find(k);
+    if (it != g->map.end()) {
+        PTT_CUDA(cudaGraphLaunch(it->second.exec, c->stream));
+        c->launches += it->second.kernels;
+        return PTT_OK;
+    }
+    if (g->map.size() >= GRAPH_CACHE_MAX) ptt_graph_clear(c);
+    PTT_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const long long l0 = c->launches;
+    int rc = issue();
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (rc || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return rc ? rc : ptt_cuda_check(e, "graph capture");
+    }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return ptt_cuda_check(e, "graph instantiate");
+    g->map.emplace(std::move(k), GraphEntry{exec, c->launches - l0});
+    PTT_CUDA(cudaGraphLaunch(exec, c->stream));
+    return PTT_OK;
+}
+
+extern "C" int ptt_ctx_graphs(ptt_ctx* c, int on) {
+    if (!c) return ptt_set_error(PTT_ERR_ARG, "null context");
+    c->graphs = on ? 1 : 0;
+    return PTT_OK;
+}
+
 extern "C" void ptt_ctx_destroy(ptt_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     cudaStreamSynchronize(c->side);
+    ptt_graph_clear(c);
+    delete (GraphCache*)c->graph_cache;
     cudaFree(c->ws);
     cudaFree(c->ws2);
     cudaFree(c->ws3);

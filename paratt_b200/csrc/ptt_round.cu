@@ -897,68 +897,99 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
         PTT_LAUNCHED(c);
         return PTT_OK;
     };
-    if (phases & 4) {
-        const int i = only;
-        double* wsb;
-        Plan pl = bond(i, &wsb);
-        if ((rc = factor(i, LEFT, Wl[i], pl, wsb))) return rc;
-        if ((rc = apply(i, 1, LEFT, Wl[i], rk[i + 1]))) return rc;
-        k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i, -1, &pl.info->q, pl.info);
-        PTT_LAUNCHED(c);
-        return PTT_OK;
+    // the launches below, as one unit that can be captured and replayed;
+    // the key holds every value they bake in
+    struct Key {
+        int tag, d, phases, only;
+        const void *dd, *ws, *cnt, *status, *stats;
+        long long stride;
+        int Pcap;
+        double delta;
+        int n[PTT_MAX_DIM], rk[PTT_MAX_DIM + 1], mr[PTT_MAX_DIM + 1];
+    } key;
+    memset(&key, 0, sizeof(key));
+    key.tag = 1;
+    key.d = d;
+    key.phases = phases;
+    key.only = only;
+    key.dd = x->dd;
+    key.ws = ws;
+    key.cnt = c->d_counters;
+    key.status = c->d_status;
+    key.stats = c->d_stats;
+    key.stride = wp.stride;
+    key.Pcap = wp.Pcap;
+    key.delta = delta;
+    for (int i = 0; i < d; i++) key.n[i] = x->n[i];
+    for (int i = 0; i <= d; i++) {
+        key.rk[i] = rk[i];
+        key.mr[i] = maxr ? maxr[i] : -1;
     }
-    if (phases & 1) {
-        int Wmax = 1, cmax = 1;
-        for (int i = 0; i < d - 1; i++) {
-            cmax = rk[i + 1] > cmax ? rk[i + 1] : cmax;
+    auto issue = [&]() -> int {
+        if (phases & 4) {
+            const int i = only;
             double* wsb;
             Plan pl = bond(i, &wsb);
             if ((rc = factor(i, LEFT, Wl[i], pl, wsb))) return rc;
-            Wmax = Wl[i] > Wmax ? Wl[i] : Wmax;
-            const long long ncap = (long long)x->n[i + 1] * rk[i + 2];
-            int gy = (int)((ncap + GT - 1) / GT);
-            if (gy > 4096) gy = 4096;
-            k_gemm_rx<<<dim3(1, gy), 256, 0, c->stream>>>(x->dd, i + 1, pl, wsb);
+            if ((rc = apply(i, 1, LEFT, Wl[i], rk[i + 1]))) return rc;
+            k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i, -1, &pl.info->q, pl.info);
             PTT_LAUNCHED(c);
-            k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i + 1, -1, &pl.info->q, pl.info);
-            PTT_LAUNCHED(c);
+            return PTT_OK;
         }
-        if (d > 1) {
-            if ((rc = apply(0, d - 1, LEFT, Wmax, cmax))) return rc;
-            k_wswap<<<1, 64, 0, c->stream>>>(x->dd, 0, d - 1, c->d_status);
-            PTT_LAUNCHED(c);
+        if (phases & 1) {
+            int Wmax = 1, cmax = 1;
+            for (int i = 0; i < d - 1; i++) {
+                cmax = rk[i + 1] > cmax ? rk[i + 1] : cmax;
+                double* wsb;
+                Plan pl = bond(i, &wsb);
+                if ((rc = factor(i, LEFT, Wl[i], pl, wsb))) return rc;
+                Wmax = Wl[i] > Wmax ? Wl[i] : Wmax;
+                const long long ncap = (long long)x->n[i + 1] * rk[i + 2];
+                int gy = (int)((ncap + GT - 1) / GT);
+                if (gy > 4096) gy = 4096;
+                k_gemm_rx<<<dim3(1, gy), 256, 0, c->stream>>>(x->dd, i + 1, pl, wsb);
+                PTT_LAUNCHED(c);
+                k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i + 1, -1, &pl.info->q, pl.info);
+                PTT_LAUNCHED(c);
+            }
+            if (d > 1) {
+                if ((rc = apply(0, d - 1, LEFT, Wmax, cmax))) return rc;
+                k_wswap<<<1, 64, 0, c->stream>>>(x->dd, 0, d - 1, c->d_status);
+                PTT_LAUNCHED(c);
+            }
         }
-    }
-    if (phases & 2) {
-        int Wmax = 1, cmax = 1;
-        for (int i = d - 1; i >= 1; i--) {
-            cmax = rk[i] > cmax ? rk[i] : cmax;
-            double* wsb;
-            Plan pl = bond(i, &wsb);
-            if ((rc = factor(i, RIGHT_T, Wr[i], pl, wsb))) return rc;
-            Wmax = Wr[i] > Wmax ? Wr[i] : Wmax;
-            const int mr = maxr ? maxr[i] : rk[i];
-            ptt_time_begin(c, PTT_TIME_SVD);
-            k_svd_jacobi<32><<<1, svd_nt<32>(), svd_smem<32>(), c->stream>>>(pl, wsb, delta, mr, i, c->d_status);
-            ptt_time_end(c, PTT_TIME_SVD);
-            PTT_LAUNCHED(c);
-            const long long mcap = (long long)rk[i - 1] * x->n[i - 1];
-            int gx = (int)((mcap + GT - 1) / GT);
-            if (gx > 4096) gx = 4096;
-            k_gemm_xm<<<dim3(gx, 1), 256, 0, c->stream>>>(x->dd, i - 1, pl, wsb);
-            PTT_LAUNCHED(c);
-            k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i, i - 1, -1, &pl.info->rank, pl.info);
-            PTT_LAUNCHED(c);
+        if (phases & 2) {
+            int Wmax = 1, cmax = 1;
+            for (int i = d - 1; i >= 1; i--) {
+                cmax = rk[i] > cmax ? rk[i] : cmax;
+                double* wsb;
+                Plan pl = bond(i, &wsb);
+                if ((rc = factor(i, RIGHT_T, Wr[i], pl, wsb))) return rc;
+                Wmax = Wr[i] > Wmax ? Wr[i] : Wmax;
+                const int mr = maxr ? maxr[i] : rk[i];
+                ptt_time_begin(c, PTT_TIME_SVD);
+                k_svd_jacobi<32><<<1, svd_nt<32>(), svd_smem<32>(), c->stream>>>(pl, wsb, delta, mr, i, c->d_status);
+                ptt_time_end(c, PTT_TIME_SVD);
+                PTT_LAUNCHED(c);
+                const long long mcap = (long long)rk[i - 1] * x->n[i - 1];
+                int gx = (int)((mcap + GT - 1) / GT);
+                if (gx > 4096) gx = 4096;
+                k_gemm_xm<<<dim3(gx, 1), 256, 0, c->stream>>>(x->dd, i - 1, pl, wsb);
+                PTT_LAUNCHED(c);
+                k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i, i - 1, -1, &pl.info->rank, pl.info);
+                PTT_LAUNCHED(c);
+            }
+            if (d > 1) {
+                k_svd_replay_b<<<dim3(4, d - 1), 256, replay_smem<32>(), c->stream>>>(base, ws, wp.stride, 1);
+                PTT_LAUNCHED(c);
+                if ((rc = apply(1, d - 1, RIGHT_T, Wmax, cmax))) return rc;
+                k_wswap<<<1, 64, 0, c->stream>>>(x->dd, 1, d, c->d_status);
+                PTT_LAUNCHED(c);
+            }
         }
-        if (d > 1) {
-            k_svd_replay_b<<<dim3(4, d - 1), 256, replay_smem<32>(), c->stream>>>(base, ws, wp.stride, 1);
-            PTT_LAUNCHED(c);
-            if ((rc = apply(1, d - 1, RIGHT_T, Wmax, cmax))) return rc;
-            k_wswap<<<1, 64, 0, c->stream>>>(x->dd, 1, d, c->d_status);
-            PTT_LAUNCHED(c);
-        }
-    }
-    return PTT_OK;
+        return PTT_OK;
+    };
+    return ptt_graph_run(c, &key, sizeof(key), issue);
 }
 
 }  // namespace

@@ -99,3 +99,30 @@ def test_fixed_plans_same_result(ctx):
     a, b = A.get(), B.get()
     assert O.ranks_of(a) == O.ranks_of(b)
     assert O.rel_diff_exact(a, b) <= 1e-13
+
+
+def test_graph_replay_bit_exact(ctx):
+    """Roundings replayed from cached CUDA graphs equal direct launches
+    bit for bit: first call (capture), repeats (replay), other ranks (a
+    second graph), and a train at a new address."""
+    shapes = [([6, 5, 7, 4, 6], [1, 6, 8, 9, 6, 1], [1, 3, 4, 5, 2, 1]),
+              ([9, 8, 7, 6], [1, 7, 12, 5, 1], [1, 4, 6, 3, 1])]
+    for dims, full, keep in shapes:
+        x = gapped_tt(dims, full, 12, keep)
+        tol = 1e-6 * O.norm(x)
+        A = P.TT.from_cores(ctx, x)
+        A.round(tol, 64)
+        a = A.get()
+        A.close()
+        ctx.graphs(True)
+        try:
+            for _ in range(3):
+                B = P.TT.from_cores(ctx, x)
+                B.round(tol, 64)
+                b = B.get()
+                B.close()
+                assert O.ranks_of(a) == O.ranks_of(b)
+                for u, v in zip(a, b):
+                    np.testing.assert_array_equal(u, v)
+        finally:
+            ctx.graphs(False)
