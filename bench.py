@@ -513,10 +513,13 @@ def run_one_step(args, local_rank):
         ls.step(U)  # first learned step: the MLP and sketch workspaces warm up
         step = ls.step
     ctx.sync()
-    print(f"launches before the measured step: {ctx.launches}", flush=True)
+    l0 = ctx.launches
+    print(f"launches before the measured step: {l0}", flush=True)
+    ctx.mark(0)
     step(U)
+    ctx.mark(1)
     ctx.sync()
-    print(f"launches in the step: {ctx.launches}", flush=True)
+    print(f"launches in the step: {ctx.launches - l0}, device time {ctx.elapsed_ms(0, 1):.2f} ms", flush=True)
     ctx.close()
     return 0
 
