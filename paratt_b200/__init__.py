@@ -80,6 +80,8 @@ _SIGS = {
     "ptt_ctx_mark": (_i, [_p, _i]),
     "ptt_ctx_fixed_plans": (_i, [_p, _i]),
     "ptt_ctx_graphs": (_i, [_p, _i]),
+    "ptt_ctx_cholqr": (_i, [_p, _i]),
+    "ptt_ctx_qr_counts": (_i, [_p, C.POINTER(C.c_longlong)]),
     "ptt_ctx_elapsed": (_i, [_p, _i, _i, _dp]),
     "ptt_ctx_time_kernels": (_i, [_p, _i]),
     "ptt_ctx_kernel_time": (_i, [_p, _dp, C.POINTER(C.c_longlong)]),
@@ -167,6 +169,17 @@ class Context:
     def fixed_plans(self, on=True):
         """Size rounding plans by capacity (no rank read-back) when on."""
         _check(lib().ptt_ctx_fixed_plans(self.h, 1 if on else 0))
+
+    def cholqr(self, on=True):
+        """Cholesky-QR factorisation of unfoldings with <= 32 columns (default
+        on; off = Householder TSQR only)."""
+        _check(lib().ptt_ctx_cholqr(self.h, 1 if on else 0))
+
+    def qr_counts(self):
+        """(finished by Cholesky QR, fell back to Householder, Gram stages)."""
+        v = (C.c_longlong * 3)()
+        _check(lib().ptt_ctx_qr_counts(self.h, v))
+        return tuple(int(a) for a in v)
 
     def graphs(self, on=True):
         """Replay roundings from cached CUDA graphs when on (same results)."""

@@ -22,6 +22,7 @@ static int lane_ctx(ptt_ctx* c, int i, ptt_ctx** out) {
         l->shared_status = 1;
         c->lanes[c->nlanes++] = l;
     }
+    c->lanes[i]->no_cholqr = c->no_cholqr;
     *out = c->lanes[i];
     return PTT_OK;
 }

@@ -70,6 +70,11 @@ struct ptt_ctx {
     // captured launch sequences (ptt_graph_run): on/off and the cache
     int graphs;
     void* graph_cache;
+    // Cholesky-QR factorisation of unfoldings with <= 32 columns: 0 = used
+    // (default), 1 = Householder TSQR only; device counters [finished,
+    // fell back, Gram stages of the finished ones]
+    int no_cholqr;
+    long long* d_qrstat;
 };
 
 // Event pair around a launch of kind `kind` when that class is being timed.

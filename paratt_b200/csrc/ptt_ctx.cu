@@ -70,6 +70,8 @@ extern "C" ptt_ctx* ptt_ctx_create(int device) {
         ptt_cuda_check(cudaMalloc(&c->d_stats, sizeof(double) * PTT_STAT_LEN * (PTT_MAX_DIM + 1)), "cudaMalloc stats") ||
         ptt_cuda_check(cudaMalloc(&c->d_work, sizeof(double) * 4), "cudaMalloc work") ||
         ptt_cuda_check(cudaMemset(c->d_work, 0, sizeof(double) * 4), "memset") ||
+        ptt_cuda_check(cudaMalloc(&c->d_qrstat, sizeof(long long) * 4), "cudaMalloc qr counters") ||
+        ptt_cuda_check(cudaMemset(c->d_qrstat, 0, sizeof(long long) * 4), "memset") ||
         ptt_cuda_check(cudaMemset(c->d_stats, 0, sizeof(double) * PTT_STAT_LEN * (PTT_MAX_DIM + 1)), "memset")) {
         free(c);
         return NULL;
@@ -133,6 +135,26 @@ int ptt_graph_run(ptt_ctx* c, const void* key, size_t keylen, const std::functio
     return PTT_OK;
 }
 
+extern "C" int ptt_ctx_cholqr(ptt_ctx* c, int on) {
+    if (!c) return ptt_set_error(PTT_ERR_ARG, "null context");
+    c->no_cholqr = on ? 0 : 1;
+    return PTT_OK;
+}
+
+extern "C" int ptt_ctx_qr_counts(ptt_ctx* c, long long* out) {
+    if (!c || !out) return ptt_set_error(PTT_ERR_ARG, "ptt_ctx_qr_counts: bad arguments");
+    long long v[4] = {0, 0, 0, 0};
+    for (int i = -1; i < c->nlanes; i++) {
+        ptt_ctx* l = i < 0 ? c : c->lanes[i];
+        long long w[4];
+        PTT_CUDA(cudaStreamSynchronize(l->stream));
+        PTT_CUDA(cudaMemcpy(w, l->d_qrstat, sizeof(w), cudaMemcpyDeviceToHost));
+        for (int j = 0; j < 3; j++) v[j] += w[j];
+    }
+    for (int j = 0; j < 3; j++) out[j] = v[j];
+    return PTT_OK;
+}
+
 extern "C" int ptt_ctx_graphs(ptt_ctx* c, int on) {
     if (!c) return ptt_set_error(PTT_ERR_ARG, "null context");
     c->graphs = on ? 1 : 0;
@@ -156,6 +178,7 @@ extern "C" void ptt_ctx_destroy(ptt_ctx* c) {
     cudaFree(c->d_scalars);
     cudaFree(c->d_stats);
     cudaFree(c->d_work);
+    cudaFree(c->d_qrstat);
     cudaFreeHost(c->h_scalars);
     for (int i = 0; i < 64; i++)
         if (c->marks[i]) cudaEventDestroy(c->marks[i]);

@@ -18,6 +18,7 @@
 // a rounding is a fixed launch sequence with no host synchronisation.
 #include "ptt_tsqr.cuh"
 
+#include <cooperative_groups.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -801,6 +802,7 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
 }
 
 #include "ptt_wtsqr.cuh"
+#include "ptt_cholqr.cuh"
 
 // Rounding of a train whose ranks stay <= 32 on the warp-level TSQR.
 // Per bond only the factorisation, the small product that moves R (or U S)
@@ -818,6 +820,8 @@ static bool wt_fits(const ptt_tt* x, const int* rk) {
     return true;
 }
 
+static int g_cq_csmax = cq::CSMAX;  // cluster size the device can schedule
+
 static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr, int phases, int only) {
     using namespace wt;
     ptt_ctx* c = x->ctx;
@@ -829,6 +833,28 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
         PTT_CUDA(cudaFuncSetAttribute(k_wfactor<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wfactor_smem()));
         PTT_CUDA(cudaFuncSetAttribute(k_wfactor<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wfactor_smem()));
         PTT_CUDA(cudaFuncSetAttribute(k_wfactor<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wfactor_smem()));
+        for (auto f : {(const void*)cq::k_cq_factor<16>, (const void*)cq::k_cq_factor<24>,
+                       (const void*)cq::k_cq_factor<32>}) {
+            PTT_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cq::SMEM_MAX));
+            PTT_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        }
+        // largest cluster the device can hold with one full-size CTA per SM
+        cudaLaunchConfig_t qc = {};
+        qc.gridDim = dim3(cq::CSMAX);
+        qc.blockDim = dim3(cq::NT);
+        qc.dynamicSmemBytes = cq::SMEM_MAX;
+        cudaLaunchAttribute qa[1];
+        qa[0].id = cudaLaunchAttributeClusterDimension;
+        qa[0].val.clusterDim.x = cq::CSMAX;
+        qa[0].val.clusterDim.y = 1;
+        qa[0].val.clusterDim.z = 1;
+        qc.attrs = qa;
+        qc.numAttrs = 1;
+        int ncl = 0;
+        if (cudaOccupancyMaxActiveClusters(&ncl, (const void*)cq::k_cq_factor<32>, &qc) != cudaSuccess || ncl < 1) {
+            cudaGetLastError();
+            g_cq_csmax = 8;
+        }
         wattr = true;
     }
     int Wl[PTT_MAX_DIM], Wr[PTT_MAX_DIM], Pcap = 1;
@@ -850,6 +876,10 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
     o += (long long)Pcap * 32;
     wp.o_tn = o;
     o += (long long)Pcap * 32;
+    // Cholesky-QR record
+    const int use_cq = c->no_cholqr ? 0 : 1;
+    wp.o_cq = o;
+    o += cq::REGION;
     wp.stride = (o + 31) / 32 * 32;
     wp.Pcap = Pcap;
     base.o_Rn = wp.o_R;  // root R = slot 0 (read by the SVD and the R product)
@@ -875,12 +905,45 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
         const dim3 g((W + FPB - 1) / FPB), b(32 * FPB);
         const size_t sm = wfactor_smem();
         ptt_time_begin(c, PTT_TIME_TSQR);
+        if (use_cq) {
+            // Cholesky QR by one cluster; the TSQR below only runs for a bond
+            // it did not finish
+            const int mp = W * 32;  // bound on the unfolding's rows
+            int cs = 1;
+            while (cs < g_cq_csmax && (long long)cs * cq::RTARGET < mp) cs <<= 1;
+            int rpb = (mp + cs - 1) / cs;
+            const int rmax = cb == 16 ? cq::rpb_max<16>() : (cb == 24 ? cq::rpb_max<24>() : cq::rpb_max<32>());
+            if (rpb > rmax) {  // too tall for the cluster's shared memory: falls back at once
+                cs = 1;
+                rpb = 1;
+            }
+            cudaLaunchConfig_t lc = {};
+            lc.gridDim = dim3(cs);
+            lc.blockDim = dim3(cq::NT);
+            lc.dynamicSmemBytes = cb == 16 ? cq::smem<16>(rpb) : (cb == 24 ? cq::smem<24>(rpb) : cq::smem<32>(rpb));
+            lc.stream = c->stream;
+            cudaLaunchAttribute la[1];
+            la[0].id = cudaLaunchAttributeClusterDimension;
+            la[0].val.clusterDim.x = cs;
+            la[0].val.clusterDim.y = 1;
+            la[0].val.clusterDim.z = 1;
+            lc.attrs = la;
+            lc.numAttrs = 1;
+            const DevDesc* dd = x->dd;
+            if (cb == 16)
+                PTT_CUDA(cudaLaunchKernelEx(&lc, cq::k_cq_factor<16>, dd, i, mode, pl, wp, wsb, rpb, c->d_qrstat));
+            else if (cb == 24)
+                PTT_CUDA(cudaLaunchKernelEx(&lc, cq::k_cq_factor<24>, dd, i, mode, pl, wp, wsb, rpb, c->d_qrstat));
+            else
+                PTT_CUDA(cudaLaunchKernelEx(&lc, cq::k_cq_factor<32>, dd, i, mode, pl, wp, wsb, rpb, c->d_qrstat));
+            PTT_LAUNCHED(c);
+        }
         if (cb == 16)
-            k_wfactor<16><<<g, b, sm, c->stream>>>(x->dd, i, mode, pl, wp, wsb, c->d_status);
+            k_wfactor<16><<<g, b, sm, c->stream>>>(x->dd, i, mode, pl, wp, wsb, use_cq, c->d_status);
         else if (cb == 24)
-            k_wfactor<24><<<g, b, sm, c->stream>>>(x->dd, i, mode, pl, wp, wsb, c->d_status);
+            k_wfactor<24><<<g, b, sm, c->stream>>>(x->dd, i, mode, pl, wp, wsb, use_cq, c->d_status);
         else
-            k_wfactor<32><<<g, b, sm, c->stream>>>(x->dd, i, mode, pl, wp, wsb, c->d_status);
+            k_wfactor<32><<<g, b, sm, c->stream>>>(x->dd, i, mode, pl, wp, wsb, use_cq, c->d_status);
         ptt_time_end(c, PTT_TIME_TSQR);
         PTT_LAUNCHED(c);
         return PTT_OK;
@@ -889,18 +952,30 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
         const int cb = cbound(cmax);
         const dim3 g((Wmax + WPB - 1) / WPB, nb), b(32 * WPB);
         if (cb == 16)
-            k_wapply<16><<<g, b, 0, c->stream>>>(x->dd, k0, mode, base, wp, ws);
+            k_wapply<16><<<g, b, 0, c->stream>>>(x->dd, k0, mode, base, wp, ws, use_cq);
         else if (cb == 24)
-            k_wapply<24><<<g, b, 0, c->stream>>>(x->dd, k0, mode, base, wp, ws);
+            k_wapply<24><<<g, b, 0, c->stream>>>(x->dd, k0, mode, base, wp, ws, use_cq);
         else
-            k_wapply<32><<<g, b, 0, c->stream>>>(x->dd, k0, mode, base, wp, ws);
+            k_wapply<32><<<g, b, 0, c->stream>>>(x->dd, k0, mode, base, wp, ws, use_cq);
         PTT_LAUNCHED(c);
+        if (use_cq && mode == RIGHT_T) {  // LEFT: the cluster wrote Q already
+            long long gx = ((long long)Wmax * 32 + cq::NT - 1) / cq::NT;
+            gx = gx < 1 ? 1 : (gx > 4096 ? 4096 : gx);
+            const dim3 gw((unsigned)gx, nb);
+            if (cb == 16)
+                cq::k_cq_write<16><<<gw, cq::NT, 0, c->stream>>>(x->dd, k0, base, wp, ws);
+            else if (cb == 24)
+                cq::k_cq_write<24><<<gw, cq::NT, 0, c->stream>>>(x->dd, k0, base, wp, ws);
+            else
+                cq::k_cq_write<32><<<gw, cq::NT, 0, c->stream>>>(x->dd, k0, base, wp, ws);
+            PTT_LAUNCHED(c);
+        }
         return PTT_OK;
     };
     // the launches below, as one unit that can be captured and replayed;
     // the key holds every value they bake in
     struct Key {
-        int tag, d, phases, only;
+        int tag, d, phases, only, use_cq;
         const void *dd, *ws, *cnt, *status, *stats;
         long long stride;
         int Pcap;
@@ -912,6 +987,7 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
     key.d = d;
     key.phases = phases;
     key.only = only;
+    key.use_cq = use_cq;
     key.dd = x->dd;
     key.ws = ws;
     key.cnt = c->d_counters;

@@ -32,6 +32,7 @@ constexpr int WPB = 4;  // warps per block
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int SLOT = 32 * 32;
 constexpr int PMAX = 4096;  // leaves per bond (m <= 131072)
+constexpr int CQ_DONE = 1;  // Cholesky-QR state: the bond is factored, skip it here
 
 // Per-bond tree records.  Bond (core) k's region starts at ws + k * stride;
 // offsets are in doubles within a region; counters of bond k at cnt + k * Pcap.
@@ -39,6 +40,7 @@ struct WP {
     long long o_R;   // (2 Pcap - 1) slots, R or vectors, row-major 32 x 32
     long long o_tl;  // leaf taus, Pcap x 32
     long long o_tn;  // node taus, Pcap x 32
+    long long o_cq;  // Cholesky-QR record (ptt_cholqr.cuh); its first int is the bond's state
     long long stride;
     int Pcap;
     int* cnt;        // zero between launches; reset by the combining warp
@@ -186,8 +188,10 @@ __host__ __device__ constexpr size_t wfactor_smem() { return sizeof(double) * FP
 
 template <int CB>
 __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, int mode, Plan pl, WP wp,
-                                                      double* wsb, int* status) {
+                                                      double* wsb, int use_cq, int* status) {
     extern __shared__ double fsm[];
+    // a bond the Cholesky sequence finished needs no Householder factors
+    if (use_cq && *(const int*)(wsb + wp.o_cq) == CQ_DONE) return;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int p = blockIdx.x * FPB + wid;
     const View A = make_view(D, k, mode, false);
@@ -203,7 +207,7 @@ __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, i
         return;  // uniform over the block
     }
     if (blockIdx.x * FPB >= W) return;  // uniform over the block
-    if (pl.work && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(pl.work, 16.0 * (double)m * (double)c);
+    if (pl.work && !use_cq && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(pl.work, 16.0 * (double)m * (double)c);
     double* sw = fsm + wid * (32 * 33);
     const bool valid = p < W;
     const int r0 = p * 32;
@@ -298,12 +302,14 @@ __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, i
 //   LEFT:    B = I_q;                       out (m x q, column-major) -> alt[k]
 //   RIGHT_T: B = V_r (Bn, row-major 32 x KC); out(row, col) -> alt[k][row * rank + col]
 template <int CB>
-__global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, int mode, Plan pl, WP wp, double* ws) {
+__global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, int mode, Plan pl, WP wp, double* ws,
+                                                     int use_cq) {
     __shared__ double sh[WPB][32 * 33];
     __shared__ double stau[WPB][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int k = k0 + blockIdx.y;
     double* wsb = ws + (long long)k * wp.stride;
+    if (use_cq && *(const int*)(wsb + wp.o_cq) == CQ_DONE) return;  // k_cq_write forms this Q
     const Info* info = (const Info*)(wsb + pl.o_info_d);
     if (info->status) return;
     const int m = info->m, c = info->c, q = info->q;
