@@ -106,7 +106,9 @@ PTT_API int ptt_tt_reserve(ptt_tt* t, const int* rank_cap);
  * ranks[k]*n[k]*ranks[k+1] doubles).  Synchronous w.r.t. the host buffers. */
 PTT_API int ptt_tt_set(ptt_tt* t, const int* ranks, const double* const* cores);
 /* Read ranks (d+1 ints) and, if cores != NULL, the cores (each cores[k]
- * must hold ranks[k]*n[k]*ranks[k+1] doubles).  Synchronises the stream. */
+ * must hold ranks[k]*n[k]*ranks[k+1] doubles).  Synchronises the stream;
+ * with cores != NULL it also returns (and clears), like ptt_ctx_synchronize,
+ * a device-side error raised by the context's earlier work. */
 PTT_API int ptt_tt_get(ptt_tt* t, int* ranks, double* const* cores);
 PTT_API int ptt_tt_get_ranks(ptt_tt* t, int* ranks);
 /* dst <- src (shapes must agree, capacity of dst must cover src). */

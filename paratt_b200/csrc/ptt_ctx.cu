@@ -565,7 +565,9 @@ extern "C" int ptt_tt_get(ptt_tt* t, int* ranks, double* const* cores) {
             PTT_CUDA(cudaMemcpyAsync(cores[k], t->hd.core[k], cnt * sizeof(double), cudaMemcpyDefault,
                                      t->ctx->stream));
         }
-        PTT_CUDA(cudaStreamSynchronize(t->ctx->stream));
+        // the data is on the host: report (and clear) a device-side error of
+        // the work that produced it, as ptt_ctx_synchronize does
+        return ptt_ctx_synchronize(t->ctx);
     }
     return PTT_OK;
 }

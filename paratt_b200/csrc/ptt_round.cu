@@ -261,6 +261,7 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws
     __shared__ double s_sig[CT + 2];
     __shared__ int s_ord[CT + 2];
     __shared__ int s_rot;
+    __shared__ double s_thr2;
     const int tid = threadIdx.x;
     const int grp = tid >> 3, p = tid & 7;  // 64 pair slots x 8 lanes
     const unsigned gm = group_mask8(tid);
@@ -293,6 +294,18 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws
         }
         if (tid == 0) s_rot = 0;
         __syncthreads();
+        // Columns below the numerical-rank threshold (sqrt(q) eps_LAPACK times
+        // the largest column norm) are rounding noise: rotating noise against
+        // noise is a random walk that never meets the relative criterion, and
+        // their values are discarded by the rank rule anyway, so pairs with
+        // such a column are left alone.
+        if (tid == 0) {
+            double mx = 0.0;
+            for (int j = 0; j < qq; j++) mx = fmax(mx, s_nrm[j]);
+            s_thr2 = (double)q * 1.232595164407831e-32 * mx;  // (sqrt(q) * 2^-53)^2 * max |a_j|^2
+        }
+        __syncthreads();
+        const double thr2 = s_thr2;
         int myrot = 0;
         for (int rd = 0; rd < qq - 1; rd++) {
             for (int i = grp; i < qq / 2; i += SVD_NT / 8) {
@@ -314,7 +327,7 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws
                 const double ga = gsum8(g0 + g1, gm);
                 const double al = s_nrm[pc], be = s_nrm[qc];
                 double cs = 1.0, sn = 0.0;
-                if (ga != 0.0 && fabs(ga) > tol * sqrt(al * be)) {
+                if (ga != 0.0 && al > thr2 && be > thr2 && fabs(ga) > tol * sqrt(al * be)) {
                     // t = tan(theta) = sign(z)/(|z| + sqrt(1+z^2)), z = (be-al)/(2 ga),
                     // written as g2/(dd + sign(dd) sqrt(dd^2 + g2^2)): one sqrt, one reciprocal
                     const double dd = be - al, g2 = 2.0 * ga;

@@ -118,14 +118,132 @@ __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, long long zoff, int kpe
     }
 }
 
+// Split-K for C small (M, N <= 32) and K long: slice blockIdx.x of batch
+// blockIdx.y multiplies the KS-long chunk of K; every element of the chunk is
+// requested before the first product (the loads of one slice are in flight
+// together), and the slice's partial C goes to part[slice][b][M][N].
+constexpr int KS = 128;
+constexpr size_t SKINNY_SMEM = sizeof(double) * 2 * KS * 33;
+
+__global__ void __launch_bounds__(256) k_gemm_skinny(GemmB g, int ns, double* part) {
+    extern __shared__ double ssm[];
+    double* sA = ssm;            // [KS][33]: sA[k][i] = A(i, k0 + k)
+    double* sB = ssm + KS * 33;  // [KS][33]: sB[k][j] = B(k0 + k, j)
+    const int sl = blockIdx.x, bz = blockIdx.y;
+    const int b1 = bz % g.nb1, b2 = bz / g.nb1;
+    const double* A = g.A + b1 * g.ab1 + b2 * g.ab2;
+    const double* B = g.B + b1 * g.bb1 + b2 * g.bb2;
+    const int k0 = sl * KS;
+    const int kn = (g.K - k0) < KS ? (g.K - k0) : KS;
+    const int tid = threadIdx.x;
+    // A chunk: M x kn, walked along whichever index is contiguous
+    {
+        const int tot = g.M * KS;
+        for (int base = tid; base < tot; base += 256 * 8) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int e = base + u * 256;
+                int i, k;
+                if (g.acs == 1) {
+                    k = e % KS;
+                    i = e / KS;
+                } else {
+                    i = e % g.M;
+                    k = e / g.M;
+                }
+                v[u] = (e < tot && k < kn) ? A[(long long)i * g.ars + (long long)(k0 + k) * g.acs] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int e = base + u * 256;
+                if (e < tot) {
+                    int i, k;
+                    if (g.acs == 1) {
+                        k = e % KS;
+                        i = e / KS;
+                    } else {
+                        i = e % g.M;
+                        k = e / g.M;
+                    }
+                    sA[k * 33 + i] = v[u];
+                }
+            }
+        }
+    }
+    {
+        const int tot = g.N * KS;
+        for (int base = tid; base < tot; base += 256 * 8) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int e = base + u * 256;
+                int j, k;
+                if (g.brs == 1) {
+                    k = e % KS;
+                    j = e / KS;
+                } else {
+                    j = e % g.N;
+                    k = e / g.N;
+                }
+                v[u] = (e < tot && k < kn) ? B[(long long)(k0 + k) * g.brs + (long long)j * g.bcs] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int e = base + u * 256;
+                if (e < tot) {
+                    int j, k;
+                    if (g.brs == 1) {
+                        k = e % KS;
+                        j = e / KS;
+                    } else {
+                        j = e % g.N;
+                        k = e / g.N;
+                    }
+                    sB[k * 33 + j] = v[u];
+                }
+            }
+        }
+    }
+    __syncthreads();
+    const int tx = tid & 15, ty = tid >> 4;
+    double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll 8
+    for (int k = 0; k < KS; k++) {
+        const double a0 = sA[k * 33 + ty], a1 = sA[k * 33 + ty + 16];
+        const double c0 = sB[k * 33 + tx], c1 = sB[k * 33 + tx + 16];
+        acc[0][0] = fma(a0, c0, acc[0][0]);
+        acc[0][1] = fma(a0, c1, acc[0][1]);
+        acc[1][0] = fma(a1, c0, acc[1][0]);
+        acc[1][1] = fma(a1, c1, acc[1][1]);
+    }
+    const long long nb = (long long)g.nb1 * g.nb2;
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+            const int i = ty + 16 * a, j = tx + 16 * b;
+            if (i < g.M && j < g.N) part[(((long long)sl * nb + bz) * g.M + i) * g.N + j] = acc[a][b];
+        }
+}
+
 // C[b][r][c] = alpha * sum_s part[s][b][r][c] + beta * C, slices in order
+// (eight slices' loads in flight at a time)
 __global__ void k_gemm_red(GemmB g, int ns, const double* part) {
     const long long nb = (long long)g.nb1 * g.nb2;
     const long long per = (long long)g.M * g.N, tot = per * nb;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
          e += (long long)gridDim.x * blockDim.x) {
         double acc = 0.0;
-        for (int s = 0; s < ns; s++) acc += part[(long long)s * tot + e];
+        int s = 0;
+        for (; s + 8 <= ns; s += 8) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) v[u] = part[(long long)(s + u) * tot + e];
+#pragma unroll
+            for (int u = 0; u < 8; u++) acc += v[u];
+        }
+        for (; s < ns; s++) acc += part[(long long)s * tot + e];
         const int bz = (int)(e / per);
         const long long rc = e - (long long)bz * per;
         const int gr = (int)(rc / g.N), gc = (int)(rc - (long long)gr * g.N);
@@ -139,6 +257,30 @@ int gemm(ptt_ctx* c, const GemmB& g) {
     if (g.M <= 0 || g.N <= 0 || g.nb1 <= 0 || g.nb2 <= 0) return PTT_OK;
     const long long nb = (long long)g.nb1 * g.nb2;
     if (c->tkind == PTT_TIME_GEMM) c->hwork[PTT_TIME_GEMM] += 2.0 * g.M * (double)g.N * g.K * (double)nb;
+    if (g.M <= 32 && g.N <= 32 && g.K >= 2 * KS) {
+        // small C, long K: one block per KS-long slice of K, then the ordered sum
+        const int ns = (g.K + KS - 1) / KS;
+        if (nb > 65535) return ptt_set_error(PTT_ERR_CAPACITY, "sketch contraction: %lld batches", nb);
+        const size_t need = sizeof(double) * (size_t)ns * (size_t)nb * (size_t)g.M * (size_t)g.N;
+        int rc = ptt_ws3_reserve(c, need);
+        if (rc) return rc;
+        double* part = (double*)c->ws3;
+        static bool attr = false;
+        if (!attr) {
+            PTT_CUDA(cudaFuncSetAttribute(k_gemm_skinny, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SKINNY_SMEM));
+            attr = true;
+        }
+        ptt_time_begin(c, PTT_TIME_GEMM);
+        k_gemm_skinny<<<dim3(ns, (unsigned)nb), 256, SKINNY_SMEM, c->stream>>>(g, ns, part);
+        PTT_LAUNCHED(c);
+        const long long tot = (long long)g.M * g.N * nb;
+        long long nbk = (tot + 255) / 256;
+        if (nbk > 1184) nbk = 1184;
+        k_gemm_red<<<(int)nbk, 256, 0, c->stream>>>(g, ns, part);
+        PTT_LAUNCHED(c);
+        ptt_time_end(c, PTT_TIME_GEMM);
+        return PTT_OK;
+    }
     const bool big = g.M >= 48 && g.N >= 48;
     const int TM = big ? 64 : 32;
     dim3 grid((g.M + TM - 1) / TM, (g.N + TM - 1) / TM, 1);

@@ -126,3 +126,35 @@ def test_graph_replay_bit_exact(ctx):
                     np.testing.assert_array_equal(u, v)
         finally:
             ctx.graphs(False)
+
+
+@pytest.mark.parametrize("decay", [1e-3, 1e-9, 1e-14, 0.0])
+def test_cholqr_matches_householder(ctx, decay):
+    """The Cholesky-QR factorisation (default for <= 32 columns) and the
+    Householder TSQR give the same rounding, for well separated, graded,
+    near-singular and exactly rank-deficient unfoldings; the Cholesky path is
+    the one that ran."""
+    dims, full, keep = [9, 16, 7, 12, 8], [1, 7, 12, 10, 9, 1], [1, 4, 6, 5, 3, 1]
+    x = gapped_tt(dims, full, 13, keep, decay=decay)
+    if decay == 0.0:
+        x = O.axpby(1.0, x, 0.5, x)  # repeated columns in every unfolding (ranks <= 24)
+    tol = 1e-6 * O.norm(x)
+    got = {}
+    for on in (False, True):
+        ctx.cholqr(on)
+        before = ctx.qr_counts()
+        X = P.TT.from_cores(ctx, x)
+        X.round(tol, 64)
+        got[on] = X.get()
+        X.close()
+        after = ctx.qr_counts()
+        if on:
+            assert after[0] > before[0]
+        else:
+            assert after == before
+    ctx.cholqr(True)
+    ref = O.round_tt(x, tol, 10**6)
+    for on in (False, True):
+        assert O.ranks_of(got[on]) == O.ranks_of(ref)
+        assert O.rel_diff_exact(got[on], ref) <= 1e-12
+    assert O.rel_diff_exact(got[True], got[False]) <= 1e-12
