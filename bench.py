@@ -22,9 +22,10 @@ the events).  `err_vs_plain` is the relative L2 difference between one
 learned and one plain step from the same state; `fallback_rate` the share of
 sketch roundings the judge sent back to the deterministic path.  `e2e` is the
 learned method with the state on the host (page-locked): upload, step,
-download every step, timed by the host clock.  `roofline` is the dominant
-kernel class (TSQR factorisation) timed launch by launch with events during
-the learned steps.  `cpu_baseline` / `--impl reference` time the reference's
+download every step, timed by the host clock.  `roofline` is the
+factorisation class (per bond: the cluster Cholesky QR, with the Householder
+TSQR for a bond it does not finish) timed launch by launch with events during
+a second pass of the learned steps.  `cpu_baseline` / `--impl reference` time the reference's
 own C (oracle/_ref/libparatt_ref.so: paratt_truncate, pattacHadamard,
 attac_tt_axpby) composing the same RK2 step on this host's cores.
 """
@@ -307,7 +308,7 @@ def run_ours(args, rank, world, local_rank):
     hbm, src = peaks()
     achieved = (kwork / 1e9) / (ktime_ms / 1e3) if ktime_ms > 0 else 0.0  # GB/s
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "traffic": None, "kernel": "TSQR factorisation (k_wfactor, k_tsqr_factor)",
+            "frac": achieved / hbm, "traffic": None, "kernel": "factorisation: k_cq_factor (cluster Cholesky QR), k_wfactor/k_tsqr_factor fallback",
             "launches": klaunch, "avg_launch_us": 1e3 * ktime_ms / max(klaunch, 1),
             "algorithmic_bytes_per_launch": kwork / max(klaunch, 1),
             "timing": "event pair per launch in a second pass of the same K learned steps",
