@@ -308,7 +308,12 @@ def run_ours(args, rank, world, local_rank):
     hbm, src = peaks()
     achieved = (kwork / 1e9) / (ktime_ms / 1e3) if ktime_ms > 0 else 0.0  # GB/s
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "traffic": None, "kernel": "factorisation: k_cq_factor (cluster Cholesky QR), k_wfactor/k_tsqr_factor fallback",
+            "frac": achieved / hbm,
+            # DRAM read + write of one k_cq_factor<16> launch of this step
+            # (an ~3072 x <= 16 unfolding), from an ncu --set full capture
+            "traffic": 376576.0,
+            "traffic_source": "ncu: one k_cq_factor<16> launch of the learned step (m ~3072, c <= 16)",
+            "kernel": "factorisation: k_cq_factor (cluster Cholesky QR), k_wfactor/k_tsqr_factor fallback",
             "launches": klaunch, "avg_launch_us": 1e3 * ktime_ms / max(klaunch, 1),
             "algorithmic_bytes_per_launch": kwork / max(klaunch, 1),
             "timing": "event pair per launch in a second pass of the same K learned steps",

@@ -88,6 +88,12 @@ PTT_API int ptt_ctx_graphs(ptt_ctx* ctx, int on);
  * and its batch workers: [0] factorisations finished by Cholesky QR, [1] fell
  * back, [2] Gram stages of the finished ones (synchronises). */
 PTT_API int ptt_ctx_cholqr(ptt_ctx* ctx, int on);
+/* Programmatic dependent launch of the rounding's kernel chain (no counterpart
+ * in the reference): with on != 0 (the default) each kernel of a rounding may
+ * be scheduled while its predecessor finishes and waits on the device for it
+ * before touching memory, which hides most of the launch gap; on == 0 launches
+ * them plainly.  Results are identical. */
+PTT_API int ptt_ctx_pdl(ptt_ctx* ctx, int on);
 PTT_API int ptt_ctx_qr_counts(ptt_ctx* ctx, long long* out3);
 /* Overwrite a device buffer of twice the L2 size on the context's stream. */
 PTT_API int ptt_ctx_flush_l2(ptt_ctx* ctx);

@@ -81,6 +81,7 @@ _SIGS = {
     "ptt_ctx_fixed_plans": (_i, [_p, _i]),
     "ptt_ctx_graphs": (_i, [_p, _i]),
     "ptt_ctx_cholqr": (_i, [_p, _i]),
+    "ptt_ctx_pdl": (_i, [_p, _i]),
     "ptt_ctx_qr_counts": (_i, [_p, C.POINTER(C.c_longlong)]),
     "ptt_ctx_elapsed": (_i, [_p, _i, _i, _dp]),
     "ptt_ctx_time_kernels": (_i, [_p, _i]),
@@ -174,6 +175,10 @@ class Context:
         """Cholesky-QR factorisation of unfoldings with <= 32 columns (default
         on; off = Householder TSQR only)."""
         _check(lib().ptt_ctx_cholqr(self.h, 1 if on else 0))
+
+    def pdl(self, on=True):
+        """Programmatic dependent launch of the rounding chain (default on)."""
+        _check(lib().ptt_ctx_pdl(self.h, 1 if on else 0))
 
     def qr_counts(self):
         """(finished by Cholesky QR, fell back to Householder, Gram stages)."""

@@ -23,6 +23,7 @@ static int lane_ctx(ptt_ctx* c, int i, ptt_ctx** out) {
         c->lanes[c->nlanes++] = l;
     }
     c->lanes[i]->no_cholqr = c->no_cholqr;
+    c->lanes[i]->no_pdl = c->no_pdl;
     *out = c->lanes[i];
     return PTT_OK;
 }

@@ -202,6 +202,7 @@ __device__ __forceinline__ void warp_first_order(const double* sG, int c, double
 template <int CB>
 __global__ void __launch_bounds__(NT, 1) k_cq_factor(const DevDesc* D, int k, int mode, Plan pl, wt::WP wp,
                                                   double* wsb, int rpb, long long* qstat) {
+    PTT_PDL_ENTRY();
     constexpr int XP = Cfg<CB>::XP, TS = Cfg<CB>::TS, UP = Cfg<CB>::UP, EPT = Cfg<CB>::EPT;
     cg::cluster_group cl = cg::this_cluster();
     const int CS = (int)cl.num_blocks();
@@ -464,6 +465,7 @@ __global__ void __launch_bounds__(NT, 1) k_cq_factor(const DevDesc* D, int k, in
 // (row-major rows of c), V_r in Bn (row-major 32 x KC).
 template <int CB>
 __global__ void __launch_bounds__(NT) k_cq_write(const DevDesc* D, int k0, Plan pl, wt::WP wp, double* ws) {
+    PTT_PDL_ENTRY();
     __shared__ double sB[32 * 33];
     const int k = k0 + blockIdx.y;
     double* wsb = ws + (long long)k * wp.stride;

@@ -75,7 +75,38 @@ struct ptt_ctx {
     // fell back, Gram stages of the finished ones]
     int no_cholqr;
     long long* d_qrstat;
+    // programmatic dependent launch of the rounding chain: 0 = used (default)
+    int no_pdl;
+    int capturing;                // inside ptt_graph_run's own capture
 };
+
+// Programmatic dependent launch.  A kernel launched through ptt_launch may be
+// scheduled while the previous kernel on the stream is still running; it must
+// start with PTT_PDL_ENTRY(), which waits (griddepcontrol.wait) until the
+// previous grid has completed and its writes are visible -- before any memory
+// access -- and then lets the next kernel be scheduled in turn.  Launched
+// without the attribute, the two instructions have no effect.
+#define PTT_PDL_ENTRY()                                          \
+    do {                                                         \
+        asm volatile("griddepcontrol.wait;" ::: "memory");       \
+        asm volatile("griddepcontrol.launch_dependents;" ::: ); \
+    } while (0)
+
+template <typename... KArgs, typename... Args>
+static inline cudaError_t ptt_launch(const ptt_ctx* c, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                     Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = (c->no_pdl || c->capturing) ? 0 : 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
 
 // Event pair around a launch of kind `kind` when that class is being timed.
 void ptt_time_begin(ptt_ctx* c, int kind);

@@ -118,7 +118,9 @@ int ptt_graph_run(ptt_ctx* c, const void* key, size_t keylen, const std::functio
     if (g->map.size() >= GRAPH_CACHE_MAX) ptt_graph_clear(c);
     PTT_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     const long long l0 = c->launches;
+    c->capturing = 1;  // plain launches inside the graph
     int rc = issue();
+    c->capturing = 0;
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     if (rc || e != cudaSuccess) {
@@ -132,6 +134,12 @@ int ptt_graph_run(ptt_ctx* c, const void* key, size_t keylen, const std::functio
     if (e != cudaSuccess) return ptt_cuda_check(e, "graph instantiate");
     g->map.emplace(std::move(k), GraphEntry{exec, c->launches - l0});
     PTT_CUDA(cudaGraphLaunch(exec, c->stream));
+    return PTT_OK;
+}
+
+extern "C" int ptt_ctx_pdl(ptt_ctx* c, int on) {
+    if (!c) return ptt_set_error(PTT_ERR_ARG, "null context");
+    c->no_pdl = on ? 0 : 1;
     return PTT_OK;
 }
 
@@ -364,6 +372,7 @@ struct RankVals {
 };
 
 __global__ void k_set_ranks(DevDesc* D, int k0, int cnt, RankVals rv) {
+    PTT_PDL_ENTRY();
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) D->r[k0 + i] = rv.v[i];
 }
 
@@ -371,7 +380,7 @@ int ptt_set_ranks_async(ptt_tt* t, int k0, const int* vals, int cnt) {
     if (k0 < 0 || cnt < 0 || k0 + cnt > t->d + 1) return ptt_set_error(PTT_ERR_ARG, "rank range");
     RankVals rv;
     memcpy(rv.v, vals, sizeof(int) * cnt);
-    k_set_ranks<<<1, 128, 0, t->ctx->stream>>>(t->dd, k0, cnt, rv);
+    PTT_CUDA(ptt_launch(t->ctx, k_set_ranks, dim3(1), dim3(128), 0, t->dd, k0, cnt, rv));
     PTT_LAUNCHED(t->ctx);
     return PTT_OK;
 }

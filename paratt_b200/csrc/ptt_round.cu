@@ -252,6 +252,7 @@ __host__ __device__ constexpr int svd_nt() {
 template <int CT>
 __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws, double delta, int maxr, int bond,
                                                        int* status) {
+    PTT_PDL_ENTRY();
     constexpr int SVD_NT = svd_nt<CT>();
     extern __shared__ double sm[];
     constexpr int S = CT + 1;
@@ -278,6 +279,7 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws
     double2* rot = (double2*)(ws + pl.o_rot);
     const int npair = (CT + 2) / 2;
     const double tol = (double)(c < 16 ? 16 : c) * 2.220446049250313e-16;
+    const double tol2 = tol * tol;  // |ga| > tol sqrt(al be), compared in squares
     int sweeps = 0;
     bool conv = (qq < 2);
     for (int sw = 0; sw < MAXSW && !conv; sw++) {
@@ -327,7 +329,7 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws
                 const double ga = gsum8(g0 + g1, gm);
                 const double al = s_nrm[pc], be = s_nrm[qc];
                 double cs = 1.0, sn = 0.0;
-                if (ga != 0.0 && al > thr2 && be > thr2 && fabs(ga) > tol * sqrt(al * be)) {
+                if (ga != 0.0 && al > thr2 && be > thr2 && ga * ga > tol2 * (al * be)) {
                     // t = tan(theta) = sign(z)/(|z| + sqrt(1+z^2)), z = (be-al)/(2 ga),
                     // written as g2/(dd + sign(dd) sqrt(dd^2 + g2^2)): one sqrt, one reciprocal
                     const double dd = be - al, g2 = 2.0 * ga;
@@ -490,6 +492,7 @@ __global__ void __launch_bounds__(256) k_svd_replay(Plan pl, double* ws) {
 
 // the same for bonds k0 .. k0 + gridDim.y - 1, bond k's records at ws + k * stride
 __global__ void __launch_bounds__(256) k_svd_replay_b(Plan pl, double* ws, long long stride, int k0) {
+    PTT_PDL_ENTRY();
     double* wsb = ws + (long long)(k0 + blockIdx.y) * stride;
     svd_replay_body(pl, wsb, (const Info*)(wsb + pl.o_info_d), blockIdx.x);
 }
@@ -555,6 +558,7 @@ __device__ void gemm_tile(GV A, GV B, double* C, long long crs, long long ccs, i
 
 // core[i+1] <- R * core[i+1]   (R = root factor, q x c, row-major CT)
 __global__ void __launch_bounds__(256) k_gemm_rx(const DevDesc* D, int i1, Plan pl, double* ws) {
+    PTT_PDL_ENTRY();
     if (pl.info->status) return;
     const int q = pl.info->q, c = pl.info->c;
     const int N = D->n[i1] * D->r[i1 + 1];
@@ -569,6 +573,7 @@ __global__ void __launch_bounds__(256) k_gemm_rx(const DevDesc* D, int i1, Plan 
 
 // core[i-1] <- core[i-1] * US   (US = c x rank, column-major ld CT)
 __global__ void __launch_bounds__(256) k_gemm_xm(const DevDesc* D, int im1, Plan pl, double* ws) {
+    PTT_PDL_ENTRY();
     if (pl.info->status) return;
     const int c = pl.info->c, rank = pl.info->rank;
     const int M = D->r[im1] * D->n[im1];
@@ -583,6 +588,7 @@ __global__ void __launch_bounds__(256) k_gemm_xm(const DevDesc* D, int im1, Plan
 
 // publish a bond's new rank and swap the two rewritten cores
 __global__ void k_bond_finalize(DevDesc* D, int kq, int ka, int kb, const int* val, const Info* info) {
+    PTT_PDL_ENTRY();
     if (threadIdx.x == 0 && info->status == 0) {
         D->r[kq] = *val;
         double* t = D->core[ka];
@@ -935,13 +941,15 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
             lc.blockDim = dim3(cq::NT);
             lc.dynamicSmemBytes = cb == 16 ? cq::smem<16>(rpb) : (cb == 24 ? cq::smem<24>(rpb) : cq::smem<32>(rpb));
             lc.stream = c->stream;
-            cudaLaunchAttribute la[1];
+            cudaLaunchAttribute la[2];
             la[0].id = cudaLaunchAttributeClusterDimension;
             la[0].val.clusterDim.x = cs;
             la[0].val.clusterDim.y = 1;
             la[0].val.clusterDim.z = 1;
+            la[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            la[1].val.programmaticStreamSerializationAllowed = 1;
             lc.attrs = la;
-            lc.numAttrs = 1;
+            lc.numAttrs = (c->no_pdl || c->capturing) ? 1 : 2;
             const DevDesc* dd = x->dd;
             if (cb == 16)
                 PTT_CUDA(cudaLaunchKernelEx(&lc, cq::k_cq_factor<16>, dd, i, mode, pl, wp, wsb, rpb, c->d_qrstat));
@@ -952,11 +960,11 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
             PTT_LAUNCHED(c);
         }
         if (cb == 16)
-            k_wfactor<16><<<g, b, sm, c->stream>>>(x->dd, i, mode, pl, wp, wsb, use_cq, c->d_status);
+            PTT_CUDA(ptt_launch(c, k_wfactor<16>, dim3(g), dim3(b), sm, x->dd, i, mode, pl, wp, wsb, use_cq, c->d_status));
         else if (cb == 24)
-            k_wfactor<24><<<g, b, sm, c->stream>>>(x->dd, i, mode, pl, wp, wsb, use_cq, c->d_status);
+            PTT_CUDA(ptt_launch(c, k_wfactor<24>, dim3(g), dim3(b), sm, x->dd, i, mode, pl, wp, wsb, use_cq, c->d_status));
         else
-            k_wfactor<32><<<g, b, sm, c->stream>>>(x->dd, i, mode, pl, wp, wsb, use_cq, c->d_status);
+            PTT_CUDA(ptt_launch(c, k_wfactor<32>, dim3(g), dim3(b), sm, x->dd, i, mode, pl, wp, wsb, use_cq, c->d_status));
         ptt_time_end(c, PTT_TIME_TSQR);
         PTT_LAUNCHED(c);
         return PTT_OK;
@@ -965,22 +973,22 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
         const int cb = cbound(cmax);
         const dim3 g((Wmax + WPB - 1) / WPB, nb), b(32 * WPB);
         if (cb == 16)
-            k_wapply<16><<<g, b, 0, c->stream>>>(x->dd, k0, mode, base, wp, ws, use_cq);
+            PTT_CUDA(ptt_launch(c, k_wapply<16>, dim3(g), dim3(b), 0, x->dd, k0, mode, base, wp, ws, use_cq));
         else if (cb == 24)
-            k_wapply<24><<<g, b, 0, c->stream>>>(x->dd, k0, mode, base, wp, ws, use_cq);
+            PTT_CUDA(ptt_launch(c, k_wapply<24>, dim3(g), dim3(b), 0, x->dd, k0, mode, base, wp, ws, use_cq));
         else
-            k_wapply<32><<<g, b, 0, c->stream>>>(x->dd, k0, mode, base, wp, ws, use_cq);
+            PTT_CUDA(ptt_launch(c, k_wapply<32>, dim3(g), dim3(b), 0, x->dd, k0, mode, base, wp, ws, use_cq));
         PTT_LAUNCHED(c);
         if (use_cq && mode == RIGHT_T) {  // LEFT: the cluster wrote Q already
             long long gx = ((long long)Wmax * 32 + cq::NT - 1) / cq::NT;
             gx = gx < 1 ? 1 : (gx > 4096 ? 4096 : gx);
             const dim3 gw((unsigned)gx, nb);
             if (cb == 16)
-                cq::k_cq_write<16><<<gw, cq::NT, 0, c->stream>>>(x->dd, k0, base, wp, ws);
+                PTT_CUDA(ptt_launch(c, cq::k_cq_write<16>, dim3(gw), dim3(cq::NT), 0, x->dd, k0, base, wp, ws));
             else if (cb == 24)
-                cq::k_cq_write<24><<<gw, cq::NT, 0, c->stream>>>(x->dd, k0, base, wp, ws);
+                PTT_CUDA(ptt_launch(c, cq::k_cq_write<24>, dim3(gw), dim3(cq::NT), 0, x->dd, k0, base, wp, ws));
             else
-                cq::k_cq_write<32><<<gw, cq::NT, 0, c->stream>>>(x->dd, k0, base, wp, ws);
+                PTT_CUDA(ptt_launch(c, cq::k_cq_write<32>, dim3(gw), dim3(cq::NT), 0, x->dd, k0, base, wp, ws));
             PTT_LAUNCHED(c);
         }
         return PTT_OK;
@@ -1021,7 +1029,7 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
             Plan pl = bond(i, &wsb);
             if ((rc = factor(i, LEFT, Wl[i], pl, wsb))) return rc;
             if ((rc = apply(i, 1, LEFT, Wl[i], rk[i + 1]))) return rc;
-            k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i, -1, &pl.info->q, pl.info);
+            PTT_CUDA(ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i + 1, i, -1, &pl.info->q, pl.info));
             PTT_LAUNCHED(c);
             return PTT_OK;
         }
@@ -1036,14 +1044,14 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
                 const long long ncap = (long long)x->n[i + 1] * rk[i + 2];
                 int gy = (int)((ncap + GT - 1) / GT);
                 if (gy > 4096) gy = 4096;
-                k_gemm_rx<<<dim3(1, gy), 256, 0, c->stream>>>(x->dd, i + 1, pl, wsb);
+                PTT_CUDA(ptt_launch(c, k_gemm_rx, dim3(dim3(1, gy)), dim3(256), 0, x->dd, i + 1, pl, wsb));
                 PTT_LAUNCHED(c);
-                k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i + 1, -1, &pl.info->q, pl.info);
+                PTT_CUDA(ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i + 1, i + 1, -1, &pl.info->q, pl.info));
                 PTT_LAUNCHED(c);
             }
             if (d > 1) {
                 if ((rc = apply(0, d - 1, LEFT, Wmax, cmax))) return rc;
-                k_wswap<<<1, 64, 0, c->stream>>>(x->dd, 0, d - 1, c->d_status);
+                PTT_CUDA(ptt_launch(c, k_wswap, dim3(1), dim3(64), 0, x->dd, 0, d - 1, c->d_status));
                 PTT_LAUNCHED(c);
             }
         }
@@ -1057,22 +1065,22 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
                 Wmax = Wr[i] > Wmax ? Wr[i] : Wmax;
                 const int mr = maxr ? maxr[i] : rk[i];
                 ptt_time_begin(c, PTT_TIME_SVD);
-                k_svd_jacobi<32><<<1, svd_nt<32>(), svd_smem<32>(), c->stream>>>(pl, wsb, delta, mr, i, c->d_status);
+                PTT_CUDA(ptt_launch(c, k_svd_jacobi<32>, dim3(1), dim3(svd_nt<32>()), svd_smem<32>(), pl, wsb, delta, mr, i, c->d_status));
                 ptt_time_end(c, PTT_TIME_SVD);
                 PTT_LAUNCHED(c);
                 const long long mcap = (long long)rk[i - 1] * x->n[i - 1];
                 int gx = (int)((mcap + GT - 1) / GT);
                 if (gx > 4096) gx = 4096;
-                k_gemm_xm<<<dim3(gx, 1), 256, 0, c->stream>>>(x->dd, i - 1, pl, wsb);
+                PTT_CUDA(ptt_launch(c, k_gemm_xm, dim3(dim3(gx, 1)), dim3(256), 0, x->dd, i - 1, pl, wsb));
                 PTT_LAUNCHED(c);
-                k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i, i - 1, -1, &pl.info->rank, pl.info);
+                PTT_CUDA(ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i, i - 1, -1, &pl.info->rank, pl.info));
                 PTT_LAUNCHED(c);
             }
             if (d > 1) {
-                k_svd_replay_b<<<dim3(4, d - 1), 256, replay_smem<32>(), c->stream>>>(base, ws, wp.stride, 1);
+                PTT_CUDA(ptt_launch(c, k_svd_replay_b, dim3(dim3(4, d - 1)), dim3(256), replay_smem<32>(), base, ws, wp.stride, 1));
                 PTT_LAUNCHED(c);
                 if ((rc = apply(1, d - 1, RIGHT_T, Wmax, cmax))) return rc;
-                k_wswap<<<1, 64, 0, c->stream>>>(x->dd, 1, d, c->d_status);
+                PTT_CUDA(ptt_launch(c, k_wswap, dim3(1), dim3(64), 0, x->dd, 1, d, c->d_status));
                 PTT_LAUNCHED(c);
             }
         }

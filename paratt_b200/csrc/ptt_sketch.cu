@@ -37,6 +37,7 @@ struct GemmB {
 // second kernel adds the slices in order (deterministic).
 template <int TM>
 __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, long long zoff, int kper, double* part) {
+    PTT_PDL_ENTRY();
     constexpr int BK = 16;
     constexpr int RT = TM / 16;
     __shared__ double sA[BK][TM + 1];
@@ -126,6 +127,7 @@ constexpr int KS = 128;
 constexpr size_t SKINNY_SMEM = sizeof(double) * 2 * KS * 33;
 
 __global__ void __launch_bounds__(256) k_gemm_skinny(GemmB g, int ns, double* part) {
+    PTT_PDL_ENTRY();
     extern __shared__ double ssm[];
     double* sA = ssm;            // [KS][33]: sA[k][i] = A(i, k0 + k)
     double* sB = ssm + KS * 33;  // [KS][33]: sB[k][j] = B(k0 + k, j)
@@ -230,6 +232,7 @@ __global__ void __launch_bounds__(256) k_gemm_skinny(GemmB g, int ns, double* pa
 // C[b][r][c] = alpha * sum_s part[s][b][r][c] + beta * C, slices in order
 // (eight slices' loads in flight at a time)
 __global__ void k_gemm_red(GemmB g, int ns, const double* part) {
+    PTT_PDL_ENTRY();
     const long long nb = (long long)g.nb1 * g.nb2;
     const long long per = (long long)g.M * g.N, tot = per * nb;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
@@ -271,12 +274,12 @@ int gemm(ptt_ctx* c, const GemmB& g) {
             attr = true;
         }
         ptt_time_begin(c, PTT_TIME_GEMM);
-        k_gemm_skinny<<<dim3(ns, (unsigned)nb), 256, SKINNY_SMEM, c->stream>>>(g, ns, part);
+        PTT_CUDA(ptt_launch(c, k_gemm_skinny, dim3(dim3(ns, (unsigned)nb)), dim3(256), SKINNY_SMEM, g, ns, part));
         PTT_LAUNCHED(c);
         const long long tot = (long long)g.M * g.N * nb;
         long long nbk = (tot + 255) / 256;
         if (nbk > 1184) nbk = 1184;
-        k_gemm_red<<<(int)nbk, 256, 0, c->stream>>>(g, ns, part);
+        PTT_CUDA(ptt_launch(c, k_gemm_red, dim3((int)nbk), dim3(256), 0, g, ns, part));
         PTT_LAUNCHED(c);
         ptt_time_end(c, PTT_TIME_GEMM);
         return PTT_OK;
@@ -308,16 +311,16 @@ int gemm(ptt_ctx* c, const GemmB& g) {
     for (long long z0 = 0; z0 < nz; z0 += 65535) {
         grid.z = (unsigned)((nz - z0) < 65535 ? (nz - z0) : 65535);
         if (big)
-            k_gemm_b<64><<<grid, 256, 0, c->stream>>>(g, z0, kper, part);
+            PTT_CUDA(ptt_launch(c, k_gemm_b<64>, dim3(grid), dim3(256), 0, g, z0, kper, part));
         else
-            k_gemm_b<32><<<grid, 256, 0, c->stream>>>(g, z0, kper, part);
+            PTT_CUDA(ptt_launch(c, k_gemm_b<32>, dim3(grid), dim3(256), 0, g, z0, kper, part));
         PTT_LAUNCHED(c);
     }
     if (part) {
         const long long tot = (long long)g.M * g.N * nb;
         long long nbk = (tot + 255) / 256;
         if (nbk > 1184) nbk = 1184;
-        k_gemm_red<<<(int)nbk, 256, 0, c->stream>>>(g, ns, part);
+        PTT_CUDA(ptt_launch(c, k_gemm_red, dim3((int)nbk), dim3(256), 0, g, ns, part));
         PTT_LAUNCHED(c);
     }
     ptt_time_end(c, PTT_TIME_GEMM);
@@ -336,6 +339,7 @@ __device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
 }
 
 __global__ void k_gauss(double* G, long long cnt, unsigned long long seed, int core) {
+    PTT_PDL_ENTRY();
     const unsigned long long base = splitmix64(seed ^ (0xD1B54A32D192ED03ull * (unsigned long long)(core + 1)));
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt;
          e += (long long)gridDim.x * blockDim.x) {
@@ -348,6 +352,7 @@ __global__ void k_gauss(double* G, long long cnt, unsigned long long seed, int c
 }
 
 __global__ void k_fill(double* p, long long cnt, double v) {
+    PTT_PDL_ENTRY();
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt;
          e += (long long)gridDim.x * blockDim.x)
         p[e] = v;
@@ -438,10 +443,10 @@ static int sketch_round(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* 
 
     for (int k = 1; k < d; k++) {
         const long long cnt = (long long)L[k] * n[k] * L[k + 1];
-        k_gauss<<<blocks_for(cnt), 256, 0, c->stream>>>(ws + oG[k], cnt, seed, k);
+        PTT_CUDA(ptt_launch(c, k_gauss, dim3(blocks_for(cnt)), dim3(256), 0, ws + oG[k], cnt, seed, k));
         PTT_LAUNCHED(c);
     }
-    k_fill<<<1, 32, 0, c->stream>>>(ws + oW[d], 1, 1.0);
+    PTT_CUDA(ptt_launch(c, k_fill, dim3(1), dim3(32), 0, ws + oW[d], 1, 1.0));
     PTT_LAUNCHED(c);
 
     // ---- right-to-left sketch contractions -------------------------------
@@ -490,7 +495,7 @@ static int sketch_round(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* 
     // ---- left-to-right orthogonalisation against the sketch ----------------
     double* M = ws + oM0;
     double* Mn = ws + oM1;
-    k_fill<<<1, 32, 0, c->stream>>>(M, 1, 1.0);
+    PTT_CUDA(ptt_launch(c, k_fill, dim3(1), dim3(32), 0, M, 1, 1.0));
     PTT_LAUNCHED(c);
     int r = 1;
     int zr[PTT_MAX_DIM + 1];

@@ -189,6 +189,7 @@ __host__ __device__ constexpr size_t wfactor_smem() { return sizeof(double) * FP
 template <int CB>
 __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, int mode, Plan pl, WP wp,
                                                       double* wsb, int use_cq, int* status) {
+    PTT_PDL_ENTRY();
     extern __shared__ double fsm[];
     // a bond the Cholesky sequence finished needs no Householder factors
     if (use_cq && *(const int*)(wsb + wp.o_cq) == CQ_DONE) return;
@@ -304,6 +305,7 @@ __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, i
 template <int CB>
 __global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, int mode, Plan pl, WP wp, double* ws,
                                                      int use_cq) {
+    PTT_PDL_ENTRY();
     __shared__ double sh[WPB][32 * 33];
     __shared__ double stau[WPB][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -415,6 +417,7 @@ __global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, i
 
 // swap core and alt of cores [k0, k1) unless an error was recorded
 __global__ void k_wswap(DevDesc* D, int k0, int k1, const int* status) {
+    PTT_PDL_ENTRY();
     if (*status) return;
     for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
         double* t = D->core[k];

@@ -158,3 +158,21 @@ def test_cholqr_matches_householder(ctx, decay):
         assert O.ranks_of(got[on]) == O.ranks_of(ref)
         assert O.rel_diff_exact(got[on], ref) <= 1e-12
     assert O.rel_diff_exact(got[True], got[False]) <= 1e-12
+
+
+def test_pdl_same_bits(ctx):
+    """Programmatic dependent launch changes scheduling only: the rounding is
+    bit-identical with it on (default) and off."""
+    x = gapped_tt([9, 16, 7, 12, 8], [1, 7, 12, 10, 9, 1], 14, [1, 4, 6, 5, 3, 1], decay=1e-10)
+    tol = 1e-8 * O.norm(x)
+    got = []
+    for on in (True, False):
+        ctx.pdl(on)
+        X = P.TT.from_cores(ctx, x)
+        X.round(tol, 64)
+        got.append(X.get())
+        X.close()
+    ctx.pdl(True)
+    assert O.ranks_of(got[0]) == O.ranks_of(got[1])
+    for a, b in zip(*got):
+        np.testing.assert_array_equal(a, b)
