@@ -237,7 +237,10 @@ __global__ void __launch_bounds__(NT, 1) k_cq_factor(const DevDesc* D, int k, in
     const int h = (m - r0) < rpb ? ((m - r0) > 0 ? (m - r0) : 0) : rpb;
     // this CTA's rows: zero, then every element by cp.async (all in flight)
     for (int e = tid; e < h * XP; e += NT) Xs[e] = 0.0;
-    for (int e = tid; e < 32 * 33; e += NT) sT[e] = ((e / 33) == (e % 33) && (e / 33) < c) ? 1.0 : 0.0;
+    for (int e = tid; e < 32 * 33; e += NT) {
+        sT[e] = ((e / 33) == (e % 33) && (e / 33) < c) ? 1.0 : 0.0;
+        sTn[e] = 0.0;
+    }
     __syncthreads();
     {
         const int tot = h * c;
@@ -388,11 +391,13 @@ __global__ void __launch_bounds__(NT, 1) k_cq_factor(const DevDesc* D, int k, in
         }
         if (dec == DONE || dec == FALLBACK) break;
         nst = stage + 1;
-        // R <- R_{stage+1} R (both upper triangular), into the other buffer
+        // R <- R_{stage+1} R (both upper triangular), into the other buffer;
+        // the entries below the diagonal of sTn stay zero from the start
         for (int e = tid; e < 32 * 32; e += NT) {
             const int i = e >> 5, j = e & 31;
+            if (j < i) continue;
             double a0 = 0.0, a1 = 0.0;
-            if (i <= j && j < c) {
+            if (j < c) {
                 int t = i;
                 for (; t + 1 <= j; t += 2) {
                     a0 = fma(sR[i * 33 + t], sT[t * 33 + j], a0);

@@ -345,18 +345,23 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws
                         s_nrm[pc] = al - t * ga;
                         s_nrm[qc] = be + t * ga;
                     }
-                    myrot = 1;
+                    // bit 1: a rotation of a pair whose cosine exceeded 1e-8
+                    myrot |= (ga * ga > 1e-16 * (al * be)) ? 3 : 1;
                 }
                 if (p == 0) rot[((long long)sw * (CT + 1) + rd) * npair + i] = make_double2(cs, sn);
             }
             __syncthreads();
         }
-        if (myrot) atomicOr(&s_rot, 1);
+        if (myrot) atomicOr(&s_rot, myrot);
         __syncthreads();
         if (s_rot == 0) {
             conv = true;
         } else {
             sweeps = sw + 1;
+            // cyclic Jacobi converges quadratically at the end: after a sweep
+            // whose cosines all stayed below 1e-8 the next one would only
+            // meet cosines ~1e-16, so it is not run
+            if (!(s_rot & 2)) conv = true;
         }
     }
     if (!conv && tid == 0) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);

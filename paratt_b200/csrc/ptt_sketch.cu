@@ -38,8 +38,9 @@ struct GemmB {
 template <int TM>
 __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, long long zoff, int kper, double* part) {
     PTT_PDL_ENTRY();
-    constexpr int BK = 16;
+    constexpr int BK = 32;
     constexpr int RT = TM / 16;
+    constexpr int NL = TM * BK / 256;  // elements of each operand tile per thread
     __shared__ double sA[BK][TM + 1];
     __shared__ double sB[BK][TM + 1];
     const long long nb = (long long)g.nb1 * g.nb2;
@@ -62,7 +63,11 @@ __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, long long zoff, int kpe
 #pragma unroll
         for (int j = 0; j < RT; j++) acc[i][j] = 0.0;
     for (int k0 = kbeg; k0 < kend; k0 += BK) {
-        for (int e = tid; e < TM * BK; e += 256) {
+        // every element of both tiles is requested before the first store
+        double va[NL], vb[NL];
+#pragma unroll
+        for (int u = 0; u < NL; u++) {
+            const int e = tid + u * 256;
             int r, kk;
             if (a_colmajor) {
                 r = e % TM;
@@ -72,19 +77,29 @@ __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, long long zoff, int kpe
                 r = e / BK;
             }
             const int gr = m0 + r, gk = k0 + kk;
-            sA[kk][r] = (gr < g.M && gk < kend) ? A[(long long)gr * g.ars + (long long)gk * g.acs] : 0.0;
-        }
-        for (int e = tid; e < TM * BK; e += 256) {
-            int cn, kk;
+            va[u] = (gr < g.M && gk < kend) ? A[(long long)gr * g.ars + (long long)gk * g.acs] : 0.0;
+            int cn, kb;
             if (b_rowfast) {
                 cn = e % TM;
-                kk = e / TM;
+                kb = e / TM;
             } else {
-                kk = e % BK;
+                kb = e % BK;
                 cn = e / BK;
             }
-            const int gk = k0 + kk, gc = n0 + cn;
-            sB[kk][cn] = (gk < kend && gc < g.N) ? B[(long long)gk * g.brs + (long long)gc * g.bcs] : 0.0;
+            const int gkb = k0 + kb, gc = n0 + cn;
+            vb[u] = (gkb < kend && gc < g.N) ? B[(long long)gkb * g.brs + (long long)gc * g.bcs] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < NL; u++) {
+            const int e = tid + u * 256;
+            if (a_colmajor)
+                sA[e / TM][e % TM] = va[u];
+            else
+                sA[e % BK][e / BK] = va[u];
+            if (b_rowfast)
+                sB[e / TM][e % TM] = vb[u];
+            else
+                sB[e % BK][e / BK] = vb[u];
         }
         __syncthreads();
 #pragma unroll
@@ -229,30 +244,44 @@ __global__ void __launch_bounds__(256) k_gemm_skinny(GemmB g, int ns, double* pa
         }
 }
 
-// C[b][r][c] = alpha * sum_s part[s][b][r][c] + beta * C, slices in order
-// (eight slices' loads in flight at a time)
+// C[b][r][c] = alpha * sum_s part[s][b][r][c] + beta * C.  Eight lanes per
+// output: lane l sums the slices l, l + 8, ... in order (eight loads in
+// flight), then the eight sums are added by a fixed butterfly -- the same
+// bits in every lane and on every run.
 __global__ void k_gemm_red(GemmB g, int ns, const double* part) {
     PTT_PDL_ENTRY();
     const long long nb = (long long)g.nb1 * g.nb2;
     const long long per = (long long)g.M * g.N, tot = per * nb;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
-         e += (long long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31, sub = lane & 7;
+    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = wid * 4; base < tot; base += nw * 4) {  // uniform over the warp
+        const long long e = base + (lane >> 3);
+        const bool ok = e < tot;
         double acc = 0.0;
-        int s = 0;
-        for (; s + 8 <= ns; s += 8) {
-            double v[8];
+        if (ok) {
+            for (int s = sub; s < ns; s += 64) {
+                double v[8];
 #pragma unroll
-            for (int u = 0; u < 8; u++) v[u] = part[(long long)(s + u) * tot + e];
+                for (int u = 0; u < 8; u++) {
+                    const int ss = s + 8 * u;
+                    v[u] = ss < ns ? part[(long long)ss * tot + e] : 0.0;
+                }
 #pragma unroll
-            for (int u = 0; u < 8; u++) acc += v[u];
+                for (int u = 0; u < 8; u++) acc += v[u];
+            }
         }
-        for (; s < ns; s++) acc += part[(long long)s * tot + e];
-        const int bz = (int)(e / per);
-        const long long rc = e - (long long)bz * per;
-        const int gr = (int)(rc / g.N), gc = (int)(rc - (long long)gr * g.N);
-        const int b1 = bz % g.nb1, b2 = bz / g.nb1;
-        double* cp = g.C + b1 * g.cb1 + b2 * g.cb2 + (long long)gr * g.crs + (long long)gc * g.ccs;
-        *cp = (g.beta != 0.0) ? fma(g.alpha, acc, g.beta * *cp) : g.alpha * acc;
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+        if (ok && sub == 0) {
+            const int bz = (int)(e / per);
+            const long long rc = e - (long long)bz * per;
+            const int gr = (int)(rc / g.N), gc = (int)(rc - (long long)gr * g.N);
+            const int b1 = bz % g.nb1, b2 = bz / g.nb1;
+            double* cp = g.C + b1 * g.cb1 + b2 * g.cb2 + (long long)gr * g.crs + (long long)gc * g.ccs;
+            *cp = (g.beta != 0.0) ? fma(g.alpha, acc, g.beta * *cp) : g.alpha * acc;
+        }
     }
 }
 
@@ -277,7 +306,7 @@ int gemm(ptt_ctx* c, const GemmB& g) {
         PTT_CUDA(ptt_launch(c, k_gemm_skinny, dim3(dim3(ns, (unsigned)nb)), dim3(256), SKINNY_SMEM, g, ns, part));
         PTT_LAUNCHED(c);
         const long long tot = (long long)g.M * g.N * nb;
-        long long nbk = (tot + 255) / 256;
+        long long nbk = (8 * tot + 255) / 256;  // eight lanes per output
         if (nbk > 1184) nbk = 1184;
         PTT_CUDA(ptt_launch(c, k_gemm_red, dim3((int)nbk), dim3(256), 0, g, ns, part));
         PTT_LAUNCHED(c);
@@ -296,7 +325,7 @@ int gemm(ptt_ctx* c, const GemmB& g) {
         ns = (int)(want < kmax ? want : kmax);
         if (ns > 64) ns = 64;
         kper = (g.K + ns - 1) / ns;
-        kper = (kper + 15) / 16 * 16;
+        kper = (kper + 31) / 32 * 32;
         ns = (g.K + kper - 1) / kper;
     }
     double* part = nullptr;
@@ -318,7 +347,7 @@ int gemm(ptt_ctx* c, const GemmB& g) {
     }
     if (part) {
         const long long tot = (long long)g.M * g.N * nb;
-        long long nbk = (tot + 255) / 256;
+        long long nbk = (8 * tot + 255) / 256;  // eight lanes per output
         if (nbk > 1184) nbk = 1184;
         PTT_CUDA(ptt_launch(c, k_gemm_red, dim3((int)nbk), dim3(256), 0, g, ns, part));
         PTT_LAUNCHED(c);
