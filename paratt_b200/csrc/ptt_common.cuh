@@ -1,5 +1,6 @@
 // Internal definitions shared by the paratt_b200 CUDA sources.
 #pragma once
+#include <atomic>
 #include <functional>
 
 #include <cuda_runtime.h>
@@ -79,6 +80,15 @@ struct ptt_ctx {
     int no_pdl;
     int capturing;                // inside ptt_graph_run's own capture
 };
+
+// Per-device one-time set-up (kernel attributes are per device): returns the
+// current device's bit of `mask` and whether it was already set.
+static inline bool ptt_device_done(std::atomic<unsigned long long>& mask, unsigned long long* bit) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    *bit = 1ull << (dev & 63);
+    return (mask.load() & *bit) != 0;
+}
 
 // Programmatic dependent launch.  A kernel launched through ptt_launch may be
 // scheduled while the previous kernel on the stream is still running; it must

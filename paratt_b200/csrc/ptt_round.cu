@@ -680,8 +680,9 @@ static size_t replay_smem() {
 
 template <int CT>
 static int set_attrs() {
-    static bool done = false;
-    if (done) return PTT_OK;
+    static std::atomic<unsigned long long> done{0};
+    unsigned long long bit;
+    if (ptt_device_done(done, &bit)) return PTT_OK;
     PTT_CUDA(cudaFuncSetAttribute(k_tsqr_factor<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)factor_smem<CT>()));
     PTT_CUDA(cudaFuncSetAttribute(k_apply_leaf<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -692,7 +693,7 @@ static int set_attrs() {
                                   (int)svd_smem<CT>()));
     PTT_CUDA(cudaFuncSetAttribute(k_svd_replay, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)replay_smem<128>()));
-    done = true;
+    done.fetch_or(bit);
     return PTT_OK;
 }
 
@@ -844,7 +845,7 @@ static bool wt_fits(const ptt_tt* x, const int* rk) {
     return true;
 }
 
-static int g_cq_csmax = cq::CSMAX;  // cluster size the device can schedule
+static int g_cq_csmax[64];  // per device: cluster size it can schedule
 
 static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr, int phases, int only) {
     using namespace wt;
@@ -852,8 +853,13 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
     const int d = x->d;
     int rc = set_attrs<32>();
     if (rc) return rc;
-    static bool wattr = false;
-    if (!wattr) {
+    static std::atomic<unsigned long long> wattr{0};
+    unsigned long long wbit;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    dev &= 63;
+    if (!ptt_device_done(wattr, &wbit)) {
+        g_cq_csmax[dev] = cq::CSMAX;
         PTT_CUDA(cudaFuncSetAttribute(k_wfactor<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wfactor_smem()));
         PTT_CUDA(cudaFuncSetAttribute(k_wfactor<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wfactor_smem()));
         PTT_CUDA(cudaFuncSetAttribute(k_wfactor<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wfactor_smem()));
@@ -877,9 +883,9 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
         int ncl = 0;
         if (cudaOccupancyMaxActiveClusters(&ncl, (const void*)cq::k_cq_factor<32>, &qc) != cudaSuccess || ncl < 1) {
             cudaGetLastError();
-            g_cq_csmax = 8;
+            g_cq_csmax[dev] = 8;
         }
-        wattr = true;
+        wattr.fetch_or(wbit);
     }
     int Wl[PTT_MAX_DIM], Wr[PTT_MAX_DIM], Pcap = 1;
     for (int i = 0; i < d; i++) {
@@ -934,7 +940,7 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
             // it did not finish
             const int mp = W * 32;  // bound on the unfolding's rows
             int cs = 1;
-            while (cs < g_cq_csmax && (long long)cs * cq::RTARGET < mp) cs <<= 1;
+            while (cs < g_cq_csmax[dev] && (long long)cs * cq::RTARGET < mp) cs <<= 1;
             int rpb = (mp + cs - 1) / cs;
             const int rmax = cb == 16 ? cq::rpb_max<16>() : (cb == 24 ? cq::rpb_max<24>() : cq::rpb_max<32>());
             if (rpb > rmax) {  // too tall for the cluster's shared memory: falls back at once

@@ -297,10 +297,11 @@ int gemm(ptt_ctx* c, const GemmB& g) {
         int rc = ptt_ws3_reserve(c, need);
         if (rc) return rc;
         double* part = (double*)c->ws3;
-        static bool attr = false;
-        if (!attr) {
+        static std::atomic<unsigned long long> attr{0};
+        unsigned long long bit;
+        if (!ptt_device_done(attr, &bit)) {
             PTT_CUDA(cudaFuncSetAttribute(k_gemm_skinny, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SKINNY_SMEM));
-            attr = true;
+            attr.fetch_or(bit);
         }
         ptt_time_begin(c, PTT_TIME_GEMM);
         PTT_CUDA(ptt_launch(c, k_gemm_skinny, dim3(dim3(ns, (unsigned)nb)), dim3(256), SKINNY_SMEM, g, ns, part));
