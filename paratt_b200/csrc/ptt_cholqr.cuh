@@ -38,8 +38,8 @@
 // On success Q is written once: LEFT -> alt[k] (m x c, column-major), RIGHT_T
 // -> core[k] in place (row-major rows of c; k_cq_write forms Q V_r from it
 // after the bond's SVD).  A bond that does not converge within MAXST stages or
-// meets a NaN or a zero matrix is left untouched and falls back to the
-// Householder TSQR: k_wfactor / k_wapply skip the bonds finished here and
+// meets a NaN, a zero matrix or an exactly zero column is left untouched and
+// falls back to the Householder TSQR: k_wfactor / k_wapply skip the bonds finished here and
 // k_cq_write skips the others.
 #pragma once
 
@@ -353,8 +353,11 @@ __global__ void __launch_bounds__(NT, 1) k_cq_factor(const DevDesc* D, int k, in
                 e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
             }
             nan = __any_sync(0xffffffffu, nan);
+            // an exactly zero column stays zero under every stage: leave the
+            // bond to the Householder TSQR at once
+            const bool zcol = __any_sync(0xffffffffu, lane < c && sG[lane * 33 + lane] == 0.0);
             int d;
-            if (nan || !(tr > 0.0) || !(tr < 1.0 / 0.0)) {
+            if (nan || !(tr > 0.0) || !(tr < 1.0 / 0.0) || (stage == 0 && zcol)) {
                 d = FALLBACK;
             } else if (stage >= 1 && e <= TAU) {
                 d = DONE;
