@@ -94,6 +94,17 @@ PTT_API int ptt_ctx_cholqr(ptt_ctx* ctx, int on);
  * before touching memory, which hides most of the launch gap; on == 0 launches
  * them plainly.  Results are identical. */
 PTT_API int ptt_ctx_pdl(ptt_ctx* ctx, int on);
+/* Autotuner (no counterpart in the reference): times the single-core QR of
+ * random m x c unfoldings (c = 16, 24, 32; m = 512 ... 16384) with every
+ * Cholesky-QR cluster size the device holds and keeps the fastest per
+ * (c, m) bucket in the context; roundings then use that table (results
+ * differ from the untuned sizes only by rounding order).  Takes well under a
+ * second; synchronises.  A size replaces the built-in rule (about 384 rows
+ * per CTA) only when it timed at least 15 % faster.  ptt_ctx_autotune_table
+ * writes the 18 entries (row-major [c bucket][m bucket]): the chosen size,
+ * or 0 where the rule is kept (all 0 if not tuned). */
+PTT_API int ptt_ctx_autotune(ptt_ctx* ctx);
+PTT_API int ptt_ctx_autotune_table(const ptt_ctx* ctx, int* out18);
 PTT_API int ptt_ctx_qr_counts(ptt_ctx* ctx, long long* out3);
 /* Overwrite a device buffer of twice the L2 size on the context's stream. */
 PTT_API int ptt_ctx_flush_l2(ptt_ctx* ctx);

@@ -82,6 +82,8 @@ _SIGS = {
     "ptt_ctx_graphs": (_i, [_p, _i]),
     "ptt_ctx_cholqr": (_i, [_p, _i]),
     "ptt_ctx_pdl": (_i, [_p, _i]),
+    "ptt_ctx_autotune": (_i, [_p]),
+    "ptt_ctx_autotune_table": (_i, [_p, C.POINTER(C.c_int)]),
     "ptt_ctx_qr_counts": (_i, [_p, C.POINTER(C.c_longlong)]),
     "ptt_ctx_elapsed": (_i, [_p, _i, _i, _dp]),
     "ptt_ctx_time_kernels": (_i, [_p, _i]),
@@ -175,6 +177,17 @@ class Context:
         """Cholesky-QR factorisation of unfoldings with <= 32 columns (default
         on; off = Householder TSQR only)."""
         _check(lib().ptt_ctx_cholqr(self.h, 1 if on else 0))
+
+    def autotune(self):
+        """Pick the Cholesky-QR cluster size per (columns, rows) bucket by
+        timing; returns the 3 x 6 table (columns 16/24/32 x rows 512..16384)."""
+        _check(lib().ptt_ctx_autotune(self.h))
+        return self.autotune_table()
+
+    def autotune_table(self):
+        v = (C.c_int * 18)()
+        _check(lib().ptt_ctx_autotune_table(self.h, v))
+        return np.array(list(v)).reshape(3, 6)
 
     def pdl(self, on=True):
         """Programmatic dependent launch of the rounding chain (default on)."""

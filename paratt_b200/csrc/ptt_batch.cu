@@ -12,6 +12,7 @@
 #include "ptt_common.cuh"
 
 #include <stdlib.h>
+#include <string.h>
 
 static int lane_ctx(ptt_ctx* c, int i, ptt_ctx** out) {
     while (c->nlanes <= i) {
@@ -24,6 +25,8 @@ static int lane_ctx(ptt_ctx* c, int i, ptt_ctx** out) {
     }
     c->lanes[i]->no_cholqr = c->no_cholqr;
     c->lanes[i]->no_pdl = c->no_pdl;
+    memcpy(c->lanes[i]->cq_cs, c->cq_cs, sizeof(c->cq_cs));
+    c->lanes[i]->cq_tuned = c->cq_tuned;
     *out = c->lanes[i];
     return PTT_OK;
 }

@@ -79,6 +79,11 @@ struct ptt_ctx {
     // programmatic dependent launch of the rounding chain: 0 = used (default)
     int no_pdl;
     int capturing;                // inside ptt_graph_run's own capture
+    // Cholesky-QR cluster sizes chosen by ptt_ctx_autotune: [column bound
+    // 16/24/32][rows bucket 512 .. 16384]; 0 = not tuned (size heuristic)
+    unsigned char cq_cs[3][6];
+    int cq_tuned;                 // generation of the table (0 = none)
+    int cq_cs_force;              // cluster size while tuning (0 = table/heuristic)
 };
 
 // Per-device one-time set-up (kernel attributes are per device): returns the

@@ -30,6 +30,18 @@ constexpr int MAXSW = 40;  // Jacobi sweep limit
 
 __device__ __forceinline__ unsigned group_mask8(int tid) { return 0xFFu << ((tid & 31) & ~7); }
 
+// the same for groups of LP lanes (LP = 2, 4, 8)
+template <int LP>
+__device__ __forceinline__ unsigned group_mask(int tid) {
+    return ((1u << LP) - 1u) << ((tid & 31) & ~(LP - 1));
+}
+template <int LP>
+__device__ __forceinline__ double gsum_g(double v, unsigned mask) {
+#pragma unroll
+    for (int o = LP / 2; o >= 1; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+}
+
 __device__ __forceinline__ double gsum8(double v, unsigned mask) {
     v += __shfl_xor_sync(mask, v, 4);
     v += __shfl_xor_sync(mask, v, 2);
@@ -246,17 +258,21 @@ __host__ __device__ constexpr int svd_nt() {
 }
 
 // One-sided Jacobi on the columns of L (c rows, q columns).  Each column pair
-// is handled by 8 lanes (rows p + 8v), 64 pairs per pass, so one circle-order
-// round is a single pass for q <= 128.  Column norms are tracked through the
-// rotations (a_p' = a_p - t a_pq ...) and recomputed at the start of a sweep.
-template <int CT>
-__global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws, double delta, int maxr, int bond,
-                                                       int* status) {
+// is handled by LP lanes (rows p + LP v), NTH / LP pairs per pass: with the
+// default 8 lanes and svd_nt threads one circle-order round is a single pass
+// for q <= 128.  (A one-warp form, NTH = 32 and LP = 4, measured slower on
+// the benchmark's bonds with q <= 16: 43.6 us against ~40 us, the
+// rotation chain and not the block barrier being the cost.)  Column norms
+// are tracked through the rotations (a_p' = a_p - t a_pq ...) and recomputed
+// at the start of a sweep.
+template <int CT, int NTH = svd_nt<CT>(), int LP = 8>
+__global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double delta, int maxr, int bond,
+                                                    int* status) {
     PTT_PDL_ENTRY();
-    constexpr int SVD_NT = svd_nt<CT>();
+    constexpr int SVD_NT = NTH;
     extern __shared__ double sm[];
     constexpr int S = CT + 1;
-    constexpr int NG = CT / 8;
+    constexpr int NG = CT / LP;
     double* Lc = sm;                   // (CT+1) columns x S
     __shared__ double s_nrm[CT + 2];
     __shared__ double s_sig[CT + 2];
@@ -264,8 +280,8 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws
     __shared__ int s_rot;
     __shared__ double s_thr2;
     const int tid = threadIdx.x;
-    const int grp = tid >> 3, p = tid & 7;  // 64 pair slots x 8 lanes
-    const unsigned gm = group_mask8(tid);
+    const int grp = tid / LP, p = tid % LP;  // pair slots x LP lanes
+    const unsigned gm = group_mask<LP>(tid);
     Info* info = pl.info;
     if (info->status) return;
     const int c = info->c, q = info->q;
@@ -284,14 +300,14 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws
     bool conv = (qq < 2);
     for (int sw = 0; sw < MAXSW && !conv; sw++) {
         // exact column norms at the start of every sweep
-        for (int j = tid >> 3; j < qq; j += SVD_NT / 8) {
+        for (int j = tid / LP; j < qq; j += SVD_NT / LP) {
             double s2 = 0.0;
 #pragma unroll
             for (int v = 0; v < NG; v++) {
-                const double x = Lc[j * S + p + 8 * v];
+                const double x = Lc[j * S + p + LP * v];
                 s2 += x * x;
             }
-            s2 = gsum8(s2, gm);
+            s2 = gsum_g<LP>(s2, gm);
             if (p == 0) s_nrm[j] = s2;
         }
         if (tid == 0) s_rot = 0;
@@ -310,7 +326,7 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws
         const double thr2 = s_thr2;
         int myrot = 0;
         for (int rd = 0; rd < qq - 1; rd++) {
-            for (int i = grp; i < qq / 2; i += SVD_NT / 8) {
+            for (int i = grp; i < qq / 2; i += SVD_NT / LP) {
                 const int pc = circle_col(i, rd, qq), qc = circle_col(qq - 1 - i, rd, qq);
                 double* ap = Lc + pc * S;
                 double* aq = Lc + qc * S;
@@ -318,15 +334,15 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws
                 double g0 = 0.0, g1 = 0.0;
 #pragma unroll
                 for (int v = 0; v < NG; v++) {
-                    xa[v] = ap[p + 8 * v];
-                    xb[v] = aq[p + 8 * v];
+                    xa[v] = ap[p + LP * v];
+                    xb[v] = aq[p + LP * v];
                 }
 #pragma unroll
                 for (int v = 0; v < NG; v += 2) {
                     g0 = fma(xa[v], xb[v], g0);
                     g1 = fma(xa[v + 1], xb[v + 1], g1);
                 }
-                const double ga = gsum8(g0 + g1, gm);
+                const double ga = gsum_g<LP>(g0 + g1, gm);
                 const double al = s_nrm[pc], be = s_nrm[qc];
                 double cs = 1.0, sn = 0.0;
                 if (ga != 0.0 && al > thr2 && be > thr2 && ga * ga > tol2 * (al * be)) {
@@ -338,8 +354,8 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws
                     sn = cs * t;
 #pragma unroll
                     for (int v = 0; v < NG; v++) {
-                        ap[p + 8 * v] = cs * xa[v] - sn * xb[v];
-                        aq[p + 8 * v] = sn * xa[v] + cs * xb[v];
+                        ap[p + LP * v] = cs * xa[v] - sn * xb[v];
+                        aq[p + LP * v] = sn * xa[v] + cs * xb[v];
                     }
                     if (p == 0) {
                         s_nrm[pc] = al - t * ga;
@@ -366,14 +382,14 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_jacobi(Plan pl, double* ws
     }
     if (!conv && tid == 0) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
     // singular values (column norms) and descending order
-    for (int j = tid >> 3; j < qq; j += SVD_NT / 8) {
+    for (int j = tid / LP; j < qq; j += SVD_NT / LP) {
         double s2 = 0.0;
 #pragma unroll
         for (int v = 0; v < NG; v++) {
-            const double x = Lc[j * S + p + 8 * v];
+            const double x = Lc[j * S + p + LP * v];
             s2 += x * x;
         }
-        s2 = gsum8(s2, gm);
+        s2 = gsum_g<LP>(s2, gm);
         // a NaN (corrupt input) would break the strict order below and leave
         // order slots unset; it sorts last and is reported instead
         if (p == 0) {
@@ -847,6 +863,16 @@ static bool wt_fits(const ptt_tt* x, const int* rk) {
 
 static int g_cq_csmax[64];  // per device: cluster size it can schedule
 
+// rows bucket of the autotuner's table: <= 512, 1024, ..., > 8192
+static int cq_bucket(int mp) {
+    int b = 0, lim = 512;
+    while (b < 5 && mp > lim) {
+        b++;
+        lim <<= 1;
+    }
+    return b;
+}
+
 static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr, int phases, int only) {
     using namespace wt;
     ptt_ctx* c = x->ctx;
@@ -940,9 +966,17 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
             // it did not finish
             const int mp = W * 32;  // bound on the unfolding's rows
             int cs = 1;
-            while (cs < g_cq_csmax[dev] && (long long)cs * cq::RTARGET < mp) cs <<= 1;
-            int rpb = (mp + cs - 1) / cs;
+            if (c->cq_cs_force) {
+                cs = c->cq_cs_force;
+            } else if (c->cq_tuned && c->cq_cs[cb == 16 ? 0 : (cb == 24 ? 1 : 2)][cq_bucket(mp)]) {
+                cs = c->cq_cs[cb == 16 ? 0 : (cb == 24 ? 1 : 2)][cq_bucket(mp)];
+            } else {  // row-count rule: about RTARGET rows per CTA
+                while (cs < g_cq_csmax[dev] && (long long)cs * cq::RTARGET < mp) cs <<= 1;
+            }
+            if (cs > g_cq_csmax[dev]) cs = g_cq_csmax[dev];
             const int rmax = cb == 16 ? cq::rpb_max<16>() : (cb == 24 ? cq::rpb_max<24>() : cq::rpb_max<32>());
+            while (cs < g_cq_csmax[dev] && (mp + cs - 1) / cs > rmax) cs <<= 1;  // fit the rows
+            int rpb = (mp + cs - 1) / cs;
             if (rpb > rmax) {  // too tall for the cluster's shared memory: falls back at once
                 cs = 1;
                 rpb = 1;
@@ -1007,7 +1041,7 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
     // the launches below, as one unit that can be captured and replayed;
     // the key holds every value they bake in
     struct Key {
-        int tag, d, phases, only, use_cq;
+        int tag, d, phases, only, use_cq, tuned;
         const void *dd, *ws, *cnt, *status, *stats;
         long long stride;
         int Pcap;
@@ -1020,6 +1054,7 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
     key.phases = phases;
     key.only = only;
     key.use_cq = use_cq;
+    key.tuned = c->cq_tuned;
     key.dd = x->dd;
     key.ws = ws;
     key.cnt = c->d_counters;
@@ -1076,7 +1111,8 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
                 Wmax = Wr[i] > Wmax ? Wr[i] : Wmax;
                 const int mr = maxr ? maxr[i] : rk[i];
                 ptt_time_begin(c, PTT_TIME_SVD);
-                PTT_CUDA(ptt_launch(c, k_svd_jacobi<32>, dim3(1), dim3(svd_nt<32>()), svd_smem<32>(), pl, wsb, delta, mr, i, c->d_status));
+                PTT_CUDA(ptt_launch(c, k_svd_jacobi<32>, dim3(1), dim3(svd_nt<32>()), svd_smem<32>(), pl, wsb, delta, mr, i,
+                                    c->d_status));
                 ptt_time_end(c, PTT_TIME_SVD);
                 PTT_LAUNCHED(c);
                 const long long mcap = (long long)rk[i - 1] * x->n[i - 1];
@@ -1160,4 +1196,110 @@ extern "C" int ptt_ctx_fixed_plans(ptt_ctx* c, int on) {
 
 extern "C" int ptt_round(ptt_tt* x, double tol, const int* maxrank) {
     return ptt_round_phases(x, tol, maxrank, 3, 0);
+}
+
+// ---------------------------------------------------------------------------
+// autotuner of the Cholesky-QR cluster size
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void k_tune_fill(double* p, long long cnt, unsigned long long seed) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt;
+         e += (long long)gridDim.x * blockDim.x) {
+        unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(e + 1);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        p[e] = (double)(z >> 11) * 1.1102230246251565e-16 - 0.5;  // uniform in [-0.5, 0.5)
+    }
+}
+}  // namespace
+
+// For each column bound (16, 24, 32) and rows bucket (512 ... 16384), time the
+// QR of one core (the single-core phase of a rounding, the path the sketch
+// uses per core) of a random m x c unfolding with every cluster size the
+// device can hold, and keep the fastest in the context's table.
+extern "C" int ptt_ctx_autotune(ptt_ctx* c) {
+    if (!c) return ptt_set_error(PTT_ERR_ARG, "null context");
+    cudaSetDevice(c->device);
+    const int graphs = c->graphs, tkind = c->tkind;
+    c->graphs = 0;
+    c->tkind = 0;
+    int rc = PTT_OK;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ptt_tt *x = nullptr, *x0 = nullptr;
+    PTT_CUDA(cudaEventCreate(&e0));
+    PTT_CUDA(cudaEventCreate(&e1));
+    static const int cbs[3] = {16, 24, 32};
+    for (int ci = 0; ci < 3 && !rc; ci++) {
+        for (int bi = 0; bi < 6 && !rc; bi++) {
+            const int cb = cbs[ci], m = 512 << bi;
+            int n[2] = {m, 1}, cap[3] = {1, cb, 1}, rk[3] = {1, cb, 1};
+            x = ptt_tt_create(c, 2, n, cap);
+            x0 = ptt_tt_create(c, 2, n, cap);
+            if (!x || !x0) {
+                rc = ptt_last_error() ? ptt_last_error() : PTT_ERR_CUDA;
+                break;
+            }
+            if ((rc = ptt_pull_desc(x0))) break;
+            k_tune_fill<<<148, 256, 0, c->stream>>>(x0->hd.core[0], (long long)m * cb, 1234567ull + 977ull * bi + ci);
+            k_tune_fill<<<1, 32, 0, c->stream>>>(x0->hd.core[1], cb, 7654321ull + ci);
+            if ((rc = ptt_cuda_check(cudaGetLastError(), "tune fill"))) break;
+            float best = 1e30f, theur = 1e30f;
+            int bestcs = 1;
+            // the size the row-count heuristic would take
+            int hcs = 1;
+            {
+                const int dev = c->device & 63;
+                const int csmax = g_cq_csmax[dev] ? g_cq_csmax[dev] : cq::CSMAX;
+                while (hcs < csmax && (long long)hcs * cq::RTARGET < m) hcs <<= 1;
+            }
+            for (int cs = 1; cs <= cq::CSMAX && !rc; cs <<= 1) {
+                int dev = c->device & 63;
+                if (g_cq_csmax[dev] && cs > g_cq_csmax[dev]) break;
+                const int rmax = cb == 16 ? cq::rpb_max<16>() : (cb == 24 ? cq::rpb_max<24>() : cq::rpb_max<32>());
+                if ((m + cs - 1) / cs > rmax) continue;
+                c->cq_cs_force = cs;
+                float tmin = 1e30f;
+                for (int rep = 0; rep < 7 && !rc; rep++) {
+                    if ((rc = ptt_tt_copy(x, x0))) break;
+                    if ((rc = ptt_ctx_synchronize(c))) break;
+                    PTT_CUDA(cudaEventRecord(e0, c->stream));
+                    if ((rc = ptt_round_phases_rk(x, rk, 0.0, NULL, 4, 0))) break;
+                    PTT_CUDA(cudaEventRecord(e1, c->stream));
+                    PTT_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    PTT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    if (rep > 0 && ms < tmin) tmin = ms;  // rep 0 warms up
+                }
+                if (tmin < best) {
+                    best = tmin;
+                    bestcs = cs;
+                }
+                if (cs == hcs) theur = tmin;
+            }
+            // a single timed QR is noisy: leave the heuristic's size unless
+            // another one is clearly faster
+            if (theur < 1e30f && !(best < 0.85f * theur)) bestcs = 0;  // 0: keep the row-count rule
+            c->cq_cs[ci][bi] = (unsigned char)bestcs;
+            ptt_tt_destroy(x);
+            ptt_tt_destroy(x0);
+            x = x0 = nullptr;
+        }
+    }
+    if (x) ptt_tt_destroy(x);
+    if (x0) ptt_tt_destroy(x0);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->cq_cs_force = 0;
+    c->graphs = graphs;
+    c->tkind = tkind;
+    if (rc) return rc;
+    c->cq_tuned++;
+    return ptt_ctx_synchronize(c);
+}
+
+extern "C" int ptt_ctx_autotune_table(const ptt_ctx* c, int* out) {
+    if (!c || !out) return ptt_set_error(PTT_ERR_ARG, "ptt_ctx_autotune_table: bad arguments");
+    for (int i = 0; i < 18; i++) out[i] = c->cq_tuned ? c->cq_cs[i / 6][i % 6] : 0;
+    return PTT_OK;
 }

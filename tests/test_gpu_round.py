@@ -176,3 +176,23 @@ def test_pdl_same_bits(ctx):
     assert O.ranks_of(got[0]) == O.ranks_of(got[1])
     for a, b in zip(*got):
         np.testing.assert_array_equal(a, b)
+
+
+def test_autotune(ctx):
+    """The autotuner keeps a valid cluster size (or the built-in rule) for
+    every bucket, and roundings with its table agree with the untuned ones."""
+    x = gapped_tt([9, 16, 7, 12, 8], [1, 7, 12, 10, 9, 1], 15, [1, 4, 6, 5, 3, 1], decay=1e-9)
+    tol = 1e-8 * O.norm(x)
+    X = P.TT.from_cores(ctx, x)
+    X.round(tol, 64)
+    before = X.get()
+    X.close()
+    table = ctx.autotune()
+    assert table.shape == (3, 6)
+    assert all(v in (0, 1, 2, 4, 8, 16) for v in table.ravel())  # 0: the row-count rule is kept
+    X = P.TT.from_cores(ctx, x)
+    X.round(tol, 64)
+    after = X.get()
+    X.close()
+    assert O.ranks_of(after) == O.ranks_of(before)
+    assert O.rel_diff_exact(after, before) <= 1e-12
