@@ -133,6 +133,26 @@ PTT_API int ptt_tt_copy(ptt_tt* dst, const ptt_tt* src);
 /* Raw device addresses of the current core buffers (valid until the next
  * operation on t) and of the device rank array. */
 PTT_API int ptt_tt_device_cores(const ptt_tt* t, double** cores, int** ranks);
+/* The context a train belongs to. */
+PTT_API ptt_ctx* ptt_tt_context(const ptt_tt* t);
+
+/* ---- checkpoint / resume (the reference's .cr core files) -------------- */
+/* Snapshot of a train into <folder>/core_<k+1>.cr, the format of
+ * pattac_write_tt_folder (paratt.c:1621-1706): header "r_l,N,r_r", values
+ * "%+1.16e" column-major, which round-trips every double.  The cores are
+ * copied to page-locked host memory in stream order and a background thread
+ * writes the files (write-behind): the call returns at once (after reading
+ * the ranks), later work on the train does not change the snapshot, and
+ * ptt_checkpoint_wait blocks until the files are written, returns the
+ * outcome and releases the handle.  NULL on a bad argument or a failed
+ * allocation. */
+typedef struct ptt_checkpoint ptt_checkpoint;
+PTT_API ptt_checkpoint* ptt_checkpoint_begin(ptt_tt* t, const char* folder);
+PTT_API int ptt_checkpoint_wait(ptt_checkpoint* cp);
+/* Resume: load a folder of .cr files (from either library, d files matching
+ * t's mode sizes, ranks continuing from 1 to 1) into t, growing its rank
+ * capacity if needed (pattac_load_tt_folder, paratt.c:1744-1892). */
+PTT_API int ptt_tt_load_folder(ptt_tt* t, const char* folder);
 
 /* ---- hot path ---------------------------------------------------------- */
 /* paratt_truncate semantics (paratt.c:316-342, pattac.c:590-675): tol is

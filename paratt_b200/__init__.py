@@ -83,6 +83,9 @@ _SIGS = {
     "ptt_ctx_cholqr": (_i, [_p, _i]),
     "ptt_ctx_pdl": (_i, [_p, _i]),
     "ptt_ctx_autotune": (_i, [_p]),
+    "ptt_checkpoint_begin": (_p, [_p, C.c_char_p]),
+    "ptt_checkpoint_wait": (_i, [_p]),
+    "ptt_tt_load_folder": (_i, [_p, C.c_char_p]),
     "ptt_ctx_autotune_table": (_i, [_p, C.POINTER(C.c_int)]),
     "ptt_ctx_qr_counts": (_i, [_p, C.POINTER(C.c_longlong)]),
     "ptt_ctx_elapsed": (_i, [_p, _i, _i, _dp]),
@@ -335,10 +338,35 @@ class TT:
         _check(lib().ptt_tt_copy(self.h, other.h))
         return self
 
+    def checkpoint(self, folder):
+        """Start writing this train to `folder` as reference .cr core files
+        (write-behind); returns a Checkpoint whose wait() finishes it."""
+        h = lib().ptt_checkpoint_begin(self.h, os.fsencode(folder))
+        if not h:
+            raise RuntimeError(f"checkpoint of the train to {folder} could not start")
+        return Checkpoint(h)
+
+    def load_folder(self, folder):
+        """Resume: read reference .cr core files from `folder` into this train."""
+        _check(lib().ptt_tt_load_folder(self.h, os.fsencode(folder)))
+        return self
+
     def close(self):
         if self.h:
             lib().ptt_tt_destroy(self.h)
             self.h = None
+
+
+class Checkpoint:
+    """A checkpoint being written in the background (TT.checkpoint)."""
+
+    def __init__(self, h):
+        self.h = h
+
+    def wait(self):
+        if self.h:
+            h, self.h = self.h, None
+            _check(lib().ptt_checkpoint_wait(h))
 
 
 class HostTrain:

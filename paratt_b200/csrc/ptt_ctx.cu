@@ -581,6 +581,8 @@ extern "C" int ptt_tt_get(ptt_tt* t, int* ranks, double* const* cores) {
     return PTT_OK;
 }
 
+extern "C" ptt_ctx* ptt_tt_context(const ptt_tt* t) { return t ? t->ctx : NULL; }
+
 extern "C" int ptt_tt_device_cores(const ptt_tt* t, double** cores, int** ranks) {
     if (!t) return ptt_set_error(PTT_ERR_ARG, "null tt");
     int rc = ptt_pull_desc((ptt_tt*)t);

@@ -45,3 +45,13 @@ def test_no_gpu_fails_loudly():
         P.Context(0)
     assert e.value.code == P.PTT_ERR_NOGPU
     assert b"no CPU" in P.lib().ptt_last_error_message() or b"CUDA" in P.lib().ptt_last_error_message()
+
+
+def test_checkpoint_argument_errors():
+    """The checkpoint and resume entry points reject null trains and paths
+    before touching a device (no GPU needed)."""
+    import paratt_b200 as P
+    L = P.lib()
+    assert not L.ptt_checkpoint_begin(None, b"/tmp/x")
+    assert L.ptt_checkpoint_wait(None) != 0
+    assert L.ptt_tt_load_folder(None, b"/tmp/x") != 0
