@@ -346,12 +346,18 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
                 const double al = s_nrm[pc], be = s_nrm[qc];
                 double cs = 1.0, sn = 0.0;
                 if (ga != 0.0 && al > thr2 && be > thr2 && ga * ga > tol2 * (al * be)) {
-                    // t = tan(theta) = sign(z)/(|z| + sqrt(1+z^2)), z = (be-al)/(2 ga),
-                    // written as g2/(dd + sign(dd) sqrt(dd^2 + g2^2)): one sqrt, one reciprocal
+                    // the smaller rotation of the pair: with dd = be - al, g2 = 2 ga,
+                    // cos 2theta = |dd| / r, sin 2theta = sign(dd) g2 / r,
+                    // r = sqrt(dd^2 + g2^2); then cos theta = sqrt((1 + cos 2theta) / 2),
+                    // sin theta = sin 2theta / (2 cos theta), t = tan theta -- two
+                    // reciprocal square roots on the chain, no square root or division
                     const double dd = be - al, g2 = 2.0 * ga;
-                    const double t = g2 * __drcp_rn(dd + copysign(sqrt(fma(dd, dd, g2 * g2)), dd));
-                    cs = rsqrt(fma(t, t, 1.0));
-                    sn = cs * t;
+                    const double ri = rsqrt(fma(dd, dd, g2 * g2));
+                    const double hc = fma(0.5 * fabs(dd), ri, 0.5);  // (1 + cos 2theta) / 2, in [1/2, 1]
+                    const double ic = rsqrt(hc);                      // 1 / cos theta
+                    cs = hc * ic;
+                    sn = 0.5 * copysign(1.0, dd) * g2 * ri * ic;
+                    const double t = sn * ic;
 #pragma unroll
                     for (int v = 0; v < NG; v++) {
                         ap[p + LP * v] = cs * xa[v] - sn * xb[v];
