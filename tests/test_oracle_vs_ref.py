@@ -58,7 +58,9 @@ def test_ic_fixture_is_the_gaussian_pdf():
 
 
 def test_round_known_answer():
-    """round(a f + b f) has rank(f) and norm |a + b| ||f|| (SURVEY 8c KAT 2)."""
+    """round(a f + b f) has rank(f) and norm |a + b| ||f|| (a known-answer
+    case: the reference's truncation of the formal sum must drop the
+    duplicated half exactly)."""
     f = O.random_tt([7, 6, 5, 8], [1, 3, 4, 2, 1], 5)
     z = O.axpby(1.0, f, 2.0, f)
     g = O.round_tt(z, 1e-12 * O.norm(z), 64)
@@ -68,7 +70,8 @@ def test_round_known_answer():
 
 def test_stencil_known_answer():
     """[1,-2,1] on a sampled sine along one mode multiplies it by the
-    eigenvalue 2 cos(2 pi k / n) - 2 (SURVEY 8c KAT 3)."""
+    eigenvalue 2 cos(2 pi k / n) - 2 (a known-answer case of the periodic
+    stencil)."""
     n, k = 32, 3
     v = np.sin(2 * np.pi * k * np.arange(n) / n)
     f = [v.reshape(1, n, 1), np.ones((1, 5, 1))]
