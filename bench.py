@@ -176,25 +176,11 @@ def run_ours(args, rank, world, local_rank):
     from paratt_b200 import learned as Lr
     from paratt_b200 import workloads as Wl
 
-    dist = None
-    if world > 1:
-        import torch
-        import torch.distributed as td
-        from datetime import timedelta
-        torch.cuda.set_device(local_rank)
-        td.init_process_group("nccl", timeout=timedelta(seconds=600))
-        dist = (torch, td)
-
-    def barrier():
-        if dist:
-            dist[1].barrier()
-
-    def max_over_ranks(v):
-        if not dist:
-            return v
-        t = dist[0].tensor([v], device="cuda")
-        dist[1].all_reduce(t, op=dist[1].ReduceOp.MAX)
-        return float(t.item())
+    # independent replicas: NCCL only for the barrier and the max of the times
+    from paratt_b200.replicas import Replicas
+    rep = Replicas("nccl")
+    barrier = rep.barrier
+    max_over_ranks = rep.max
 
     d, n, maxr, dt = CFG["d"], CFG["n"], CFG["maxrank"], CFG["dt"]
     ctx = P.Context(local_rank)
@@ -302,8 +288,7 @@ def run_ours(args, rank, world, local_rank):
     host.close()
 
     if rank != 0:
-        if dist:
-            dist[1].destroy_process_group()
+        rep.close()
         return 0
 
     hbm, src = peaks()
@@ -357,8 +342,7 @@ def run_ours(args, rank, world, local_rank):
     ls.close()
     plain.close()
     ctx.close()
-    if dist:
-        dist[1].destroy_process_group()
+    rep.close()
     return 0
 
 
