@@ -13,7 +13,8 @@
 //     is then orthonormal to O(c^2 max|E|^2)); when max|E| <= FIRST_DONE that
 //     is below TAU and Q_s R_{s+1}^{-1} is final without another Gram stage;
 //   * otherwise R_{s+1} = chol(G_s), or chol(G_s + sigma I) when a pivot is not
-//     positive or the pivots span more than 12 decades (condition > 1e6):
+//     positive or the pivots span more than 12 decades (condition > 1e6) --
+//     two warps form both factors at once and the plain one is kept if valid:
 //     shifted Cholesky QR (Fukaya, Kannan, Nakatsukasa, Yamamoto, Yanagisawa,
 //     SIAM J. Sci. Comput. 42 (2020)) with their shift
 //     sigma = 11 (m c + c (c + 1)) u ||Q_s||_F^2, which cannot break down and
@@ -39,8 +40,8 @@
 // -> core[k] in place (row-major rows of c; k_cq_write forms Q V_r from it
 // after the bond's SVD).  A bond that does not converge within MAXST stages or
 // meets a NaN, a zero matrix or an exactly zero column is left untouched and
-// falls back to the Householder TSQR: k_wfactor / k_wapply skip the bonds finished here and
-// k_cq_write skips the others.
+// falls back to the Householder TSQR: k_wfactor / k_wapply skip the bonds
+// finished here and k_cq_write skips the others.
 #pragma once
 
 namespace cq {
