@@ -35,6 +35,17 @@ typedef struct {
 static mirror_t* g_mir = NULL;
 static int g_nmir = 0, g_capmir = 0;
 
+/* host allocation that stops with a message instead of returning NULL (the
+   reference dereferences its unchecked malloc results) */
+static void* xmalloc(size_t bytes) {
+    void* p = malloc(bytes ? bytes : 1);
+    if (!p) {
+        fprintf(stderr, "paratt_b200: out of host memory (%zu bytes)\n", bytes);
+        exit(1);
+    }
+    return p;
+}
+
 static void fail(const char* where) {
     fprintf(stderr, "paratt_b200: %s: %s\n", where, ptt_last_error_message());
     exit(1);
@@ -104,7 +115,12 @@ static void host_fit(attac_tt* x, const int* ranks) {
     for (int k = 0; k < x->numDim; k++) {
         int need = x->dim[k] * ranks[k] * ranks[k + 1];
         if (x->coreMem[k] < need) {
-            x->coreList[k] = (double*)realloc(x->coreList[k], sizeof(double) * (size_t)need);
+            double* p = (double*)realloc(x->coreList[k], sizeof(double) * (size_t)need);
+            if (!p) {  /* the reference would crash on the NULL core; stop with a message */
+                fprintf(stderr, "paratt_b200: out of host memory growing core %d\n", k);
+                exit(1);
+            }
+            x->coreList[k] = p;
             x->coreMem[k] = need;
         }
     }
@@ -123,17 +139,17 @@ static void download(attac_tt* x, ptt_tt* m) {
 /* allocation                                                               */
 /* ------------------------------------------------------------------------ */
 attac_tt* alloc_tt(int ndims, int* d, int* ttR) {
-    attac_tt* t = (attac_tt*)malloc(sizeof(attac_tt));
+    attac_tt* t = (attac_tt*)xmalloc(sizeof(attac_tt));
     t->numDim = ndims;
-    t->dim = (int*)malloc(sizeof(int) * ndims);
-    t->ttRank = (int*)malloc(sizeof(int) * (ndims + 1));
-    t->coreList = (double**)malloc(sizeof(double*) * ndims);
-    t->coreMem = (int*)malloc(sizeof(int) * ndims);
+    t->dim = (int*)xmalloc(sizeof(int) * ndims);
+    t->ttRank = (int*)xmalloc(sizeof(int) * (ndims + 1));
+    t->coreList = (double**)xmalloc(sizeof(double*) * ndims);
+    t->coreMem = (int*)xmalloc(sizeof(int) * ndims);
     for (int k = 0; k < ndims; k++) {
         t->dim[k] = d[k];
         t->ttRank[k] = ttR[k];
         int sz = d[k] * (k == 0 ? 1 : ttR[k]) * ttR[k + 1];
-        t->coreList[k] = (double*)malloc(sizeof(double) * (size_t)sz);
+        t->coreList[k] = (double*)xmalloc(sizeof(double) * (size_t)sz);
         t->coreMem[k] = sz;
     }
     t->ttRank[ndims] = ttR[ndims];
@@ -143,14 +159,14 @@ attac_tt* alloc_tt(int ndims, int* d, int* ttR) {
 }
 
 paratt* alloc_ptt(int ndims, int* d, int* ttR) {
-    paratt* p = (paratt*)malloc(sizeof(paratt));
+    paratt* p = (paratt*)xmalloc(sizeof(paratt));
     p->mpi_rk = 0;
     p->mpi_sz = 1;
     p->numDim = ndims;
-    p->dim = (int*)malloc(sizeof(int) * ndims);
-    p->distrib_dim_mat = (int*)malloc(sizeof(int) * ndims);
+    p->dim = (int*)xmalloc(sizeof(int) * ndims);
+    p->distrib_dim_mat = (int*)xmalloc(sizeof(int) * ndims);
     for (int k = 0; k < ndims; k++) p->dim[k] = p->distrib_dim_mat[k] = d[k];
-    p->iwk = (int*)malloc(sizeof(int) * (ndims + 1));
+    p->iwk = (int*)xmalloc(sizeof(int) * (ndims + 1));
     p->iwksz = ndims + 1;
     p->orthog_wk = NULL;
     p->x = alloc_tt(ndims, d, ttR);
@@ -296,7 +312,7 @@ void pattac_apply_periodic_stencil(paratt* f, int mode, double* sten, int slen) 
 }
 
 void attac_set_rank1(attac_tt** x_ptr, double** vec, int ndims, int* d) {
-    int* r = (int*)malloc(sizeof(int) * (ndims + 1));
+    int* r = (int*)xmalloc(sizeof(int) * (ndims + 1));
     for (int i = 0; i <= ndims; i++) r[i] = 1;
     attac_tt* x = alloc_tt(ndims, d, r);
     for (int i = 0; i < ndims; i++) memcpy(x->coreList[i], vec[i], sizeof(double) * d[i]);
@@ -313,7 +329,7 @@ attac_tt* attac_sum_of_product(double*** vec, int ndims, int* d, int R) {
         attac_set_rank1(&x, vec[0], ndims, d);
         return x;
     }
-    int* r = (int*)malloc(sizeof(int) * (ndims + 1));
+    int* r = (int*)xmalloc(sizeof(int) * (ndims + 1));
     r[0] = r[ndims] = 1;
     for (int i = 1; i < ndims; i++) r[i] = R;
     attac_tt* x = alloc_tt(ndims, d, r);
@@ -433,7 +449,13 @@ void load_core_slice(char* fname, double** cr, int* cr_sz, int* rl, int* N, int*
     }
     int need = sz[0] * (N_end - N_beg) * sz[2];
     if (*cr_sz < need) {
-        *cr = (double*)realloc(*cr, sizeof(double) * (size_t)need);
+        double* p = (double*)realloc(*cr, sizeof(double) * (size_t)(need ? need : 1));
+        if (!p) {
+            fclose(fp);
+            fprintf(stderr, "\nload_core_slice error: out of host memory.\n");
+            exit(1);
+        }
+        *cr = p;
         *cr_sz = need;
     }
     *rl = sz[0];
@@ -457,8 +479,8 @@ void load_core_slice(char* fname, double** cr, int* cr_sz, int* rl, int* N, int*
 
 paratt* pattac_load_tt_folder(char* folder, int ndims) {
     char name[4096];
-    int* dim = (int*)malloc(sizeof(int) * ndims);
-    int* r = (int*)malloc(sizeof(int) * (ndims + 1));
+    int* dim = (int*)xmalloc(sizeof(int) * ndims);
+    int* r = (int*)xmalloc(sizeof(int) * (ndims + 1));
     int rl = 0, rr = 0, prev = 1;
     for (int k = 0; k < ndims; k++) {
         snprintf(name, sizeof(name), "%s/core_%d.cr", folder, k + 1);
