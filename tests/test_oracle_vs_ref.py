@@ -118,6 +118,27 @@ def test_round_rank_deficient_vs_reference():
 
 
 @needs_ref
+def test_round_zero_and_repeated_columns_vs_reference():
+    """Exact zero columns inside every core (a left-orthonormal train with
+    bond spectra cut to zero) plus the repeated blocks of x + x/2: the case
+    in which the GPU Jacobi once ran to its sweep limit on noise columns."""
+    rng = np.random.default_rng(13)
+    dims, full, keep = [9, 16, 7, 12, 8], [1, 7, 12, 10, 9, 1], [1, 4, 6, 5, 3, 1]
+    x = []
+    for k, n in enumerate(dims):
+        q, _ = np.linalg.qr(rng.standard_normal((full[k] * n, full[k + 1])))
+        if k < len(dims) - 1:
+            q[:, keep[k + 1]:] = 0.0
+        x.append(q.reshape(full[k], n, full[k + 1], order="F"))
+    z = O.axpby(1.0, x, 0.5, x)
+    for rtol in (0.0, 1e-6):
+        tol = rtol * O.norm(z)
+        got, ref = O.round_tt(z, tol, 64), R.ref_truncate(z, tol, 64)
+        assert O.ranks_of(got) == O.ranks_of(ref)
+        assert O.rel_diff_exact(got, ref) < 1e-12
+
+
+@needs_ref
 def test_ops_vs_reference():
     x = O.random_tt([6, 5, 7, 4, 6], [1, 3, 4, 5, 3, 1], 1)
     y = O.random_tt([6, 5, 7, 4, 6], [1, 2, 3, 3, 2, 1], 2)
