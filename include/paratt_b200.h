@@ -92,7 +92,10 @@ PTT_API int ptt_ctx_cholqr(ptt_ctx* ctx, int on);
  * in the reference): with on != 0 (the default) each kernel of a rounding may
  * be scheduled while its predecessor finishes and waits on the device for it
  * before touching memory, which hides most of the launch gap; on == 0 launches
- * them plainly.  Results are identical. */
+ * them plainly.  Results are identical.  The library's own graph captures
+ * launch plainly; inside a capture the caller makes, the launches become
+ * programmatic edges of the caller's graph -- call ptt_ctx_pdl(ctx, 0) first
+ * where that is not wanted. */
 PTT_API int ptt_ctx_pdl(ptt_ctx* ctx, int on);
 /* Autotuner (no counterpart in the reference): times the single-core QR of
  * random m x c unfoldings (c = 16, 24, 32; m = 512 ... 16384) with every
