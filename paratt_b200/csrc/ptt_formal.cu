@@ -30,6 +30,17 @@ static inline int elem_blocks(long long maxcnt) {
     return (int)b;
 }
 
+// Blocks per core of a launch over all d cores (grid y = core).  The count is
+// sized by the capacity, which can be far above the actual ranks: a few
+// waves over the GPU (148 SMs x 32 blocks) are enough at full size, and the
+// grid-stride loops cover any core with any grid.
+static inline int core_blocks(long long maxcnt, int d) {
+    const int b = elem_blocks(maxcnt);
+    int cap = 4736 / (d > 0 ? d : 1);
+    if (cap < 1) cap = 1;
+    return b < cap ? b : cap;
+}
+
 // ---------------------------------------------------------------------------
 // finalize: publish ranks computed by a kernel and swap the written cores
 // ---------------------------------------------------------------------------
@@ -161,7 +172,7 @@ extern "C" int ptt_axpby(double a, const ptt_tt* x, double b, const ptt_tt* y, p
     if (!newr) return ptt_set_error(PTT_ERR_ARG, "d too large");
     long long mx = 0;
     for (int k = 0; k < d; k++) mx = z->cap[k] > mx ? z->cap[k] : mx;
-    k_axpby<<<dim3(elem_blocks(mx), d), 256, 0, c->stream>>>(x->dd, y->dd, z->dd, a, b, newr, c->d_status);
+    k_axpby<<<dim3(core_blocks(mx, d), d), 256, 0, c->stream>>>(x->dd, y->dd, z->dd, a, b, newr, c->d_status);
     PTT_LAUNCHED(c);
     return finalize(z, newr, 0, d, 1);
 }
@@ -212,7 +223,7 @@ extern "C" int ptt_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z) {
     if (!newr) return ptt_set_error(PTT_ERR_ARG, "d too large");
     long long mx = 0;
     for (int k = 0; k < d; k++) mx = z->cap[k] > mx ? z->cap[k] : mx;
-    k_hadamard<<<dim3(elem_blocks(mx), d), 256, 0, c->stream>>>(x->dd, y->dd, z->dd, newr, c->d_status);
+    k_hadamard<<<dim3(core_blocks(mx, d), d), 256, 0, c->stream>>>(x->dd, y->dd, z->dd, newr, c->d_status);
     PTT_LAUNCHED(c);
     return finalize(z, newr, 0, d, 1);
 }
@@ -283,7 +294,7 @@ extern "C" int ptt_square_sym(const ptt_tt* x, ptt_tt* z) {
     if (!newr) return ptt_set_error(PTT_ERR_ARG, "d too large");
     long long mx = 0;
     for (int k = 0; k < d; k++) mx = z->cap[k] > mx ? z->cap[k] : mx;
-    k_square_sym<<<dim3(elem_blocks(mx), d), 256, 0, c->stream>>>(x->dd, z->dd, newr, c->d_status);
+    k_square_sym<<<dim3(core_blocks(mx, d), d), 256, 0, c->stream>>>(x->dd, z->dd, newr, c->d_status);
     PTT_LAUNCHED(c);
     return finalize(z, newr, 0, d, 1);
 }
@@ -470,7 +481,7 @@ extern "C" int ptt_op_sum(const ptt_tt* x, const double* sten, int slen, double 
     int* newr = ranks_scratch(c, d);
     long long mx = 0;
     for (int k = 0; k < d; k++) mx = y->cap[k] > mx ? y->cap[k] : mx;
-    k_opsum<<<dim3(elem_blocks(mx), d), 256, 0, c->stream>>>(x->dd, y->dd, st, shift, newr, c->d_status);
+    k_opsum<<<dim3(core_blocks(mx, d), d), 256, 0, c->stream>>>(x->dd, y->dd, st, shift, newr, c->d_status);
     PTT_LAUNCHED(c);
     return finalize(y, newr, 0, d, 1);
 }
