@@ -644,6 +644,9 @@ extern "C" int ptt_tt_copy(ptt_tt* dst, const ptt_tt* src) {
     for (int k = 0; k < src->d; k++) mx = src->cap[k] > mx ? src->cap[k] : mx;
     int bx = (int)((mx + 255) / 256);
     if (bx > 1184) bx = 1184;
+    // a few waves over the GPU in total; the loop strides over any core size
+    const int bcap = 4736 / src->d > 0 ? 4736 / src->d : 1;
+    if (bx > bcap) bx = bcap;
     if (src->ctx != c) {
         PTT_CUDA(cudaEventRecord(src->ctx->ev_fork, src->ctx->stream));
         PTT_CUDA(cudaStreamWaitEvent(c->stream, src->ctx->ev_fork, 0));
