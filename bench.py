@@ -204,6 +204,7 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         plain.step(S0)
     spec0 = Lr.kind_spectra(plain, d)
+    plain.log(False)  # the timed plain steps read nothing back
     ctx.sync()
 
     def copy_of(src):
@@ -333,16 +334,30 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    # the rank-64 -> 32 rounding of config 1 (d=40, n=256), recorded beside
+    # the step: the path that the step's low ranks never reach
+    c1 = config1_rounding(P, ctx, 3, 1)
+    out["round_c1"] = {k: c1[k] for k in ("ms", "ranks_out", "achieved_gbs", "frac", "fp64_tflops", "breakdown")}
     if world == 1 and not args.no_cpu_baseline:
         nthr = cpu_threads()
         os.environ.setdefault("OPENBLAS_NUM_THREADS", str(nthr))
         try:
-            _, ts = reference_steps(start_cores, tol, 2)
+            ref_state, ts = reference_steps(start_cores, tol, 2)
             sec = sum(ts) / len(ts)
             out["cpu_baseline"] = {"value": 1.0 / sec, "unit": "RK2 steps/s",
                                    "cores": int(os.environ["OPENBLAS_NUM_THREADS"]), "kind": "reference",
                                    "sample": f"2 full RK2 steps of the reference routines from the warmed-up "
                                              f"state (rank {max(r.shape[2] for r in start_cores[:-1])})"}
+            # parity: the same 2 plain steps on the GPU from the same state
+            G = copy_of(S0)
+            plain.step(G)
+            plain.step(G)
+            Rt = P.TT(ctx, [n] * d, cap, ref_state)
+            ref_ranks = [1] + [c.shape[2] for c in ref_state]
+            out["parity"] = {"ranks_equal": G.ranks() == ref_ranks, "rel_l2": rel_diff(G, Rt),
+                             "steps": 2, "against": "reference C (paratt_truncate composition), plain GPU step"}
+            G.close()
+            Rt.close()
         except Exception as e:
             out["cpu_baseline"] = {"value": None, "unit": "RK2 steps/s", "cores": 0, "kind": "reference",
                                    "sample": f"unavailable: {e}"}
@@ -432,19 +447,16 @@ def run_batch(args, rank, world, local_rank):
 # ---------------------------------------------------------------------------
 # single rounding (--workload round): x + y of two rank-32 trains -> rank 32
 # ---------------------------------------------------------------------------
-def run_round(args, rank, world, local_rank):
+def config1_rounding(P, ctx, steps, warmup):
     """d=40, n=256: z = x + y of two seeded random trains of interior rank
     32 (entries N(0, 1/(n r)) -- std 1/sqrt(n r)), rounded to tol 1e-10 x
     ||z||_RMS with rank cap 32, plain FP64.  Device time by events on the
-    context stream, L2 flushed before each rounding; roofline against the
-    algorithmic bytes 8 sum_k (3 R_k n R_{k+1} + r_k n r_{k+1})."""
-    import paratt_b200 as P
-
-    if rank != 0:
-        return 0
+    context stream, L2 flushed before each rounding (outside the events);
+    roofline against the algorithmic bytes 8 sum_k (3 R_k n R_{k+1} +
+    r_k n r_{k+1}); the algorithmic FP64 flops (Householder QR and Q of every
+    left unfolding, R X, LQ and Q of every right unfolding, 22 c^3 per SVD,
+    V_r^T Q and X U_r S_r) are reported beside it."""
     d, n, r = 40, 256, 32
-    ctx = P.Context(local_rank)
-    tuned = autotune(ctx)  # Cholesky-QR cluster sizes, timed once per context
     sd = 1.0 / np.sqrt(n * r)
 
     def rnd(seed):
@@ -460,32 +472,71 @@ def run_round(args, rank, world, local_rank):
     tol = 1e-10 * Z.norm()
     W = P.TT(ctx, [n] * d, cap)
     ts = []
-    for i in range(args.warmup + args.steps):
+    for i in range(warmup + steps):
         W.copy_from(Z)
         ctx.flush_l2()
         ctx.mark(0)
         W.round(tol, r)
         ctx.mark(1)
         ctx.sync()
-        if i >= args.warmup:
+        if i >= warmup:
             ts.append(ctx.elapsed_ms(0, 1))
     rk_in, rk_out = Z.ranks(), W.ranks()
     alg = 8.0 * sum(3 * rk_in[k] * n * rk_in[k + 1] + rk_out[k] * n * rk_out[k + 1] for k in range(d))
+    flops = 0.0
+    for k in range(d - 1):  # orthogonalisation: QR + Q of (R_k n) x R_{k+1}, then R X_{k+1}
+        m, c = rk_in[k] * n, rk_in[k + 1]
+        flops += 2 * (2.0 * m * c * c - 2.0 * c ** 3 / 3) + 2.0 * c * c * n * rk_in[k + 2]
+    for k in range(d - 1, 0, -1):  # truncation: LQ + Q, SVD, V_r^T Q, X_{k-1} U_r S_r
+        m, c, q = n * rk_out[k + 1], rk_in[k], rk_out[k]
+        flops += 2 * (2.0 * m * c * c - 2.0 * c ** 3 / 3) + 22.0 * c ** 3 + 2.0 * q * c * m
+        flops += 2.0 * rk_in[k - 1] * n * c * q
     t = statistics.median(ts)
+    # per kernel class: one more rounding with every launch of that class
+    # timed by its own event pair (outside the timed repetitions above)
+    breakdown = {}
+    for name, kind in (("factorisation", P.TIME_TSQR), ("svd", P.TIME_SVD)):
+        W.copy_from(Z)
+        ctx.sync()
+        ctx.time_kernels(kind)
+        W.round(tol, r)
+        kms, kl = ctx.kernel_time()
+        ctx.time_kernels(0)
+        breakdown[name] = {"ms": kms, "launches": kl}
+    sweeps = [int(v) for v in ctx.round_stats(d)[1:, 2]]
+    for t_ in (X, Y, Z, W):
+        t_.close()
     hbm, src = peaks()
+    return {"ms": t, "ms_all": ts, "ranks_out": max(rk_out), "algorithmic_bytes": alg, "algorithmic_flops": flops,
+            "achieved_gbs": alg / (t / 1e3) / 1e9, "frac": alg / (t / 1e3) / 1e9 / hbm, "peak": hbm,
+            "peak_source": src, "fp64_tflops": flops / (t / 1e3) / 1e12, "breakdown": breakdown,
+            "jacobi_sweeps": sweeps}
+
+
+def run_round(args, rank, world, local_rank):
+    """The rank-64 -> 32 rounding of config1_rounding as its own JSON line."""
+    import paratt_b200 as P
+
+    if rank != 0:
+        return 0
+    ctx = P.Context(local_rank)
+    autotune(ctx)  # Cholesky-QR cluster sizes, timed once per context
+    c1 = config1_rounding(P, ctx, args.steps, args.warmup)
+    t = c1["ms"]
     out = {
         "metric": "TT rounding d=40, n=256, ranks 64 -> 32 (plain FP64), roundings/s", "value": 1e3 / t,
         "unit": "roundings/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "round(x + y), x, y seeded rank-32 trains, N(0, 1/(n r)) entries, tol 1e-10 x "
-                               "||z||_RMS, rank cap 32", "ranks_out": max(rk_out), "l2": "flushed before each"},
-        "roofline": {"bound": "hbm", "achieved": alg / (t / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
-                     "frac": alg / (t / 1e3) / 1e9 / hbm, "traffic": None, "algorithmic_bytes": alg,
-                     "peak_source": src},
+                               "||z||_RMS, rank cap 32", "ranks_out": c1["ranks_out"], "l2": "flushed before each"},
+        "roofline": {"bound": "hbm", "achieved": c1["achieved_gbs"], "peak": c1["peak"], "unit": "GB/s",
+                     "frac": c1["frac"], "traffic": None, "algorithmic_bytes": c1["algorithmic_bytes"],
+                     "peak_source": c1["peak_source"]},
+        "fp64": {"algorithmic_flops": c1["algorithmic_flops"], "tflops": c1["fp64_tflops"]},
+        "breakdown": c1["breakdown"],
+        "jacobi_sweeps": c1["jacobi_sweeps"],
     }
     print(json.dumps(out))
-    for t_ in (X, Y, Z, W):
-        t_.close()
     ctx.close()
     return 0
 

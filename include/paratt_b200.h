@@ -109,6 +109,11 @@ PTT_API int ptt_ctx_pdl(ptt_ctx* ctx, int on);
 PTT_API int ptt_ctx_autotune(ptt_ctx* ctx);
 PTT_API int ptt_ctx_autotune_table(const ptt_ctx* ctx, int* out18);
 PTT_API int ptt_ctx_qr_counts(ptt_ctx* ctx, long long* out3);
+/* Device memory held by the context's grow-on-demand workspaces (bytes), and
+ * cudaMemGetInfo for the context's device (the caller's current device is
+ * kept).  For checking that a call allocated nothing. */
+PTT_API int ptt_ctx_workspace_bytes(const ptt_ctx* ctx, unsigned long long* bytes);
+PTT_API int ptt_ctx_mem_info(const ptt_ctx* ctx, unsigned long long* free_bytes, unsigned long long* total_bytes);
 /* Overwrite a device buffer of twice the L2 size on the context's stream. */
 PTT_API int ptt_ctx_flush_l2(ptt_ctx* ctx);
 /* Page-lock / release host memory for fast transfers (cudaHostRegister). */
@@ -292,10 +297,12 @@ PTT_API int ptt_entry(const ptt_tt* x, const int* idx, double* out);
  * Scratch lives in a fixed device array of PTT_DOT_NOALLOC_MAX_DOUBLES
  * doubles (4 MiB, held by every GPU that loads the library until exit); a
  * call needs 2*max_k(rx_k ry_k) + max_k(rx_k n_k ry_{k+1}) doubles and fails
- * with PTT_ERR_CAPACITY beyond that.  The first call on a device looks up the
- * array's address on that device: make it before any stream capture.  All
- * calls share the array, so calls that overlap on the GPU race.  Reads the
- * ranks and the result back (synchronises). */
+ * with PTT_ERR_CAPACITY beyond that.  ptt_ctx_create loads the array and looks
+ * up its address on the context's device, so the array is reserved when the
+ * context is created (create it before another allocator takes the GPU's
+ * memory) and no call loads or allocates anything later.  All calls share the
+ * array, so calls that overlap on the GPU race.  Reads the ranks and the
+ * result back (synchronises). */
 #define PTT_DOT_NOALLOC_MAX_DOUBLES (1 << 19)
 PTT_API int ptt_dot_noalloc(const ptt_tt* x, const ptt_tt* y, double* out);
 

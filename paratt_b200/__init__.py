@@ -88,6 +88,8 @@ _SIGS = {
     "ptt_tt_load_folder": (_i, [_p, C.c_char_p]),
     "ptt_ctx_autotune_table": (_i, [_p, C.POINTER(C.c_int)]),
     "ptt_ctx_qr_counts": (_i, [_p, C.POINTER(C.c_longlong)]),
+    "ptt_ctx_workspace_bytes": (_i, [_p, C.POINTER(C.c_ulonglong)]),
+    "ptt_ctx_mem_info": (_i, [_p, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
     "ptt_ctx_elapsed": (_i, [_p, _i, _i, _dp]),
     "ptt_ctx_time_kernels": (_i, [_p, _i]),
     "ptt_ctx_kernel_time": (_i, [_p, _dp, C.POINTER(C.c_longlong)]),
@@ -201,6 +203,18 @@ class Context:
         v = (C.c_longlong * 3)()
         _check(lib().ptt_ctx_qr_counts(self.h, v))
         return tuple(int(a) for a in v)
+
+    def workspace_bytes(self) -> int:
+        """Device bytes held by the context's grow-on-demand workspaces."""
+        v = C.c_ulonglong(0)
+        _check(lib().ptt_ctx_workspace_bytes(self.h, C.byref(v)))
+        return int(v.value)
+
+    def mem_info(self):
+        """(free, total) device bytes of the context's device (cudaMemGetInfo)."""
+        f, t = C.c_ulonglong(0), C.c_ulonglong(0)
+        _check(lib().ptt_ctx_mem_info(self.h, C.byref(f), C.byref(t)))
+        return int(f.value), int(t.value)
 
     def graphs(self, on=True):
         """Replay roundings from cached CUDA graphs when on (same results)."""

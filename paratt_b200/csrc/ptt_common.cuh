@@ -165,6 +165,9 @@ int ptt_ws3_reserve(ptt_ctx* c, size_t bytes);
 int ptt_push_desc(ptt_tt* t);
 int ptt_set_ranks_async(ptt_tt* t, int k0, const int* vals, int cnt);
 int ptt_ones(ptt_ctx* c, int n);  // make c->d_ones hold at least n ones
+// Device address of ptt_dot_noalloc's fixed scratch array on `device`
+// (looked up once per device; the caller's current device is kept).
+int ptt_dot_scratch_init(int device, double** out);
 
 // Swap core[k] <-> alt[k] for k in [k0, k1).
 int ptt_swap(ptt_tt* t, int k0, int k1);

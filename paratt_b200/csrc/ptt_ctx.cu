@@ -72,7 +72,10 @@ extern "C" ptt_ctx* ptt_ctx_create(int device) {
         ptt_cuda_check(cudaMemset(c->d_work, 0, sizeof(double) * 4), "memset") ||
         ptt_cuda_check(cudaMalloc(&c->d_qrstat, sizeof(long long) * 4), "cudaMalloc qr counters") ||
         ptt_cuda_check(cudaMemset(c->d_qrstat, 0, sizeof(long long) * 4), "memset") ||
-        ptt_cuda_check(cudaMemset(c->d_stats, 0, sizeof(double) * PTT_STAT_LEN * (PTT_MAX_DIM + 1)), "memset")) {
+        ptt_cuda_check(cudaMemset(c->d_stats, 0, sizeof(double) * PTT_STAT_LEN * (PTT_MAX_DIM + 1)), "memset") ||
+        // ptt_dot_noalloc's fixed array: loaded and located now, so its calls
+        // never load a module or allocate later
+        ptt_dot_scratch_init(device, NULL)) {
         free(c);
         return NULL;
     }
@@ -653,5 +656,32 @@ extern "C" int ptt_tt_copy(ptt_tt* dst, const ptt_tt* src) {
     }
     k_copy_tt<<<dim3(bx, src->d), 256, 0, c->stream>>>(src->dd, dst->dd, c->d_status);
     PTT_LAUNCHED(c);
+    return PTT_OK;
+}
+
+extern "C" int ptt_ctx_workspace_bytes(const ptt_ctx* c, unsigned long long* bytes) {
+    if (!c || !bytes) return ptt_set_error(PTT_ERR_ARG, "ptt_ctx_workspace_bytes: bad arguments");
+    unsigned long long b = (unsigned long long)(c->ws_bytes + c->ws2_bytes + c->ws3_bytes + c->flush_bytes) +
+                           (unsigned long long)c->counters_n * sizeof(int) + (unsigned long long)c->ones_n * sizeof(double);
+    for (int i = 0; i < c->nlanes; i++) {
+        unsigned long long lb = 0;
+        if (c->lanes[i] && ptt_ctx_workspace_bytes(c->lanes[i], &lb) == PTT_OK) b += lb;
+    }
+    *bytes = b;
+    return PTT_OK;
+}
+
+extern "C" int ptt_ctx_mem_info(const ptt_ctx* c, unsigned long long* free_bytes, unsigned long long* total_bytes) {
+    if (!c) return ptt_set_error(PTT_ERR_ARG, "ptt_ctx_mem_info: null context");
+    int prev = 0;
+    PTT_CUDA(cudaGetDevice(&prev));
+    size_t f = 0, t = 0;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e == cudaSuccess) e = cudaMemGetInfo(&f, &t);
+    const cudaError_t e2 = cudaSetDevice(prev);
+    if (e != cudaSuccess) return ptt_cuda_check(e, "cudaMemGetInfo");
+    if (e2 != cudaSuccess) return ptt_cuda_check(e2, "cudaSetDevice (restore)");
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
     return PTT_OK;
 }

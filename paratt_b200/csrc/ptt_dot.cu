@@ -10,6 +10,8 @@
 //  ptt_entry  paratt_entry (paratt.c:471-499) -> pattacValue (pattac.c:82-121).
 #include "ptt_common.cuh"
 
+#include <mutex>
+
 // T[i, j, e] = sum_k a[i, k] * y[k, j, e]      (a: rx x ry, column-major ld rx)
 __global__ void k_dot_t(const DevDesc* X, const DevDesc* Y, int k, const double* a, double* T) {
     const int rx = X->r[k], ry = Y->r[k], n = X->n[k], ry1 = Y->r[k + 1];
@@ -156,24 +158,41 @@ extern "C" int ptt_entry(const ptt_tt* x, const int* idx, double* out) {
 //
 // Host code cannot use the array's name as a device address, so its address
 // is looked up once per device (cudaGetSymbolAddress, with that device
-// current) on the first call made on that device; make that first call
-// before any stream capture on the device.
+// current).  ptt_ctx_create does that lookup for its device, which also loads
+// this module (and so reserves the array) while the context is created:
+// create the context before handing the GPU's memory to another allocator.
+// A call on a device whose address is not known yet (not possible through
+// ptt_ctx_create) looks it up itself, so make the first call before any
+// stream capture.  The lookup restores the caller's current device and is
+// serialised by a mutex, so threads making their first calls at once agree.
 // ---------------------------------------------------------------------------
 static __device__ __align__(256) double g_dot_scratch[PTT_DOT_NOALLOC_MAX_DOUBLES];
 
 #define PTT_NOALLOC_MAX_DEVICES 64
-static double* g_dot_scratch_addr[PTT_NOALLOC_MAX_DEVICES];
+static std::atomic<double*> g_dot_scratch_addr[PTT_NOALLOC_MAX_DEVICES];
+static std::mutex g_dot_scratch_mu;
 
-static int dot_scratch(int device, double** out) {
+int ptt_dot_scratch_init(int device, double** out) {
     if (device < 0 || device >= PTT_NOALLOC_MAX_DEVICES)
         return ptt_set_error(PTT_ERR_ARG, "ptt_dot_noalloc: device %d out of range", device);
-    if (!g_dot_scratch_addr[device]) {
-        void* p = NULL;
-        PTT_CUDA(cudaSetDevice(device));
-        PTT_CUDA(cudaGetSymbolAddress(&p, g_dot_scratch));
-        g_dot_scratch_addr[device] = (double*)p;
+    double* a = g_dot_scratch_addr[device].load(std::memory_order_acquire);
+    if (!a) {
+        std::lock_guard<std::mutex> lock(g_dot_scratch_mu);
+        a = g_dot_scratch_addr[device].load(std::memory_order_acquire);
+        if (!a) {
+            int prev = 0;
+            PTT_CUDA(cudaGetDevice(&prev));
+            void* p = NULL;
+            cudaError_t e = cudaSetDevice(device);
+            if (e == cudaSuccess) e = cudaGetSymbolAddress(&p, g_dot_scratch);
+            const cudaError_t e2 = cudaSetDevice(prev);  // the caller's device, whatever happened
+            if (e != cudaSuccess) return ptt_cuda_check(e, "cudaGetSymbolAddress(g_dot_scratch)");
+            if (e2 != cudaSuccess) return ptt_cuda_check(e2, "cudaSetDevice (restore)");
+            a = (double*)p;
+            g_dot_scratch_addr[device].store(a, std::memory_order_release);
+        }
     }
-    *out = g_dot_scratch_addr[device];
+    if (out) *out = a;
     return PTT_OK;
 }
 
@@ -187,7 +206,7 @@ extern "C" int ptt_dot_noalloc(const ptt_tt* x, const ptt_tt* y, double* out) {
         PTT_CUDA(cudaStreamWaitEvent(c->stream, y->ctx->ev_fork, 0));
     }
     double* scratch = NULL;
-    int rc = dot_scratch(c->device, &scratch);
+    int rc = ptt_dot_scratch_init(c->device, &scratch);
     if (rc) return rc;
     // size the scratch from the actual ranks (reading them synchronises)
     int rx[PTT_MAX_DIM + 1], ry[PTT_MAX_DIM + 1];

@@ -6,7 +6,8 @@ Runs the reference's own C (oracle/_ref/libparatt_ref.so, built by
 inputs and outputs as .npz; also stores the values of one initial-condition
 core file shipped with the reference (gaussian_dim_20/core_1.cr) and a .cr
 folder written by the reference's pattac_write_tt_folder.  Needs the
-reference checkout (REF, default /root/reference); the fixtures are what the
+reference checkout ($PARATT_REFERENCE, else a folder named `reference` beside
+this repository); the fixtures are what the
 tests read, so the tests themselves never need the reference.
 """
 import os
@@ -18,7 +19,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("PARATT_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
 
 from oracle import ref_lib as R  # noqa: E402
 from oracle import tt_oracle as O  # noqa: E402

@@ -166,3 +166,22 @@ def test_five_point_stencil_reference_branches():
     t.free()
     p = R.ref_stencil(x, 2, s5)
     assert np.abs(p[2] - O.periodic_stencil(x, 2, s5)[2]).max() > 1e-3
+
+
+@needs_ref
+@pytest.mark.parametrize("ngauss,seed", [(1, 3), (2, 5)])
+def test_rk2_composition_vs_reference(ngauss, seed):
+    """The RK2 reaction-Burgers step of the oracle (tt_oracle.rxn_burgers_rk2_step)
+    against the same composition run on the reference's own C routines
+    (ref_lib.ref_rxn_burgers_rk2_step: paratt_truncate, pattacHadamard,
+    attac_tt_axpby); the midpoint step follows paratt_ode.h:77-112.  This pins
+    the composition that the GPU step, the oracle and the reference arm share."""
+    d, n, maxr, dt = 4, 16, 12, 1e-3
+    u = O.config_ic(d, n, ngauss, seed)
+    tol = 1e-8 * O.norm(u)
+    uo, ur = u, u
+    for _ in range(3):
+        uo = O.rxn_burgers_rk2_step(uo, dt, tol, maxr)
+        ur = R.ref_rxn_burgers_rk2_step(ur, dt, tol, maxr)
+        assert O.ranks_of(uo) == O.ranks_of(ur)
+        assert O.rel_diff_exact(uo, ur) <= 1e-12

@@ -29,6 +29,25 @@ def test_noalloc_dot_matches_dot_twice(ctx):
         Y.close()
 
 
+def test_noalloc_dot_allocates_nothing(ctx):
+    """With the trains made and one call done, another call leaves the
+    context's workspaces and the device's free memory as they were."""
+    dims = [32, 24, 16, 40]
+    x = O.random_tt(dims, [1, 9, 12, 7, 1], 5)
+    y = O.random_tt(dims, [1, 6, 11, 10, 1], 6)
+    X, Y = P.TT.from_cores(ctx, x), P.TT.from_cores(ctx, y)
+    first = X.dot_noalloc(Y)
+    ws0, (free0, _) = ctx.workspace_bytes(), ctx.mem_info()
+    second = X.dot_noalloc(Y)
+    ws1, (free1, _) = ctx.workspace_bytes(), ctx.mem_info()
+    assert ws1 == ws0
+    assert free1 == free0
+    assert first == second
+    assert abs(second - O.dot(x, y)) <= 1e-13 * O.norm(x) * O.norm(y)
+    X.close()
+    Y.close()
+
+
 def test_noalloc_rejects_oversize(ctx):
     dims = [256, 256, 256]
     x = O.random_tt(dims, [1, 64, 64, 1], 3)
