@@ -379,15 +379,23 @@ def run_batch(args, rank, world, local_rank):
     tol 1e-8 x its RMS norm with rank cap floor(r_k/2): ptt_round_batch
     (concurrent worker streams) against the one-train-at-a-time loop, both
     from fresh copies of the same inputs every repetition; device time by
-    events on the context stream (rank read-backs included)."""
+    events on the context stream (rank read-backs included).  With N ranks
+    the 64 trains are split by instance, balanced by rounding cost
+    (workloads.shard_by_cost), each rank rounds its share on its GPU with no
+    collective on the data path; the time of a repetition is the slowest
+    rank's, and rank 0 gathers every train's ranks."""
     import paratt_b200 as P
     from paratt_b200 import workloads as Wl
+    from paratt_b200.replicas import Replicas
 
-    if rank != 0:
-        return 0
+    rep = Replicas("nccl")
     ctx = P.Context(local_rank)
     tuned = autotune(ctx)  # Cholesky-QR cluster sizes, timed once per context
-    orig = Wl.batch_trains(ctx, 64, 4)
+    shapes = Wl.batch_shapes(64, 4)
+    costs = [Wl.rounding_cost(sh) for sh in shapes]
+    shards = Wl.shard_by_cost(costs, world)
+    mine = shards[rank]
+    orig = Wl.batch_trains(ctx, 64, 4, only=set(mine))
     tts = [t for t, _ in orig]
     caps = [sh[3] for _, sh in orig]
     tols = [1e-8 * t.norm() for t in tts]
@@ -404,11 +412,12 @@ def run_batch(args, rank, world, local_rank):
 
     def timed(fn):
         fresh()
+        rep.barrier()
         ctx.mark(0)
         fn()
         ctx.mark(1)
         ctx.sync()
-        return ctx.elapsed_ms(0, 1)
+        return rep.max(ctx.elapsed_ms(0, 1))
 
     def loop():
         for w, tol, cap in zip(work, tols, caps):
@@ -416,31 +425,44 @@ def run_batch(args, rank, world, local_rank):
 
     lanes = 8
     t_loop, t_batch = [], []
+    ranks_loop = ranks_batch = []
     for i in range(args.warmup + args.steps):
         a = timed(loop)
         ranks_loop = [w.ranks() for w in work]
-        b = timed(lambda: P.round_batch(work, tols, caps, lanes=lanes))
+        b = timed(lambda: P.round_batch(work, tols, caps, lanes=lanes) if work else None)
         ranks_batch = [w.ranks() for w in work]
         if i >= args.warmup:
             t_loop.append(a)
             t_batch.append(b)
-    same = ranks_loop == ranks_batch
-    tb, tl = statistics.median(t_batch), statistics.median(t_loop)
-    out = {
-        "metric": "batched TT rounding: 64 trains (d 10-40, n 32-512, r 8-96), roundings/s", "value": 64e3 / tb,
-        "unit": "roundings/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": tb,
-        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "batched rounding of 64 independent trains (seed 4), tol 1e-8 x ||X||_RMS, "
-                               "rank cap floor(r/2); left-orthonormal cores, bond spectra 2^-j",
-                   "lanes": lanes, "input_gb": elems * 8 / 1e9},
-        "loop": {"value": 64e3 / tl, "unit": "roundings/s", "ms": tl},
-        "batch_over_loop": tl / tb,
-        "same_ranks_as_loop": bool(same),
-    }
-    print(json.dumps(out))
+    results = rep.gather([(idx, rl, rb) for idx, rl, rb in zip(mine, ranks_loop, ranks_batch)])
+    elems_all = rep.gather(elems)
     for t in tts + work:
         t.close()
     ctx.close()
+    if rank != 0:
+        rep.close()
+        return 0
+    per_train = sorted(x for part in results for x in part)
+    same = all(rl == rb for _, rl, rb in per_train) and [x[0] for x in per_train] == list(range(64))
+    tb, tl = statistics.median(t_batch), statistics.median(t_loop)
+    loads = [sum(costs[i] for i in sh) for sh in shards]
+    out = {
+        "metric": "batched TT rounding: 64 trains (d 10-40, n 32-512, r 8-96), roundings/s", "value": 64e3 / tb,
+        "unit": "roundings/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": tb,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batched rounding of 64 independent trains (seed 4), tol 1e-8 x ||X||_RMS, "
+                               "rank cap floor(r/2); left-orthonormal cores, bond spectra 2^-j",
+                   "lanes": lanes, "input_gb": sum(elems_all) * 8 / 1e9,
+                   "parallelism": f"instances split over {world} ranks by rounding cost" if world > 1 else "one GPU",
+                   "trains_per_rank": [len(sh) for sh in shards],
+                   "cost_share_per_rank": [l / sum(loads) for l in loads]},
+        "loop": {"value": 64e3 / tl, "unit": "roundings/s", "ms": tl},
+        "batch_over_loop": tl / tb,
+        "same_ranks_as_loop": bool(same),
+        "autotune_cq_cluster_sizes": tuned,
+    }
+    print(json.dumps(out))
+    rep.close()
     return 0
 
 

@@ -285,6 +285,36 @@ PTT_API int ptt_mlp_grads(ptt_mlp* m, const float* x, const float* t, int B, flo
 PTT_API int ptt_mlp_train_step(ptt_mlp* m, const float* x, const float* t, int B, float lr, float* loss);
 PTT_API int ptt_mlp_set_under_weight(ptt_mlp* m, float w);
 
+/* ---- CDF-problem stencils and marginals (one process) ------------------
+ * The reference's post-processing for its Burgers-Hopf CDF driver, each in
+ * place on core `mode` (the ghost cells of the reference's MPI exchange are
+ * rows of the same core with one process):
+ *   ptt_cdf_stencil      pattac_apply_cdf_stencil (paratt.c:772-923): centred
+ *                        stencil (even slen drops its last tap, slen <= 15);
+ *                        below the grid the reference reads f[a - j - 1], above
+ *                        it f[2n - 1 - j] (mirrored rows)
+ *   ptt_cdf_lf_flux      pattac_apply_cdf_lf_flux (paratt.c:926-1093):
+ *                        wave_speed[n], gc_wave_speed[2], source_coef[n]
+ *   ptt_cdf_lw_rhs       pattac_apply_cdf_lw_rhs (paratt.c:1096-1250): adds
+ *                        bdry_wave_speed[n + 1]
+ *   ptt_marginal_cusum   pattac_marginal_cusum (paratt.c:1393-1445)
+ *   ptt_marginal_trap    pattac_marginal_trap (paratt.c:1448-1524)
+ *   ptt_scale_weight_sum pattac_scale_weight_sum (paratt.c:1527-1618)
+ *   ptt_apply_marginal   pattac_apply_marginal (paratt.c:1252-1390): z (d - 1
+ *                        modes, capacity for x's ranks without r_{mode+1}, or
+ *                        with r_{d-1} -> 1 when mode = d - 1) = x contracted
+ *                        along `mode` with the row vector w[n_mode]
+ * Host vectors are copied in before the call returns. */
+PTT_API int ptt_cdf_stencil(ptt_tt* x, int mode, const double* sten, int slen);
+PTT_API int ptt_cdf_lf_flux(ptt_tt* x, int mode, const double* wave_speed, const double* gc_wave_speed,
+                            const double* source_coef, double dt, double dx);
+PTT_API int ptt_cdf_lw_rhs(ptt_tt* x, int mode, const double* wave_speed, const double* gc_wave_speed,
+                           const double* bdry_wave_speed, const double* source_coef, double dt, double dx);
+PTT_API int ptt_marginal_cusum(ptt_tt* x, int mode, const double* w);
+PTT_API int ptt_marginal_trap(ptt_tt* x, int mode, const double* w);
+PTT_API int ptt_scale_weight_sum(ptt_tt* x, int mode, const double* scale, const double* sum_w);
+PTT_API int ptt_apply_marginal(const ptt_tt* x, int mode, const double* w, ptt_tt* z);
+
 /* Reductions (these read a scalar back, so they synchronise). */
 PTT_API int ptt_dot(const ptt_tt* x, const ptt_tt* y, double* out);  /* <X,Y>/prod n */
 PTT_API int ptt_norm(const ptt_tt* x, double* out);                  /* RMS norm     */

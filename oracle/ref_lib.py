@@ -259,3 +259,68 @@ def ref_rxn_burgers_rk2_step(u, dt, tol, maxr, L=10.0, nu=0.05):
     us = ref_truncate(ref_axpby(1.0, u, 0.5 * dt, k1), tol, maxr)
     k2 = ref_rxn_burgers_F(us, tol, maxr, L, nu)
     return ref_truncate(ref_axpby(1.0, u, dt, k2), tol, maxr)
+
+
+# CDF-problem stencils and marginals (paratt.c:772-1618), one process
+def _dp(v):
+    a = np.ascontiguousarray(v, dtype=np.float64)
+    return a, a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _bind_cdf():
+    L = lib()
+    P = C.POINTER(Paratt)
+    dp = C.POINTER(C.c_double)
+    L.pattac_apply_cdf_stencil.argtypes = [P, C.c_int, dp, C.c_int]
+    L.pattac_apply_cdf_lf_flux.argtypes = [P, C.c_int, dp, dp, dp, C.c_double, C.c_double]
+    L.pattac_apply_cdf_lw_rhs.argtypes = [P, C.c_int, dp, dp, dp, dp, C.c_double, C.c_double]
+    L.pattac_apply_marginal.argtypes = [P, C.POINTER(P), C.c_int, dp]
+    L.pattac_marginal_cusum.argtypes = [P, C.c_int, dp]
+    L.pattac_marginal_trap.argtypes = [P, C.c_int, dp]
+    L.pattac_scale_weight_sum.argtypes = [P, C.c_int, dp, dp]
+    return L
+
+
+def ref_cdf_op(name, cores, mode, *vecs, scalars=()):
+    """Run one of the in-place CDF/marginal routines on a copy of `cores`:
+    name in cdf_stencil, cdf_lf_flux, cdf_lw_rhs, marginal_cusum,
+    marginal_trap, scale_weight_sum; vecs are the double arrays in the
+    reference's argument order, scalars the trailing doubles (dt, dx)."""
+    L = _bind_cdf()
+    t = RefTT(cores)
+    keep = [_dp(v) for v in vecs]
+    args = [k[1] for k in keep]
+    try:
+        if name == "cdf_stencil":
+            L.pattac_apply_cdf_stencil(t.p, mode, args[0], len(keep[0][0]))
+        elif name == "cdf_lf_flux":
+            L.pattac_apply_cdf_lf_flux(t.p, mode, *args, *scalars)
+        elif name == "cdf_lw_rhs":
+            L.pattac_apply_cdf_lw_rhs(t.p, mode, *args, *scalars)
+        elif name == "marginal_cusum":
+            L.pattac_marginal_cusum(t.p, mode, args[0])
+        elif name == "marginal_trap":
+            L.pattac_marginal_trap(t.p, mode, args[0])
+        elif name == "scale_weight_sum":
+            L.pattac_scale_weight_sum(t.p, mode, args[0], args[1])
+        else:
+            raise ValueError(name)
+        return t.cores()
+    finally:
+        t.free()
+
+
+def ref_apply_marginal(cores, mode, w):
+    """pattac_apply_marginal (paratt.c:1252-1390): the d-1 mode train."""
+    L = _bind_cdf()
+    t = RefTT(cores)
+    a, p = _dp(w)
+    out = C.POINTER(Paratt)()
+    try:
+        L.pattac_apply_marginal(t.p, C.byref(out), mode, p)
+        m = RefTT(ptr=out)
+        res = m.cores()
+        m.free()
+        return res
+    finally:
+        t.free()

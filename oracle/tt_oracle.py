@@ -384,3 +384,151 @@ def config_ic(d, n, ngauss, seed, L=10.0):
     centres = rng.uniform(-2.0, 2.0, size=(ngauss, d))
     widths = rng.uniform(0.3, 0.8, size=ngauss)
     return gaussian_sum_ic(d, n, centres, widths, L)
+
+
+# --------------------------------------------------------------------------
+# CDF-problem stencils and marginals (one process: the reference's ghost
+# cells are rows of the same core).  Each works on the fibers core[i, :, k]
+# of one mode.
+# --------------------------------------------------------------------------
+def _fibers(core):
+    """(r, n, r1) -> (r * r1 fibers, n) view order and back."""
+    r, n, r1 = core.shape
+    return core.transpose(0, 2, 1).reshape(r * r1, n)
+
+
+def _unfibers(f, shape):
+    r, n, r1 = shape
+    return f.reshape(r, r1, n).transpose(0, 2, 1).copy()
+
+
+def cdf_stencil(x, mode, sten):
+    """pattac_apply_cdf_stencil (paratt.c:772-923) with one process.  An even
+    length drops its last tap; h = (s - 1) / 2.  Outside the grid the
+    reference reads ghost rows: for j < 0 the value it uses at output a is
+    f[a - j - 1] (its above-ghost counter restarts at every a, paratt.c:
+    896-903, with the ghost rows f[h - 1 - g] set at 836-842), for j >= n it
+    is f[2n - 1 - j] (the mirrored last rows, 866-872)."""
+    s = len(sten)
+    if s % 2 == 0:
+        s -= 1
+    h = (s - 1) // 2
+    out = [c.copy() for c in x]
+    f = _fibers(x[mode])
+    n = f.shape[1]
+    g = np.zeros_like(f)
+    for a in range(n):
+        acc = np.zeros(f.shape[0])
+        for t in range(s):
+            j = a - h + t
+            if j < 0:
+                v = f[:, a - j - 1]
+            elif j >= n:
+                v = f[:, 2 * n - 1 - j]
+            else:
+                v = f[:, j]
+            acc = acc + sten[t] * v
+        g[:, a] = acc
+    out[mode] = _unfibers(g, x[mode].shape)
+    return out
+
+
+def cdf_lf_flux(x, mode, wave_speed, gc_wave_speed, source_coef, dt, dx):
+    """pattac_apply_cdf_lf_flux (paratt.c:926-1093) with one process: the
+    centred difference [-1/(2dx), 0, 1/(2dx)] of -w f, with the ghost
+    neighbours -gc_w[0] f[0] below the grid and -gc_w[1] f[n-1] above it
+    (1043-1082), plus source_coef * f (1083-1090).  dt is not used by the
+    reference."""
+    out = [c.copy() for c in x]
+    f = _fibers(x[mode])
+    n = f.shape[1]
+    w = np.asarray(wave_speed, dtype=float)
+    s0, s2 = -0.5 / dx, 0.5 / dx
+    g = np.zeros_like(f)
+    for a in range(n):
+        left = -gc_wave_speed[0] * f[:, 0] if a - 1 < 0 else -w[a - 1] * f[:, a - 1]
+        right = -gc_wave_speed[1] * f[:, n - 1] if a + 1 >= n else -w[a + 1] * f[:, a + 1]
+        acc = np.zeros(f.shape[0])
+        acc = acc + s0 * left
+        acc = acc + s2 * right
+        g[:, a] = acc + source_coef[a] * f[:, a]
+    out[mode] = _unfibers(g, x[mode].shape)
+    return out
+
+
+def cdf_lw_rhs(x, mode, wave_speed, gc_wave_speed, bdry_wave_speed, source_coef, dt, dx):
+    """pattac_apply_cdf_lw_rhs (paratt.c:1096-1250) with one process:
+    Lax-Wendroff half-step values u_{a+1/2} (ghosts f[0] below, f[n-1]
+    above, 1207-1230), then -(b_{a+1} u_{a+1/2} - b_a u_{a-1/2}) / dx +
+    source_coef_a f_a (1231-1235)."""
+    out = [c.copy() for c in x]
+    f = _fibers(x[mode])
+    n = f.shape[1]
+    w = np.asarray(wave_speed, dtype=float)
+    b = np.asarray(bdry_wave_speed, dtype=float)
+    k = dt / (2.0 * dx)
+    g = np.zeros_like(f)
+    gca, gcb = f[:, 0], f[:, n - 1]
+    uh0 = 0.5 * (gca + f[:, 0]) - (w[0] * f[:, 0] - gca * gc_wave_speed[0]) * k
+    for a in range(n):
+        if a + 1 < n:
+            uh1 = 0.5 * (f[:, a + 1] + f[:, a]) - (w[a + 1] * f[:, a + 1] - w[a] * f[:, a]) * k
+        else:
+            uh1 = 0.5 * (gcb + f[:, a]) - (gcb * gc_wave_speed[1] - w[a] * f[:, a]) * k
+        g[:, a] = -(b[a + 1] * uh1 - b[a] * uh0) / dx + source_coef[a] * f[:, a]
+        uh0 = uh1
+    out[mode] = _unfibers(g, x[mode].shape)
+    return out
+
+
+def marginal_cusum(x, mode, w):
+    """pattac_marginal_cusum (paratt.c:1393-1445) with one process:
+    f[j] <- sum_{m <= j} w[m] f[m] along the mode."""
+    out = [c.copy() for c in x]
+    f = _fibers(x[mode]) * np.asarray(w, dtype=float)[None, :]
+    out[mode] = _unfibers(np.cumsum(f, axis=1), x[mode].shape)
+    return out
+
+
+def marginal_trap(x, mode, w):
+    """pattac_marginal_trap (paratt.c:1448-1524) with one process: the
+    trapezoid cumulative integral f[j] <- sum_{m=1..j} w[m] (f[m-1] + f[m]) / 2
+    (f[0] <- 0)."""
+    out = [c.copy() for c in x]
+    f = _fibers(x[mode])
+    n = f.shape[1]
+    g = np.zeros_like(f)
+    cum = np.zeros(f.shape[0])
+    for j in range(1, n):
+        delta = 0.5 * w[j] * (f[:, j - 1] + f[:, j])
+        g[:, j - 1] = cum
+        cum = cum + delta
+    g[:, n - 1] = cum
+    out[mode] = _unfibers(g, x[mode].shape)
+    return out
+
+
+def scale_weight_sum(x, mode, scale, sum_w):
+    """pattac_scale_weight_sum (paratt.c:1527-1618) with one process: the
+    trapezoid cumulative integral with weights sum_w plus scale[j] f[j]."""
+    f = _fibers(x[mode])
+    t = _fibers(marginal_trap(x, mode, sum_w)[mode])
+    out = [c.copy() for c in x]
+    out[mode] = _unfibers(t + f * np.asarray(scale, dtype=float)[None, :], x[mode].shape)
+    return out
+
+
+def apply_marginal(x, mode, w):
+    """pattac_apply_marginal (paratt.c:1252-1390) with one process: contract
+    mode `mode` with the row vector w; the d-1 mode train folds W = sum_j
+    w[j] x_mode[:, j, :] into the next core (mode < d-1, 1342-1350) or the
+    previous one (mode = d-1, 1366-1373)."""
+    d = len(x)
+    W = np.einsum("j,ajb->ab", np.asarray(w, dtype=float), x[mode])
+    if mode < d - 1:
+        nxt = x[mode + 1]
+        folded = np.einsum("ab,bjc->ajc", W, nxt)
+        return [c.copy() for c in x[:mode]] + [folded] + [c.copy() for c in x[mode + 2:]]
+    prev = x[mode - 1]
+    folded = np.einsum("ajb,b->aj", prev, W[:, 0]).reshape(prev.shape[0], prev.shape[1], 1)
+    return [c.copy() for c in x[:mode - 1]] + [folded]

@@ -89,6 +89,13 @@ _SIGS = {
     "ptt_ctx_autotune_table": (_i, [_p, C.POINTER(C.c_int)]),
     "ptt_ctx_qr_counts": (_i, [_p, C.POINTER(C.c_longlong)]),
     "ptt_ctx_workspace_bytes": (_i, [_p, C.POINTER(C.c_ulonglong)]),
+    "ptt_cdf_stencil": (_i, [_p, _i, _dp, _i]),
+    "ptt_cdf_lf_flux": (_i, [_p, _i, _dp, _dp, _dp, _d, _d]),
+    "ptt_cdf_lw_rhs": (_i, [_p, _i, _dp, _dp, _dp, _dp, _d, _d]),
+    "ptt_marginal_cusum": (_i, [_p, _i, _dp]),
+    "ptt_marginal_trap": (_i, [_p, _i, _dp]),
+    "ptt_scale_weight_sum": (_i, [_p, _i, _dp, _dp]),
+    "ptt_apply_marginal": (_i, [_p, _i, _dp, _p]),
     "ptt_ctx_mem_info": (_i, [_p, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
     "ptt_ctx_elapsed": (_i, [_p, _i, _i, _dp]),
     "ptt_ctx_time_kernels": (_i, [_p, _i]),
@@ -153,6 +160,10 @@ def _check(rc):
 
 def _iarr(v):
     return (C.c_int * len(v))(*[int(t) for t in v])
+
+
+def _vec(v):
+    return np.ascontiguousarray(v, dtype=np.float64)
 
 
 class Context:
@@ -326,6 +337,36 @@ class TT:
         s = np.ascontiguousarray(sten, dtype=np.float64)
         _check(lib().ptt_stencil(self.h, int(mode), s.ctypes.data_as(_dp), len(s)))
         return self
+
+    # CDF-problem stencils and marginals of the reference (paratt.c:772-1618)
+    def cdf_stencil(self, mode, sten):
+        s = _vec(sten)
+        _check(lib().ptt_cdf_stencil(self.h, int(mode), s.ctypes.data_as(_dp), len(s)))
+
+    def cdf_lf_flux(self, mode, wave_speed, gc_wave_speed, source_coef, dt, dx):
+        v = [_vec(t) for t in (wave_speed, gc_wave_speed, source_coef)]
+        _check(lib().ptt_cdf_lf_flux(self.h, int(mode), *[t.ctypes.data_as(_dp) for t in v], float(dt), float(dx)))
+
+    def cdf_lw_rhs(self, mode, wave_speed, gc_wave_speed, bdry_wave_speed, source_coef, dt, dx):
+        v = [_vec(t) for t in (wave_speed, gc_wave_speed, bdry_wave_speed, source_coef)]
+        _check(lib().ptt_cdf_lw_rhs(self.h, int(mode), *[t.ctypes.data_as(_dp) for t in v], float(dt), float(dx)))
+
+    def marginal_cusum(self, mode, w):
+        v = _vec(w)
+        _check(lib().ptt_marginal_cusum(self.h, int(mode), v.ctypes.data_as(_dp)))
+
+    def marginal_trap(self, mode, w):
+        v = _vec(w)
+        _check(lib().ptt_marginal_trap(self.h, int(mode), v.ctypes.data_as(_dp)))
+
+    def scale_weight_sum(self, mode, scale, sum_w):
+        a, b = _vec(scale), _vec(sum_w)
+        _check(lib().ptt_scale_weight_sum(self.h, int(mode), a.ctypes.data_as(_dp), b.ctypes.data_as(_dp)))
+
+    def apply_marginal(self, mode, w, out):
+        """out (d - 1 modes) <- this train contracted along `mode` with w."""
+        v = _vec(w)
+        _check(lib().ptt_apply_marginal(self.h, int(mode), v.ctypes.data_as(_dp), out.h))
 
     def dot(self, other):
         v = C.c_double()

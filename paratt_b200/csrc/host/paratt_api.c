@@ -348,24 +348,76 @@ attac_tt* attac_sum_of_product(double*** vec, int ndims, int* d, int R) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* outside the accelerated path                                             */
+/* CDF-problem stencils and marginals (paratt.c:772-1618), one process       */
 /* ------------------------------------------------------------------------ */
-static void out_of_scope(const char* f) {
-    fprintf(stderr,
-            "paratt_b200: %s belongs to the CDF / marginal post-processing of the reference "
-            "(paratt.c:772-1618) and is not provided by this library\n",
-            f);
-    exit(1);
+void pattac_apply_cdf_stencil(paratt* f, int mode, double* sten, int slen) {
+    ptt_tt* m = upload(f->x);
+    if (check(ptt_cdf_stencil(m, mode, sten, slen), "pattac_apply_cdf_stencil")) return;
+    download(f->x, m);
 }
-void pattac_apply_cdf_stencil(paratt* f, int m, double* s, int l) { (void)f; (void)m; (void)s; (void)l; out_of_scope(__func__); }
-void pattac_apply_cdf_lf_flux(paratt* f, int m, double* a, double* b, double* c, double dt, double dx)
-{ (void)f; (void)m; (void)a; (void)b; (void)c; (void)dt; (void)dx; out_of_scope(__func__); }
-void pattac_apply_cdf_lw_rhs(paratt* f, int m, double* a, double* b, double* c, double* e, double dt, double dx)
-{ (void)f; (void)m; (void)a; (void)b; (void)c; (void)e; (void)dt; (void)dx; out_of_scope(__func__); }
-void pattac_apply_marginal(paratt* f, paratt** o, int m, double* v) { (void)f; (void)o; (void)m; (void)v; out_of_scope(__func__); }
-void pattac_marginal_cusum(paratt* f, int m, double* v) { (void)f; (void)m; (void)v; out_of_scope(__func__); }
-void pattac_marginal_trap(paratt* f, int m, double* v) { (void)f; (void)m; (void)v; out_of_scope(__func__); }
-void pattac_scale_weight_sum(paratt* f, int m, double* s, double* w) { (void)f; (void)m; (void)s; (void)w; out_of_scope(__func__); }
+
+void pattac_apply_cdf_lf_flux(paratt* f, int mode, double* wave_speed, double* gc_wave_speed, double* source_coef,
+                              double dt, double dx) {
+    ptt_tt* m = upload(f->x);
+    if (check(ptt_cdf_lf_flux(m, mode, wave_speed, gc_wave_speed, source_coef, dt, dx), "pattac_apply_cdf_lf_flux"))
+        return;
+    download(f->x, m);
+}
+
+void pattac_apply_cdf_lw_rhs(paratt* f, int mode, double* wave_speed, double* gc_wave_speed, double* bdry_wave_speed,
+                             double* source_coef, double dt, double dx) {
+    ptt_tt* m = upload(f->x);
+    if (check(ptt_cdf_lw_rhs(m, mode, wave_speed, gc_wave_speed, bdry_wave_speed, source_coef, dt, dx),
+              "pattac_apply_cdf_lw_rhs"))
+        return;
+    download(f->x, m);
+}
+
+void pattac_marginal_cusum(paratt* f, int mode, double* row_vector) {
+    ptt_tt* m = upload(f->x);
+    if (check(ptt_marginal_cusum(m, mode, row_vector), "pattac_marginal_cusum")) return;
+    download(f->x, m);
+}
+
+void pattac_marginal_trap(paratt* f, int mode, double* row_vector) {
+    ptt_tt* m = upload(f->x);
+    if (check(ptt_marginal_trap(m, mode, row_vector), "pattac_marginal_trap")) return;
+    download(f->x, m);
+}
+
+void pattac_scale_weight_sum(paratt* f, int mode, double* scale, double* sum_w) {
+    ptt_tt* m = upload(f->x);
+    if (check(ptt_scale_weight_sum(m, mode, scale, sum_w), "pattac_scale_weight_sum")) return;
+    download(f->x, m);
+}
+
+/* The marginal with one mode fewer is allocated here, as the reference does
+ * (paratt.c:1258-1282); *marginal must be NULL on entry. */
+void pattac_apply_marginal(paratt* f, paratt** marginal, int mode, double* row_vector) {
+    if (*marginal != NULL) {
+        fprintf(stderr, "pattac_apply_marginal: Error.\nInput marginal_tt_ptr was not NULL.\n");
+        exit(1);
+    }
+    const int d = f->numDim;
+    if (d < 2 || mode < 0 || mode >= d) {
+        fprintf(stderr, "paratt_b200: pattac_apply_marginal: mode %d of a %d-mode train\n", mode, d);
+        exit(1);
+    }
+    int dims[PTT_MAX_DIM], ranks[PTT_MAX_DIM + 1];
+    for (int k = 0, t = 0; k < d; k++)
+        if (k != mode) dims[t++] = f->dim[k];
+    for (int t = 0; t < d; t++) {
+        if (mode < d - 1)
+            ranks[t] = t <= mode ? f->x->ttRank[t] : f->x->ttRank[t + 1];
+        else
+            ranks[t] = t < d - 1 ? f->x->ttRank[t] : 1;
+    }
+    *marginal = alloc_ptt(d - 1, dims, ranks);
+    ptt_tt* mx = upload(f->x);
+    ptt_tt* mz = mirror((*marginal)->x, ranks);
+    if (check(ptt_apply_marginal(mx, mode, row_vector, mz), "pattac_apply_marginal")) return;
+    download((*marginal)->x, mz);
+}
 
 /* ------------------------------------------------------------------------ */
 /* .cr files: header "r_l,N,r_r\n", then r_l*N*r_r values "%+1.16e\n" in    */

@@ -32,6 +32,7 @@ struct DevDesc {
 
 struct ptt_ctx {
     int device;
+    int nsm;                      // streaming multiprocessors of the device
     cudaStream_t stream;
     cudaStream_t side;            // second stream for overlapped work
     cudaEvent_t ev_fork, ev_join;
@@ -184,6 +185,13 @@ int ptt_graph_run(ptt_ctx* c, const void* key, size_t keylen, const std::functio
 void ptt_graph_clear(ptt_ctx* c);
 int ptt_round_phases_rk(ptt_tt* x, const int* rk, double tol, const int* maxrank, int phases, int only);
 double ptt_round_threshold(const ptt_tt* x, double tol);
+
+// Blocks per core of a grid-stride launch over d cores (grid y = core): a
+// few waves over the device (32 blocks of 256 threads per SM in total).
+static inline int ptt_core_grid_cap(const ptt_ctx* c, int d) {
+    const int cap = 32 * c->nsm / (d > 0 ? d : 1);
+    return cap < 1 ? 1 : cap;
+}
 
 // Round a size up to a multiple of 256 bytes.
 static inline size_t ptt_align(size_t b) { return (b + 255) & ~(size_t)255; }

@@ -59,6 +59,10 @@ extern "C" ptt_ctx* ptt_ctx_create(int device) {
     if (ptt_cuda_check(cudaSetDevice(device), "cudaSetDevice")) return NULL;
     ptt_ctx* c = (ptt_ctx*)calloc(1, sizeof(ptt_ctx));
     c->device = device;
+    if (cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || c->nsm < 1) {
+        cudaGetLastError();
+        c->nsm = 148;
+    }
     if (ptt_cuda_check(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream") ||
         ptt_cuda_check(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking), "stream") ||
         ptt_cuda_check(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming), "event") ||
@@ -646,9 +650,8 @@ extern "C" int ptt_tt_copy(ptt_tt* dst, const ptt_tt* src) {
     long long mx = 0;
     for (int k = 0; k < src->d; k++) mx = src->cap[k] > mx ? src->cap[k] : mx;
     int bx = (int)((mx + 255) / 256);
-    if (bx > 1184) bx = 1184;
     // a few waves over the GPU in total; the loop strides over any core size
-    const int bcap = 4736 / src->d > 0 ? 4736 / src->d : 1;
+    const int bcap = ptt_core_grid_cap(c, src->d);
     if (bx > bcap) bx = bcap;
     if (src->ctx != c) {
         PTT_CUDA(cudaEventRecord(src->ctx->ev_fork, src->ctx->stream));

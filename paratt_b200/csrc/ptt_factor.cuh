@@ -226,6 +226,8 @@ template <int CT>
 __global__ void __launch_bounds__(NT, 1) k_tsqr_factor(const DevDesc* D, int kcore, int mode, Plan pl, double* ws,
                                                        int* status) {
     constexpr int NU = FCfg<CT>::NU, NV = FCfg<CT>::NV, NG = FCfg<CT>::NG, NR = FCfg<CT>::NR, VB = FCfg<CT>::VB;
+    PTT_PDL_ENTRY();
+    if (gq_finished(pl)) return;  // factored by the grid Cholesky QR
     extern __shared__ double sm[];
     double* Rb = sm;                 // CT x CT, row-major
     double* vbuf = Rb + CT * CT;     // 2 x VB

@@ -30,15 +30,55 @@ static inline int elem_blocks(long long maxcnt) {
     return (int)b;
 }
 
-// Blocks per core of a launch over all d cores (grid y = core).  The count is
-// sized by the capacity, which can be far above the actual ranks: a few
-// waves over the GPU (148 SMs x 32 blocks) are enough at full size, and the
-// grid-stride loops cover any core with any grid.
-static inline int core_blocks(long long maxcnt, int d) {
+// Blocks per core of an element-wise launch over all d cores (grid y =
+// core): sized by the largest capacity, capped at a few waves over the
+// device; the grid-stride loops cover any core with any grid.
+static inline int core_blocks(const ptt_ctx* c, long long maxcnt, int d) {
     const int b = elem_blocks(maxcnt);
-    int cap = 4736 / (d > 0 ? d : 1);
-    if (cap < 1) cap = 1;
+    const int cap = ptt_core_grid_cap(c, d);
     return b < cap ? b : cap;
+}
+
+// Fibers of a core: element (i, f) at i + R f, f = j + n l (the column-major
+// core seen as R x (n R1)).  A group of G lanes (a power of two; 32 once
+// R >= 32) takes one fiber at a time, so a fiber's rows are contiguous
+// accesses of consecutive lanes and (j, l) cost one 32-bit division per
+// fiber instead of 64-bit divisions per element.
+struct FiberIter {
+    int G, li;
+    long long f0, fstep;
+};
+__device__ __forceinline__ FiberIter fiber_iter(int R) {
+    FiberIter it;
+    int G = 32;
+    if (R < 32) {
+        G = 1;
+        while (G < R) G <<= 1;
+    }
+    const int lane = threadIdx.x & 31;
+    const int per = 32 / G;
+    it.G = G;
+    it.li = lane & (G - 1);
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    it.f0 = warp * per + lane / G;
+    it.fstep = nw * per;
+    return it;
+}
+
+// Blocks per core of a fiber launch over d cores (grid y = core): enough for
+// the largest core's fibers at 8 per block (one per warp of 256 threads),
+// capped at 32 blocks per SM over the whole grid.
+static inline int fiber_blocks(const ptt_ctx* c, const ptt_tt* z, int d) {
+    long long nf = 1;
+    for (int k = 0; k < d; k++) {
+        const long long f = (long long)z->n[k] * z->rcap[k + 1];
+        nf = f > nf ? f : nf;
+    }
+    long long b = (nf + 7) / 8;
+    const long long cap = ptt_core_grid_cap(c, d);
+    if (b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
 }
 
 // ---------------------------------------------------------------------------
@@ -96,31 +136,34 @@ __global__ void k_axpby(const DevDesc* X, const DevDesc* Y, DevDesc* Z, double a
     const double* xc = X->core[k];
     const double* yc = Y->core[k];
     double* zc = Z->alt[k];
-    const long long stride = (long long)gridDim.x * blockDim.x;
     if (d == 1) {
+        const long long stride = (long long)gridDim.x * blockDim.x;
         for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += stride)
             zc[e] = a * xc[e] + b * yc[e];
         return;
     }
-    const long long rzn = (long long)rz * n;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += stride) {
-        const int l = (int)(e / rzn);
-        const long long rem = e - l * rzn;
-        const int j = (int)(rem / rz);
-        const int i = (int)(rem - (long long)j * rz);
-        double v;
+    // fiber (j, l) of z: x's fiber over zeros (l < rx1), zeros over y's fiber
+    // (l >= rx1); core 0 is [a x_0 | b y_0], the last core stacks x over y
+    const int NF = n * rz1;
+    const FiberIter it = fiber_iter(rz);
+    for (long long f = it.f0; f < NF; f += it.fstep) {
+        const int fi = (int)f, l = fi / n, j = fi - l * n;
+        double* zf = zc + (long long)rz * fi;
         if (k == 0) {
-            v = (l < rx1) ? a * xc[j + (long long)n * l] : b * yc[j + (long long)n * (l - rx1)];
+            if (it.li == 0) zf[0] = (l < rx1) ? a * xc[j + (long long)n * l] : b * yc[j + (long long)n * (l - rx1)];
         } else if (k == d - 1) {
-            v = (i < rx) ? xc[i + (long long)rx * j] : yc[(i - rx) + (long long)ry * j];
-        } else if (i < rx && l < rx1) {
-            v = xc[i + (long long)rx * (j + (long long)n * l)];
-        } else if (i >= rx && l >= rx1) {
-            v = yc[(i - rx) + (long long)ry * (j + (long long)n * (l - rx1))];
+#pragma unroll 4
+            for (int i = it.li; i < rz; i += it.G)
+                zf[i] = (i < rx) ? xc[i + (long long)rx * j] : yc[(i - rx) + (long long)ry * j];
+        } else if (l < rx1) {
+            const double* src = xc + (long long)rx * (j + (long long)n * l);
+#pragma unroll 4
+            for (int i = it.li; i < rz; i += it.G) zf[i] = (i < rx) ? src[i] : 0.0;
         } else {
-            v = 0.0;
+            const double* src = yc + (long long)ry * (j + (long long)n * (l - rx1));
+#pragma unroll 4
+            for (int i = it.li; i < rz; i += it.G) zf[i] = (i >= rx) ? src[i - rx] : 0.0;
         }
-        zc[e] = v;
     }
 }
 
@@ -172,7 +215,8 @@ extern "C" int ptt_axpby(double a, const ptt_tt* x, double b, const ptt_tt* y, p
     if (!newr) return ptt_set_error(PTT_ERR_ARG, "d too large");
     long long mx = 0;
     for (int k = 0; k < d; k++) mx = z->cap[k] > mx ? z->cap[k] : mx;
-    k_axpby<<<dim3(core_blocks(mx, d), d), 256, 0, c->stream>>>(x->dd, y->dd, z->dd, a, b, newr, c->d_status);
+    (void)mx;
+    k_axpby<<<dim3(fiber_blocks(c, z, d), d), 256, 0, c->stream>>>(x->dd, y->dd, z->dd, a, b, newr, c->d_status);
     PTT_LAUNCHED(c);
     return finalize(z, newr, 0, d, 1);
 }
@@ -198,16 +242,19 @@ __global__ void k_hadamard(const DevDesc* X, const DevDesc* Y, DevDesc* Z, int* 
     const double* xc = X->core[k];
     const double* yc = Y->core[k];
     double* zc = Z->alt[k];
-    const long long rzn = (long long)rz * n;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += stride) {
-        const int lz = (int)(e / rzn);
-        const long long rem = e - lz * rzn;
-        const int j = (int)(rem / rz);
-        const int iz = (int)(rem - (long long)j * rz);
-        const int ix = iz / ry, ky = iz - ix * ry;
+    // fiber (j, lz), lz = ly + ry1 jx: rows iz = ky + ry ix
+    const int NF = n * rz1;
+    const FiberIter it = fiber_iter(rz);
+    for (long long f = it.f0; f < NF; f += it.fstep) {
+        const int fi = (int)f, lz = fi / n, j = fi - lz * n;
         const int jx = lz / ry1, ly = lz - jx * ry1;
-        zc[e] = xc[ix + (long long)rx * (j + (long long)n * jx)] * yc[ky + (long long)ry * (j + (long long)n * ly)];
+        const double* xf = xc + (long long)rx * (j + (long long)n * jx);
+        const double* yf = yc + (long long)ry * (j + (long long)n * ly);
+        double* zf = zc + (long long)rz * fi;
+        for (int iz = it.li; iz < rz; iz += it.G) {
+            const int ix = iz / ry, ky = iz - ix * ry;
+            zf[iz] = xf[ix] * yf[ky];
+        }
     }
 }
 
@@ -223,7 +270,8 @@ extern "C" int ptt_hadamard(const ptt_tt* x, const ptt_tt* y, ptt_tt* z) {
     if (!newr) return ptt_set_error(PTT_ERR_ARG, "d too large");
     long long mx = 0;
     for (int k = 0; k < d; k++) mx = z->cap[k] > mx ? z->cap[k] : mx;
-    k_hadamard<<<dim3(core_blocks(mx, d), d), 256, 0, c->stream>>>(x->dd, y->dd, z->dd, newr, c->d_status);
+    (void)mx;
+    k_hadamard<<<dim3(fiber_blocks(c, z, d), d), 256, 0, c->stream>>>(x->dd, y->dd, z->dd, newr, c->d_status);
     PTT_LAUNCHED(c);
     return finalize(z, newr, 0, d, 1);
 }
@@ -294,7 +342,7 @@ extern "C" int ptt_square_sym(const ptt_tt* x, ptt_tt* z) {
     if (!newr) return ptt_set_error(PTT_ERR_ARG, "d too large");
     long long mx = 0;
     for (int k = 0; k < d; k++) mx = z->cap[k] > mx ? z->cap[k] : mx;
-    k_square_sym<<<dim3(core_blocks(mx, d), d), 256, 0, c->stream>>>(x->dd, z->dd, newr, c->d_status);
+    k_square_sym<<<dim3(core_blocks(c, mx, d), d), 256, 0, c->stream>>>(x->dd, z->dd, newr, c->d_status);
     PTT_LAUNCHED(c);
     return finalize(z, newr, 0, d, 1);
 }
@@ -348,23 +396,23 @@ extern "C" int ptt_mult_diag(ptt_tt* x, int mode, const double* vec) {
 __global__ void k_stencil(DevDesc* X, int k, Stencil st) {
     const int r = X->r[k], n = X->n[k], r1 = X->r[k + 1];
     const int h = (st.len - 1) / 2;
-    const long long slab = (long long)r * n;
     const double* in = X->core[k];
     double* out = X->alt[k];
-    for (int l = blockIdx.y; l < r1; l += gridDim.y) {
-        const double* fi = in + slab * l;
-        double* fo = out + slab * l;
-        for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < slab;
-             e += (long long)gridDim.x * blockDim.x) {
-            const int a = (int)(e / r);
-            const int i = (int)(e - (long long)a * r);
+    // fiber (a, l): out[:, a, l] = sum_t s_t in[:, (a + t - h) mod n, l]
+    const int NF = n * r1;
+    const FiberIter it = fiber_iter(r);
+    for (long long f = it.f0; f < NF; f += it.fstep) {
+        const int fi = (int)f, l = fi / n, a = fi - l * n;
+        const double* fl = in + (long long)r * n * l;
+        double* fo = out + (long long)r * fi;
+        for (int i = it.li; i < r; i += it.G) {
             double acc = 0.0;
             for (int t = 0; t < st.len; t++) {
                 int src = a + t - h;
                 src = src < 0 ? src + n : (src >= n ? src - n : src);
-                acc += st.s[t] * fi[i + (long long)r * src];
+                acc += st.s[t] * fl[i + (long long)r * src];
             }
-            fo[e] = acc;
+            fo[i] = acc;
         }
     }
 }
@@ -386,12 +434,10 @@ extern "C" int ptt_stencil(ptt_tt* x, int mode, const double* sten, int slen) {
     if ((st.len - 1) / 2 >= x->n[mode] && st.len > 1)
         return ptt_set_error(PTT_ERR_ARG, "stencil half-width exceeds mode size");
     ptt_ctx* c = x->ctx;
-    long long slab = (long long)x->rcap[mode] * x->n[mode];
-    int bx = (int)((slab + 255) / 256);
-    int by = x->rcap[mode + 1];
-    if (bx > 64) bx = 64;
-    if (by > 1024) by = 1024;
-    k_stencil<<<dim3(bx, by), 256, 0, c->stream>>>(x->dd, mode, st);
+    long long bx = ((long long)x->n[mode] * x->rcap[mode + 1] + 7) / 8;  // 8 fibers per block
+    if (bx > 8LL * c->nsm) bx = 8LL * c->nsm;
+    if (bx < 1) bx = 1;
+    k_stencil<<<dim3((unsigned)bx), 256, 0, c->stream>>>(x->dd, mode, st);
     PTT_LAUNCHED(c);
     k_finalize<<<1, 32, 0, c->stream>>>(x->dd, NULL, mode, mode + 1, 0);
     PTT_LAUNCHED(c);
@@ -435,33 +481,30 @@ __global__ void k_opsum(const DevDesc* X, DevDesc* Y, Stencil st, double shift, 
     }
     const double* xc = X->core[k];
     double* yc = Y->alt[k];
-    const long long ryn = (long long)ry * n;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int l = (int)(e / ryn);
-        const long long rem = e - l * ryn;
-        const int j = (int)(rem / ry);
-        const int i = (int)(rem - (long long)j * ry);
-        double v;
+    // fiber (j, l) of y; l' = l - r1 for the second block column
+    const int NF = n * ry1;
+    const FiberIter it = fiber_iter(ry);
+    for (long long f = it.f0; f < NF; f += it.fstep) {
+        const int fi = (int)f, l = fi / n, j = fi - l * n;
+        double* yf = yc + (long long)ry * fi;
         if (d == 1) {
-            v = sten_at(xc, 1, n, 0, j, 0, st) + shift * xc[j];
+            if (it.li == 0) yf[0] = sten_at(xc, 1, n, 0, j, 0, st) + shift * xc[j];
         } else if (k == 0) {
-            v = (l < r1) ? xc[j + (long long)n * l]
-                         : sten_at(xc, 1, n, 0, j, l - r1, st) + shift * xc[j + (long long)n * (l - r1)];
+            if (it.li == 0)
+                yf[0] = (l < r1) ? xc[j + (long long)n * l]
+                                 : sten_at(xc, 1, n, 0, j, l - r1, st) + shift * xc[j + (long long)n * (l - r1)];
         } else if (k == d - 1) {
-            v = (i < r) ? sten_at(xc, r, n, i, j, 0, st) : xc[(i - r) + (long long)r * j];
+            for (int i = it.li; i < ry; i += it.G)
+                yf[i] = (i < r) ? sten_at(xc, r, n, i, j, 0, st) : xc[(i - r) + (long long)r * j];
+        } else if (l < r1) {
+            const double* src = xc + (long long)r * (j + (long long)n * l);
+#pragma unroll 4
+            for (int i = it.li; i < ry; i += it.G) yf[i] = (i < r) ? src[i] : 0.0;
         } else {
-            const bool a = i >= r, b = l >= r1;
-            if (!a && !b)
-                v = xc[i + (long long)r * (j + (long long)n * l)];
-            else if (!a && b)
-                v = sten_at(xc, r, n, i, j, l - r1, st);
-            else if (a && b)
-                v = xc[(i - r) + (long long)r * (j + (long long)n * (l - r1))];
-            else
-                v = 0.0;
+            const int lp = l - r1;
+            const double* src = xc + (long long)r * (j + (long long)n * lp);
+            for (int i = it.li; i < ry; i += it.G) yf[i] = (i < r) ? sten_at(xc, r, n, i, j, lp, st) : src[i - r];
         }
-        yc[e] = v;
     }
 }
 
@@ -481,7 +524,8 @@ extern "C" int ptt_op_sum(const ptt_tt* x, const double* sten, int slen, double 
     int* newr = ranks_scratch(c, d);
     long long mx = 0;
     for (int k = 0; k < d; k++) mx = y->cap[k] > mx ? y->cap[k] : mx;
-    k_opsum<<<dim3(core_blocks(mx, d), d), 256, 0, c->stream>>>(x->dd, y->dd, st, shift, newr, c->d_status);
+    (void)mx;
+    k_opsum<<<dim3(fiber_blocks(c, y, d), d), 256, 0, c->stream>>>(x->dd, y->dd, st, shift, newr, c->d_status);
     PTT_LAUNCHED(c);
     return finalize(y, newr, 0, d, 1);
 }

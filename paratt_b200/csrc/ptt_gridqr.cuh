@@ -1,0 +1,542 @@
+// Cholesky QR of unfoldings with up to 64 columns by the whole GPU (included
+// by ptt_round.cu inside its anonymous namespace, after ptt_cholqr.cuh).
+//
+// At 64 columns a bond's unfolding (16384 x 64 doubles at d = 40, n = 256,
+// rank 64: 8.4 MB) no longer fits in one cluster's shared memory, and the
+// Householder TSQR costs one block barrier per reflector and tree level.
+// Here the rows are spread over all SMs and the same Gram-stage sequence as
+// the cluster kernel (ptt_cholqr.cuh) runs as one launch per stage:
+//
+//   stage 0        CTA b loads rows [b rpb, (b+1) rpb) of A, forms the
+//                  partial Gram matrix of its rows;
+//   stage s >= 1   CTA b loads its rows of Q_{s-1} (A for s = 1), applies the
+//                  factor of the previous stage by a row-wise triangular solve
+//                  (Q_s = Q_{s-1} R_s^{-1}), writes Q_s and forms the partial
+//                  Gram matrix of Q_s;
+//
+// and the partials are summed in a fixed order by the last-arriving CTA of
+// each group of GROUP CTAs (atomic ticket, no waiting), then by the
+// last-arriving group, which takes the decision of the stage exactly as the
+// cluster kernel does: done (max|Q^T Q - I| <= 1e-13), a first-order factor
+// I + striu(E) + diag(E)/2 (finishing without another Gram stage when
+// max|E| <= 1e-8), a Cholesky factor of G, or of G + sigma I when a pivot is
+// not positive or the pivots span more than 12 decades (shifted Cholesky QR,
+// Fukaya, Kannan, Nakatsukasa, Yamamoto, Yanagisawa, SIAM J. Sci. Comput. 42
+// (2020), sigma = 11 (m c + c (c + 1)) u ||Q||_F^2).  The host launches MAXST
+// stages; a stage finds the state left by the previous one and returns at
+// once when the factorisation is finished or has fallen back.  The row-wise
+// triangular solve changes A = Q R by O(u ||A||) per stage, so R carries the
+// singular values to the accuracy of a Householder R.
+//
+// Q is written to Qbuf: LEFT -> alt[k] (m x c, column-major, its final place);
+// RIGHT_T -> a scratch region (row-major rows of c), from which k_gq_write
+// forms Q V_r after the bond's SVD.  A never changes, so a bond that falls
+// back (NaN, zero matrix or column, no convergence in MAXST stages) is
+// factored by the Householder TSQR from the same input; those kernels skip
+// the bonds finished here (Plan::gqstate).
+#pragma once
+
+namespace gq {
+
+constexpr int NT = 256;
+constexpr int CB = 64;                 // column bound
+constexpr int XP = CB + 2;             // pitch of the rows in shared memory (even: 16-byte pairs)
+constexpr int RP = CB + 2;             // pitch of a factor R (row-major, upper triangular)
+constexpr int GP = CB + 1;             // pitch of the Gram matrix of the deciding CTA
+constexpr int TS = CB / 8;             // Gram tiles are TS x TS, 8 x 8 of them
+constexpr int UP = 36 * TS * TS;       // entries of the 36 upper tiles
+constexpr int NG = 7;                  // row groups of the Gram threads (36 tiles x 7 = 252)
+constexpr int GROUP = 8;               // CTAs summed by the first level
+constexpr int RPB_MAX = 112;           // rows per CTA
+constexpr int RPB_MIN = 16;
+constexpr int MAXST = 6;               // stage launches per factorisation
+constexpr int LTRI = CB * (CB + 1) / 2;
+constexpr int EPT = (LTRI + NT - 1) / NT;  // lower-triangle entries per thread of the Cholesky
+constexpr double TAU = 1e-13;
+constexpr double FIRST = 1e-7;
+constexpr double FIRST_DONE = 1e-8;
+constexpr double U = 1.1102230246251565e-16;
+constexpr size_t SMEM = sizeof(double) * ((size_t)RPB_MAX * XP + (size_t)NG * UP);
+static_assert(CB * GP + CB * RP + CB + CB * GP + 2 * CB <= NG * UP, "decision arrays fit the Gram scratch");
+static_assert(CB * RP + CB <= NG * UP, "factor fits the Gram scratch");
+
+enum { RUN = 0, DONE = 1, FALLBACK = 2, FINISH = 4 };
+
+__host__ __device__ __forceinline__ bool finished(int s) { return s == DONE || s == FINISH; }
+
+// Record of the factorisation in flight (rec[0..)):
+struct State {
+    int state;   // RUN, DONE, FALLBACK, FINISH
+    int fin;     // FINISH: the stage launch that applies the last factor
+    int nst;     // factors applied
+    int nshift;  // shifted stages (diagnostic)
+    int m, c;
+    int pad[2];
+};
+
+struct GQ {
+    double* rec;         // State, then the factor and the accumulated R
+    double* part;        // per-CTA partial Gram matrices (UP each)
+    double* gpart;       // per-group sums
+    double* qscr;        // Q rows of a RIGHT_T factorisation (row-major, pitch c)
+    int* cnt;            // tickets: [group] ... [ngroups] = top; zero between launches
+    int rpb;             // rows per CTA
+};
+constexpr long long O_FAC = 8;                   // CB x RP factor, then CB inverse pivots
+constexpr long long O_T = O_FAC + CB * RP + CB;  // CB x CB accumulated R (row-major)
+constexpr long long REC = O_T + CB * CB;
+
+// rows per CTA and CTAs for an unfolding of at most mcap rows
+__host__ __forceinline__ int rows_per_cta(long long mcap, int nsm) {
+    long long r = (mcap + nsm - 1) / nsm;
+    if (r < RPB_MIN) r = RPB_MIN;
+    if (r > RPB_MAX) r = RPB_MAX;
+    return (int)r;
+}
+__host__ __forceinline__ int ctas(long long mcap, int rpb) {
+    long long b = (mcap + rpb - 1) / rpb;
+    return (int)(b < 1 ? 1 : b);
+}
+
+// x <- x R^{-1} for one row held in shared memory (R upper triangular, pitch
+// RP, zero below the diagonal and beyond c; inverse pivots in iv).  The row
+// lives in registers; each R entry is a broadcast 16-byte load.
+__device__ __forceinline__ void row_solve(double* xs, const double* R, const double* iv, int c) {
+    double x[CB];
+#pragma unroll
+    for (int j = 0; j < CB; j += 2) {
+        const double2 v = *(const double2*)(xs + j);
+        x[j] = v.x;
+        x[j + 1] = v.y;
+    }
+#pragma unroll
+    for (int j = 0; j < CB; j++) {
+        if (j < c) {
+            const double y = x[j] * iv[j];
+            x[j] = y;
+            const double* Rj = R + j * RP;
+#pragma unroll
+            for (int l = (j + 1) & ~1; l < CB; l += 2) {
+                const double2 r2 = *(const double2*)(Rj + l);
+                if (l > j) x[l] = fma(-y, r2.x, x[l]);
+                x[l + 1] = fma(-y, r2.y, x[l + 1]);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < CB; j += 2) *(double2*)(xs + j) = make_double2(x[j], x[j + 1]);
+}
+
+// lower-triangle entry e (row-major packing) -> (i, l), l <= i
+__device__ __forceinline__ void tri_index(int e, int* i, int* l) {
+    int r = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+    while ((r + 1) * (r + 2) / 2 <= e) r++;
+    while (r * (r + 1) / 2 > e) r--;
+    *i = r;
+    *l = e - r * (r + 1) / 2;
+}
+
+// Cholesky factor of G + shift I (c x c, pitch GP) by all NT threads:
+// right-looking, every thread keeps its lower-triangle entries in registers,
+// and the column of the next step is published through a double buffer, so
+// each step costs one block barrier.  Result: R = L^T (row-major, pitch RP,
+// zero outside the upper c x c triangle) and inverse pivots iv[j].  Returns
+// false when a pivot is not positive (NaN included); *ratio = min/max pivot.
+__device__ bool block_chol(const double* G, int c, double shift, double* R, double* iv, double* col2, double* ratio) {
+    const int tid = threadIdx.x;
+    double a[EPT];
+    int ii[EPT], ll[EPT];
+#pragma unroll
+    for (int s = 0; s < EPT; s++) {
+        const int e = tid + NT * s;
+        int i = CB, l = CB;
+        if (e < LTRI) tri_index(e, &i, &l);
+        ii[s] = i;
+        ll[s] = l;
+        a[s] = (i < c && l < c) ? G[i * GP + l] + (i == l ? shift : 0.0) : 0.0;
+    }
+    for (int e = tid; e < CB * RP; e += NT) R[e] = 0.0;
+    for (int e = tid; e < CB; e += NT) iv[e] = 0.0;
+#pragma unroll
+    for (int s = 0; s < EPT; s++)
+        if (ll[s] == 0 && ii[s] < CB) col2[ii[s]] = a[s];
+    bool ok = true;
+    double dmin = 1.0 / 0.0, dmax = 0.0;
+    for (int j = 0; j < c; j++) {
+        __syncthreads();
+        const double* col = col2 + (j & 1) * CB;
+        double* nxt = col2 + ((j + 1) & 1) * CB;
+        const double d = col[j];
+        ok = ok && (d > 0.0);
+        dmin = fmin(dmin, d);
+        dmax = fmax(dmax, d);
+        const double dd = d > 0.0 ? d : 1.0;
+        const double inv = rsqrt(dd);
+        const double piv = dd * inv;
+#pragma unroll
+        for (int s = 0; s < EPT; s++) {
+            const int i = ii[s], l = ll[s];
+            if (i >= c) continue;
+            if (l == j) {
+                R[j * RP + i] = (i == j) ? piv : a[s] * inv;
+            } else if (l > j) {
+                a[s] = fma(-(col[i] * inv), col[l] * inv, a[s]);
+                if (l == j + 1) nxt[i] = a[s];
+            }
+        }
+        if (tid == 0) iv[j] = inv;
+    }
+    __syncthreads();
+    *ratio = dmax > 0.0 ? dmin / dmax : 0.0;
+    return ok;
+}
+
+// One stage of the factorisation of core k's unfolding (mode); gridDim.x CTAs
+// of g.rpb rows each.
+__global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int mode, Plan pl, GQ g, double* ws,
+                                                    int stage, long long* qstat) {
+    PTT_PDL_ENTRY();
+    extern __shared__ double gsm[];
+    double* Xs = gsm;                     // rpb x XP rows
+    double* sScr = Xs + RPB_MAX * XP;     // factor; Gram partials; decision arrays
+    __shared__ int s_state, s_fin, s_ticket, s_flags;
+    __shared__ double s_red[NT / 32][2];
+    State* st = (State*)g.rec;
+    const View A = make_view(D, k, mode, false);
+    const int m = A.m, c = A.c;
+    const int tid = threadIdx.x;
+    const int rpb = g.rpb, nb = (int)gridDim.x, b = (int)blockIdx.x;
+    if (stage == 0) {
+        if (c > CB || c < 1 || m < c || (long long)m > (long long)rpb * nb) {  // uniform
+            if (b == 0 && tid == 0) {
+                st->state = FALLBACK;
+                st->nst = 0;
+                st->m = m;
+                st->c = c;
+                if (qstat) atomicAdd((unsigned long long*)(qstat + 1), 1ull);
+            }
+            return;
+        }
+        if (pl.work && b == 0 && tid == 0) atomicAdd(pl.work, 16.0 * (double)m * (double)c);
+    } else {
+        if (tid == 0) {
+            s_state = ldcg(&st->state);
+            s_fin = ldcg(&st->fin);
+        }
+        __syncthreads();
+        if (!(s_state == RUN || (s_state == FINISH && s_fin == stage))) return;
+    }
+    const int r0 = b * rpb;
+    const int h = (m - r0) < rpb ? ((m - r0) > 0 ? (m - r0) : 0) : rpb;
+    // Qbuf: where the Q_s rows live
+    View Qv;
+    if (mode == LEFT) {
+        Qv.p = D->alt[k];
+        Qv.rs = 1;
+        Qv.cs = m;
+    } else {
+        Qv.p = g.qscr;
+        Qv.rs = c;
+        Qv.cs = 1;
+    }
+    const View& src = (stage <= 1) ? A : Qv;
+    // this CTA's rows (zero beyond c), every element in flight by cp.async
+    for (int e = tid; e < h * XP; e += NT) Xs[e] = 0.0;
+    if (stage >= 1) {  // the factor of the previous stage
+        const double* F = g.rec + O_FAC;
+        for (int e = tid; e < CB * RP + CB; e += NT) sScr[e] = ldcg(F + e);
+    }
+    __syncthreads();
+    {
+        const unsigned xs0 = (unsigned)__cvta_generic_to_shared(Xs);
+        const int tot = h * c;
+        for (int f = tid; f < tot; f += NT) {
+            int row, col;
+            if (src.rs == 1) {  // column-major: a column's rows are contiguous
+                col = f / h;
+                row = f - col * h;
+            } else {  // row-major rows of c
+                row = f / c;
+                col = f - row * c;
+            }
+            const double* gp = src.p + (long long)(r0 + row) * src.rs + (long long)col * src.cs;
+            const unsigned sa = xs0 + 8u * (unsigned)(row * XP + col);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gp) : "memory");
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+    }
+    __syncthreads();
+    if (stage >= 1) {
+        if (tid < h) row_solve(Xs + tid * XP, sScr, sScr + CB * RP, c);
+        __syncthreads();
+        const int tot = h * c;
+        for (int f = tid; f < tot; f += NT) {
+            int row, col;
+            if (Qv.rs == 1) {
+                col = f / h;
+                row = f - col * h;
+            } else {
+                row = f / c;
+                col = f - row * c;
+            }
+            Qv.p[(long long)(r0 + row) * Qv.rs + (long long)col * Qv.cs] = Xs[row * XP + col];
+        }
+        if (s_state == FINISH) return;  // the last factor is applied: Q is final
+    }
+    // partial Gram matrix (upper tiles) of this CTA's rows
+    {
+        const int q = tid % 36, grp = tid / 36;
+        int ti, tj;
+        cq::upper_tile(q, &ti, &tj);
+        ti *= TS;
+        tj *= TS;
+        if (grp < NG) {
+            double acc[TS][TS];
+#pragma unroll
+            for (int a = 0; a < TS; a++)
+#pragma unroll
+                for (int bb = 0; bb < TS; bb++) acc[a][bb] = 0.0;
+            for (int r = grp; r < h; r += NG) {
+                double xa[TS], xb[TS];
+#pragma unroll
+                for (int a = 0; a < TS; a += 2) {
+                    const double2 va = *(const double2*)(Xs + r * XP + ti + a);
+                    const double2 vb = *(const double2*)(Xs + r * XP + tj + a);
+                    xa[a] = va.x;
+                    xa[a + 1] = va.y;
+                    xb[a] = vb.x;
+                    xb[a + 1] = vb.y;
+                }
+#pragma unroll
+                for (int a = 0; a < TS; a++)
+#pragma unroll
+                    for (int bb = 0; bb < TS; bb++) acc[a][bb] = fma(xa[a], xb[bb], acc[a][bb]);
+            }
+#pragma unroll
+            for (int a = 0; a < TS; a++)
+#pragma unroll
+                for (int bb = 0; bb < TS; bb++) sScr[grp * UP + q * TS * TS + a * TS + bb] = acc[a][bb];
+        }
+    }
+    __syncthreads();
+    {
+        double* P = g.part + (long long)b * UP;
+        for (int u = tid; u < UP; u += NT) {
+            double v = sScr[u];
+#pragma unroll
+            for (int g2 = 1; g2 < NG; g2++) v += sScr[g2 * UP + u];
+            P[u] = v;
+        }
+    }
+    // first level: the last CTA of each group sums the group's partials
+    const int ngroups = (nb + GROUP - 1) / GROUP;
+    const int grp = b / GROUP;
+    const int gsize = (nb - grp * GROUP) < GROUP ? (nb - grp * GROUP) : GROUP;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_ticket = atomicAdd(&g.cnt[grp], 1);
+    __syncthreads();
+    if (s_ticket != gsize - 1) return;
+    if (tid == 0) g.cnt[grp] = 0;
+    __threadfence();
+    {
+        const double* P = g.part + (long long)grp * GROUP * UP;
+        double* Gp = g.gpart + (long long)grp * UP;
+        for (int u = tid; u < UP; u += NT) {
+            double v = 0.0;
+            for (int t = 0; t < gsize; t++) v += ldcg(P + (long long)t * UP + u);
+            Gp[u] = v;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_ticket = atomicAdd(&g.cnt[ngroups], 1);
+    __syncthreads();
+    if (s_ticket != ngroups - 1) return;
+    if (tid == 0) g.cnt[ngroups] = 0;
+    __threadfence();
+    // ---- the deciding CTA: G = sum of the groups in order --------------------
+    double* sG = sScr;              // CB x GP
+    double* sF = sG + CB * GP;      // CB x RP factor
+    double* sIv = sF + CB * RP;     // CB inverse pivots
+    double* sT = sIv + CB;          // CB x GP accumulated R (the factors applied so far)
+    double* sCol = sT + CB * GP;    // 2 x CB
+    for (int e = tid; e < CB * GP; e += NT) sG[e] = 0.0;
+    if (tid == 0) s_flags = 0;
+    __syncthreads();
+    for (int u = tid; u < UP; u += NT) {
+        double v = 0.0;
+        for (int t = 0; t < ngroups; t++) v += ldcg(g.gpart + (long long)t * UP + u);
+        const int qq = u / (TS * TS), w = u - qq * (TS * TS);
+        int a0, b0;
+        cq::upper_tile(qq, &a0, &b0);
+        const int gi = a0 * TS + w / TS, gj = b0 * TS + w % TS;
+        if (gi < c && gj < c) {
+            sG[gi * GP + gj] = v;
+            sG[gj * GP + gi] = v;
+        }
+    }
+    for (int e = tid; e < CB * GP; e += NT) {
+        const int i = e / GP, j = e - (e / GP) * GP;
+        sT[e] = (stage == 0) ? ((i == j && i < c) ? 1.0 : 0.0) : ((j < CB) ? ldcg(g.rec + O_T + i * CB + j) : 0.0);
+    }
+    __syncthreads();
+    // trace, max |G - I|, NaN, zero column
+    double tr = 0.0, emax = 0.0;
+    int fl = 0;  // bit 0: NaN, bit 1: a zero diagonal entry (an exactly zero column)
+    for (int u = tid; u < c * c; u += NT) {
+        const int i = u / c, j = u - (u / c) * c;
+        const double v = sG[i * GP + j] - (i == j ? 1.0 : 0.0);
+        if (!(v == v)) fl |= 1;
+        emax = fmax(emax, fabs(v));
+        if (i == j) {
+            tr += sG[i * GP + j];
+            if (sG[i * GP + j] == 0.0) fl |= 2;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        tr += __shfl_xor_sync(0xffffffffu, tr, o);
+        emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+        fl |= __shfl_xor_sync(0xffffffffu, fl, o);
+    }
+    if ((tid & 31) == 0) {
+        s_red[tid >> 5][0] = tr;
+        s_red[tid >> 5][1] = emax;
+        if (fl) atomicOr(&s_flags, fl);
+    }
+    __syncthreads();
+    tr = 0.0;
+    emax = 0.0;
+    for (int w = 0; w < NT / 32; w++) {  // every thread, same order: same values
+        tr += s_red[w][0];
+        emax = fmax(emax, s_red[w][1]);
+    }
+    const bool nan = (s_flags & 1) || !(emax == emax);
+    const bool zcol = (s_flags & 2) != 0;
+    int nst = (stage == 0) ? 0 : ldcg(&st->nst);
+    int nshift = (stage == 0) ? 0 : ldcg(&st->nshift);
+    int dec;
+    if (nan || !(tr > 0.0) || !(tr < 1.0 / 0.0) || (stage == 0 && zcol)) {
+        dec = FALLBACK;
+    } else if (stage >= 1 && emax <= TAU) {
+        dec = DONE;
+    } else if (stage >= 1 && emax <= FIRST) {
+        for (int e = tid; e < CB * RP; e += NT) {
+            const int j = e / RP, l = e - (e / RP) * RP;
+            double v = 0.0;
+            if (j < c && l < c) {
+                if (l > j)
+                    v = sG[j * GP + l];
+                else if (l == j)
+                    v = 1.0 + 0.5 * (sG[j * GP + j] - 1.0);
+            }
+            sF[e] = v;
+        }
+        for (int j = tid; j < CB; j += NT) sIv[j] = j < c ? 1.0 / (1.0 + 0.5 * (sG[j * GP + j] - 1.0)) : 0.0;
+        dec = emax <= FIRST_DONE ? FINISH : RUN;
+    } else if (stage == MAXST - 1) {
+        dec = FALLBACK;
+    } else {
+        double ratio;
+        bool ok = block_chol(sG, c, 0.0, sF, sIv, sCol, &ratio);
+        if (!ok || ratio < 1e-12) {
+            const double sigma = 11.0 * ((double)m * c + (double)c * (c + 1)) * U * tr;
+            ok = block_chol(sG, c, sigma, sF, sIv, sCol, &ratio);
+            nshift++;
+        }
+        dec = ok ? RUN : FALLBACK;
+    }
+    if (stage == MAXST - 1 && (dec == RUN || dec == FINISH)) dec = FALLBACK;  // no launch left to apply it
+    __syncthreads();
+    if (dec == RUN || dec == FINISH) {
+        // new accumulated R = F T (both upper triangular), into sG (no longer needed)
+        for (int e = tid; e < CB * CB; e += NT) {
+            const int i = e / CB, j = e - (e / CB) * CB;
+            double v = 0.0;
+            if (j >= i && j < c) {
+                for (int t = i; t <= j; t++) v = fma(sF[i * RP + t], sT[t * GP + j], v);
+            }
+            sG[i * GP + j] = v;
+        }
+        __syncthreads();
+        double* F = g.rec + O_FAC;
+        for (int e = tid; e < CB * RP + CB; e += NT) F[e] = sF[e];
+        double* T = g.rec + O_T;
+        for (int e = tid; e < CB * CB; e += NT) T[e] = sG[(e / CB) * GP + (e % CB)];
+        nst++;
+    }
+    const double* Rfin = (dec == DONE) ? sT : sG;  // FINISH: the new accumulated R
+    if (dec == DONE || dec == FINISH) {
+        double* Rs = ws + pl.o_Rn;  // root slot (row-major CT x CT)
+        for (int e = tid; e < pl.CT * pl.CT; e += NT) {
+            const int i = e / pl.CT, j = e - (e / pl.CT) * pl.CT;
+            Rs[e] = (i < c && j < c && j >= i) ? Rfin[i * GP + j] : 0.0;
+        }
+        if (tid == 0) {
+            Info* info = pl.info;
+            info->m = m;
+            info->c = c;
+            info->q = c;
+            info->rank = 0;
+            info->status = 0;
+            if (qstat) {
+                atomicAdd((unsigned long long*)qstat, 1ull);
+                atomicAdd((unsigned long long*)(qstat + 2), (unsigned long long)(stage + 1));
+            }
+        }
+    }
+    if (tid == 0) {
+        if (dec == FALLBACK && qstat) atomicAdd((unsigned long long*)(qstat + 1), 1ull);
+        st->fin = stage + 1;
+        st->nst = nst;
+        st->nshift = nshift;
+        st->m = m;
+        st->c = c;
+        __threadfence();
+        st->state = dec;
+    }
+}
+
+// alt[k][row * rank + col] = (Q V_r)(row, col) for a RIGHT_T bond this path
+// finished: Q rows in g.qscr (row-major, pitch c), V_r at the root B slot
+// (row-major CT x KC).  One block per WROWS rows; the writes of a block are
+// one contiguous range.
+constexpr int WROWS = 16;
+__global__ void __launch_bounds__(NT) k_gq_write(const DevDesc* D, int k, Plan pl, GQ g, double* ws) {
+    PTT_PDL_ENTRY();
+    __shared__ double sB[CB * (CB + 1)];
+    __shared__ double sQ[WROWS * (CB + 1)];
+    if (!finished(ldcg((const int*)g.rec))) return;
+    const Info* info = pl.info;
+    if (info->status) return;
+    const int m = info->m, c = info->c, rank = info->rank;
+    const int tid = threadIdx.x;
+    const double* Bn = ws + pl.o_Bn;
+    for (int e = tid; e < CB * CB; e += NT) {
+        const int t = e / CB, l = e - (e / CB) * CB;
+        sB[t * (CB + 1) + l] = (t < c && l < rank) ? Bn[(long long)t * pl.KC + l] : 0.0;
+    }
+    double* out = D->alt[k];
+    for (int r0 = blockIdx.x * WROWS; r0 < m; r0 += gridDim.x * WROWS) {
+        const int h = (m - r0) < WROWS ? (m - r0) : WROWS;
+        __syncthreads();
+        for (int e = tid; e < WROWS * CB; e += NT) {
+            const int row = e / CB, t = e - (e / CB) * CB;
+            sQ[row * (CB + 1) + t] = (row < h && t < c) ? g.qscr[(long long)(r0 + row) * c + t] : 0.0;
+        }
+        __syncthreads();
+        for (int e = tid; e < h * rank; e += NT) {
+            const int row = e / rank, col = e - (e / rank) * rank;
+            double y0 = 0.0, y1 = 0.0;
+#pragma unroll 8
+            for (int t = 0; t < CB; t += 2) {
+                y0 = fma(sQ[row * (CB + 1) + t], sB[t * (CB + 1) + col], y0);
+                y1 = fma(sQ[row * (CB + 1) + t + 1], sB[(t + 1) * (CB + 1) + col], y1);
+            }
+            out[(long long)r0 * rank + e] = y0 + y1;
+        }
+    }
+}
+
+}  // namespace gq

@@ -101,6 +101,8 @@ __device__ void replay_geqrt(double* Rp, const double* Vb, const double* taus, i
 
 template <int CT>
 __global__ void __launch_bounds__(NT) k_apply_node(Plan pl, double* ws, int first, const int* kptr) {
+    PTT_PDL_ENTRY();
+    if (gq_finished(pl)) return;
     extern __shared__ double sm[];
     constexpr int S = CT + 1;
     double* Rp = sm;             // CT x KG
@@ -165,6 +167,8 @@ __global__ void __launch_bounds__(NT) k_apply_node(Plan pl, double* ws, int firs
 template <int CT>
 __global__ void __launch_bounds__(NT) k_apply_leaf(const DevDesc* D, int kcore, int mode, Plan pl, double* ws,
                                                    const int* kptr) {
+    PTT_PDL_ENTRY();
+    if (gq_finished(pl)) return;
     extern __shared__ double sm[];
     constexpr int S = CT + 1;
     constexpr int VR = CT > H ? CT : H;
@@ -231,7 +235,8 @@ __global__ void __launch_bounds__(NT) k_apply_leaf(const DevDesc* D, int kcore, 
 
 // B = I_q at the root, zero-padded to CT x KC.
 __global__ void k_set_identity(Plan pl, double* ws) {
-    if (pl.info->status) return;
+    PTT_PDL_ENTRY();
+    if (pl.info->status || gq_finished(pl)) return;
     const int CT = pl.CT, KC = pl.KC;
     const int q = pl.info->q;
     double* B = ws + pl.o_Bn;
@@ -265,7 +270,12 @@ __host__ __device__ constexpr int svd_nt() {
 // rotation chain and not the block barrier being the cost.)  Column norms
 // are tracked through the rotations (a_p' = a_p - t a_pq ...) and recomputed
 // at the start of a sweep.
-template <int CT, int NTH = svd_nt<CT>(), int LP = 8>
+//
+// With VACC (CT <= 64) the rotations are also applied to V, kept column by
+// column in shared memory beside L, and V_r is written at the end: no
+// rotation log and no replay launch.  Each pair's positions in the circle
+// order advance by one per round (no division on the chain).
+template <int CT, int NTH = svd_nt<CT>(), int LP = 8, bool VACC = false>
 __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double delta, int maxr, int bond,
                                                     int* status) {
     PTT_PDL_ENTRY();
@@ -274,6 +284,7 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
     constexpr int S = CT + 1;
     constexpr int NG = CT / LP;
     double* Lc = sm;                   // (CT+1) columns x S
+    double* Vc = sm + (CT + 2) * S;    // VACC: (CT+1) columns of V x S
     __shared__ double s_nrm[CT + 2];
     __shared__ double s_sig[CT + 2];
     __shared__ int s_ord[CT + 2];
@@ -290,6 +301,7 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
     for (int e = tid; e < qq * S; e += SVD_NT) {
         const int j = e / S, t = e - (e / S) * S;
         Lc[e] = (j < q && t < c) ? R[(long long)j * CT + t] : 0.0;
+        if (VACC) Vc[e] = (j == t) ? 1.0 : 0.0;
     }
     __syncthreads();
     double2* rot = (double2*)(ws + pl.o_rot);
@@ -325,9 +337,21 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
         __syncthreads();
         const double thr2 = s_thr2;
         int myrot = 0;
+        // circle positions of this group's pair (one pair per group when
+        // qq / 2 <= SVD_NT / LP, the case of every VACC launch): advanced
+        // by one per round
+        int tp = grp == 0 ? 0 : (grp - 1) % (qq - 1 > 0 ? qq - 1 : 1);
+        int tq = (qq - 2 - grp) >= 0 ? (qq - 2 - grp) % (qq - 1 > 0 ? qq - 1 : 1) : 0;
         for (int rd = 0; rd < qq - 1; rd++) {
             for (int i = grp; i < qq / 2; i += SVD_NT / LP) {
-                const int pc = circle_col(i, rd, qq), qc = circle_col(qq - 1 - i, rd, qq);
+                int pc, qc;
+                if (VACC) {
+                    pc = i == 0 ? 0 : 1 + tp;
+                    qc = 1 + tq;
+                } else {
+                    pc = circle_col(i, rd, qq);
+                    qc = circle_col(qq - 1 - i, rd, qq);
+                }
                 double* ap = Lc + pc * S;
                 double* aq = Lc + qc * S;
                 double xa[NG], xb[NG];
@@ -363,6 +387,16 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
                         ap[p + LP * v] = cs * xa[v] - sn * xb[v];
                         aq[p + LP * v] = sn * xa[v] + cs * xb[v];
                     }
+                    if (VACC) {  // the same rotation of V's columns (off the chain)
+                        double* vp = Vc + pc * S;
+                        double* vq = Vc + qc * S;
+#pragma unroll
+                        for (int v = 0; v < NG; v++) {
+                            const double ya = vp[p + LP * v], yb = vq[p + LP * v];
+                            vp[p + LP * v] = cs * ya - sn * yb;
+                            vq[p + LP * v] = sn * ya + cs * yb;
+                        }
+                    }
                     if (p == 0) {
                         s_nrm[pc] = al - t * ga;
                         s_nrm[qc] = be + t * ga;
@@ -370,7 +404,11 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
                     // bit 1: a rotation of a pair whose cosine exceeded 1e-8
                     myrot |= (ga * ga > 1e-16 * (al * be)) ? 3 : 1;
                 }
-                if (p == 0) rot[((long long)sw * (CT + 1) + rd) * npair + i] = make_double2(cs, sn);
+                if (!VACC && p == 0) rot[((long long)sw * (CT + 1) + rd) * npair + i] = make_double2(cs, sn);
+            }
+            if (VACC) {
+                tp = (tp + 1 == qq - 1) ? 0 : tp + 1;
+                tq = (tq + 1 == qq - 1) ? 0 : tq + 1;
             }
             __syncthreads();
         }
@@ -467,6 +505,14 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
         const int b = e / CT, t = e - (e / CT) * CT;
         US[e] = (b < rank && t < c) ? Lc[s_ord[b] * S + t] : 0.0;
     }
+    if (VACC) {  // V_r = V[:, order[0:rank]] into Bn[root] (row-major CT x KC)
+        double* B = ws + pl.o_Bn;
+        const int KC = pl.KC;
+        for (int e = tid; e < CT * KC; e += SVD_NT) {
+            const int row = e / KC, b = e - (e / KC) * KC;
+            B[e] = (row < q && b < rank) ? Vc[s_ord[b] * S + row] : 0.0;
+        }
+    }
 }
 
 // Rebuild rows of V (q x q, V = product of the recorded rotations) and write
@@ -514,6 +560,7 @@ __device__ void svd_replay_body(const Plan& pl, double* ws, const Info* info, in
 }
 
 __global__ void __launch_bounds__(256) k_svd_replay(Plan pl, double* ws) {
+    PTT_PDL_ENTRY();
     svd_replay_body(pl, ws, pl.info, blockIdx.x);
 }
 
@@ -629,6 +676,10 @@ __global__ void k_bond_finalize(DevDesc* D, int kq, int ka, int kb, const int* v
     }
 }
 
+#include "ptt_wtsqr.cuh"
+#include "ptt_cholqr.cuh"
+#include "ptt_gridqr.cuh"
+
 // ---------------------------------------------------------------------------
 // host planning
 // ---------------------------------------------------------------------------
@@ -643,12 +694,16 @@ struct Layout {
     long long bytes;
 };
 
-static void plan_bond(int CT, long long mcap, int KC, Plan* pl) {
+// pmax bounds the leaves (and so the tree levels, one apply launch each):
+// the Householder TSQR behind the grid Cholesky QR only runs for a bond that
+// falls back, so there it takes few, long leaves and its skipped launches
+// stay few.
+static void plan_bond(int CT, long long mcap, int KC, Plan* pl, int pmax = 512) {
     int L = 2 * CT;
     if (L < 128) L = 128;
     L = (L + H - 1) / H * H;
     long long P = (mcap + L - 1) / L;
-    while (P > 512) {
+    while (P > pmax) {
         L *= 2;
         P = (mcap + L - 1) / L;
     }
@@ -658,6 +713,7 @@ static void plan_bond(int CT, long long mcap, int KC, Plan* pl) {
     pl->KL = 1 + (2 * L - 1 + H - 1) / H;
     pl->NH = (CT + H - 1) / H;
     pl->KC = KC;
+    pl->gqstate = nullptr;
 }
 
 static long long carve(Plan* pl, int PMAX, int LMAXKL) {
@@ -694,6 +750,11 @@ template <int CT>
 static size_t svd_smem() {
     return sizeof(double) * (size_t)(CT + 2) * (CT + 1);
 }
+// the same with V kept in shared memory beside L (k_svd_jacobi VACC)
+template <int CT>
+static size_t svd_smem_v() {
+    return 2 * svd_smem<CT>();
+}
 // 8 V rows + one sweep's rotation table ((CT+1) rounds x (CT+2)/2 pairs)
 template <int CT>
 static size_t replay_smem() {
@@ -713,17 +774,34 @@ static int set_attrs() {
                                   (int)apply_smem<CT>()));
     PTT_CUDA(cudaFuncSetAttribute(k_svd_jacobi<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)svd_smem<CT>()));
+    if (CT <= 64)
+        PTT_CUDA(cudaFuncSetAttribute(k_svd_jacobi<CT, svd_nt<CT>(), 8, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)svd_smem_v<CT>()));
     PTT_CUDA(cudaFuncSetAttribute(k_svd_replay, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)replay_smem<128>()));
+    PTT_CUDA(cudaFuncSetAttribute(gq::k_gq_stage, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gq::SMEM));
     done.fetch_or(bit);
     return PTT_OK;
 }
 
-// Factor the unfolding (mode) of core k; R lands at the root slot.
+// Factor the unfolding (mode) of core k; R lands at the root slot.  With the
+// grid Cholesky QR (g != null) its stage launches go first and the Householder
+// TSQR only factors a bond they did not finish.
 template <int CT>
-static int launch_factor(ptt_ctx* c, ptt_tt* x, int k, int mode, Plan& pl, double* ws) {
+static int launch_factor(ptt_ctx* c, ptt_tt* x, int k, int mode, Plan& pl, double* ws, gq::GQ* g, long long mcap) {
     ptt_time_begin(c, PTT_TIME_TSQR);
-    k_tsqr_factor<CT><<<pl.P, NT, factor_smem<CT>(), c->stream>>>(x->dd, k, mode, pl, ws, c->d_status);
+    if (g) {
+        g->rpb = gq::rows_per_cta(mcap, c->nsm);
+        const int nb = gq::ctas(mcap, g->rpb);
+        pl.gqstate = (const int*)g->rec;
+        for (int s = 0; s < gq::MAXST; s++) {
+            PTT_CUDA(ptt_launch(c, gq::k_gq_stage, dim3(nb), dim3(gq::NT), gq::SMEM, (const DevDesc*)x->dd, k, mode, pl,
+                                *g, ws, s, c->d_qrstat));
+            PTT_LAUNCHED(c);
+        }
+    }
+    PTT_CUDA(ptt_launch(c, k_tsqr_factor<CT>, dim3(pl.P), dim3(NT), factor_smem<CT>(), (const DevDesc*)x->dd, k, mode,
+                        pl, ws, c->d_status));
     ptt_time_end(c, PTT_TIME_TSQR);
     PTT_LAUNCHED(c);
     return PTT_OK;
@@ -735,12 +813,13 @@ static int launch_apply(ptt_ctx* c, ptt_tt* x, int k, int mode, Plan& pl, double
     const int kgroups = (kcap + KG - 1) / KG;
     int first = 0, cnt = 1;
     while (first + cnt <= pl.P - 1) {  // internal levels: nodes [first, first+cnt)
-        k_apply_node<CT><<<dim3(cnt, kgroups), NT, apply_smem<CT>(), c->stream>>>(pl, ws, first, kptr);
+        PTT_CUDA(ptt_launch(c, k_apply_node<CT>, dim3(cnt, kgroups), dim3(NT), apply_smem<CT>(), pl, ws, first, kptr));
         PTT_LAUNCHED(c);
         first += cnt;
         cnt *= 2;
     }
-    k_apply_leaf<CT><<<dim3(pl.P, kgroups), NT, apply_smem<CT>(), c->stream>>>(x->dd, k, mode, pl, ws, kptr);
+    PTT_CUDA(ptt_launch(c, k_apply_leaf<CT>, dim3(pl.P, kgroups), dim3(NT), apply_smem<CT>(), (const DevDesc*)x->dd, k,
+                        mode, pl, ws, kptr));
     PTT_LAUNCHED(c);
     return PTT_OK;
 }
@@ -749,40 +828,65 @@ static int launch_apply(ptt_ctx* c, ptt_tt* x, int k, int mode, Plan& pl, double
 // 4 = QR of the single core `only` (left unfolding; core <- Q, r_{only+1} <- q).
 // rk[k]: upper bound of rank k for the whole call (the capacity, or the
 // actual ranks when they were read back; ranks only shrink while rounding).
+// At CT = 64 every factorisation first runs the grid Cholesky QR
+// (ptt_gridqr.cuh) unless the context is set to Householder only.
 template <int CT>
 static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, int phases, int only) {
     ptt_ctx* c = x->ctx;
     const int d = x->d;
     int rc = set_attrs<CT>();
     if (rc) return rc;
+    const bool use_gq = (CT == gq::CB) && !c->no_cholqr;
     // plan: largest leaf count over all bonds decides the workspace
     const int KC = (CT + KG - 1) / KG * KG;
-    int PMAX = 1, KLMAX = 1;
+    int PMAX = 1, KLMAX = 1, NBMAX = 1;
+    long long MQMAX = 1;
+    const int pmax = use_gq ? 8 : 512;
     for (int i = 0; i < d; i++) {
         Plan t;
         long long ml = (long long)rk[i] * x->n[i], mr = (long long)x->n[i] * rk[i + 1];
-        plan_bond(CT, ml > mr ? ml : mr, KC, &t);
+        plan_bond(CT, ml > mr ? ml : mr, KC, &t, pmax);
         if (t.P > PMAX) PMAX = t.P;
         if (t.KL > KLMAX) KLMAX = t.KL;
+        for (long long mm : {ml, mr}) {
+            const int nb = gq::ctas(mm, gq::rows_per_cta(mm, c->nsm));
+            NBMAX = nb > NBMAX ? nb : NBMAX;
+        }
+        MQMAX = mr > MQMAX ? mr : MQMAX;
     }
     Plan base;
     plan_bond(CT, 1, KC, &base);
     base.NH = (CT + H - 1) / H;
     long long total = carve(&base, PMAX, KLMAX);
-    size_t bytes = (size_t)total * sizeof(double) + 256;
+    // grid Cholesky QR: record, partial Gram matrices, Q rows of RIGHT_T bonds
+    const int NGMAX = (NBMAX + gq::GROUP - 1) / gq::GROUP;
+    long long o_gq = (total + 31) / 32 * 32, gq_len = 0;
+    if (use_gq) gq_len = gq::REC + (long long)(NBMAX + NGMAX) * gq::UP + MQMAX * gq::CB + 64;
+    size_t bytes = (size_t)(o_gq + gq_len) * sizeof(double) + 256;
     if ((rc = ptt_ws_reserve(c, bytes))) return rc;
-    if ((rc = ptt_counters_reserve(c, (size_t)PMAX * 4 + 64))) return rc;
+    const size_t cnt_tree = (size_t)PMAX * 4 + 64;
+    if ((rc = ptt_counters_reserve(c, cnt_tree + NGMAX + 2))) return rc;
     double* ws = (double*)c->ws;
     // ints live after the doubles: qn [2P-1], pass [P], Info
     // Tree counters live alone in ctx->d_counters (zero between launches,
     // reset by the combining block); node ranks and pass flags in ws.
     int* ints = (int*)(ws + base.o_nodes);
     Info* info = (Info*)(ws + base.o_info_d);
+    gq::GQ gqs{};
+    gq::GQ* g = nullptr;
+    if (use_gq) {
+        gqs.rec = ws + o_gq;
+        gqs.part = gqs.rec + (gq::REC + 31) / 32 * 32;
+        gqs.gpart = gqs.part + (long long)NBMAX * gq::UP;
+        gqs.qscr = gqs.gpart + (long long)NGMAX * gq::UP;
+        gqs.cnt = c->d_counters + cnt_tree;
+        g = &gqs;
+    }
 
     auto mkplan = [&](long long mcap) {
         Plan pl = base;
         Plan t;
-        plan_bond(CT, mcap, KC, &t);
+        plan_bond(CT, mcap, KC, &t, pmax);
         pl.L = t.L;
         pl.P = t.P;
         pl.KL = KLMAX;
@@ -794,62 +898,81 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
         pl.work = (c->tkind == PTT_TIME_TSQR) ? c->d_work + PTT_TIME_TSQR : nullptr;
         return pl;
     };
+    const DevDesc* dd = x->dd;
 
     if (phases & 4) {
         const int i = only;
-        Plan pl = mkplan((long long)rk[i] * x->n[i]);
-        if ((rc = launch_factor<CT>(c, x, i, LEFT, pl, ws))) return rc;
-        k_set_identity<<<32, 256, 0, c->stream>>>(pl, ws);
+        const long long mcap = (long long)rk[i] * x->n[i];
+        Plan pl = mkplan(mcap);
+        if ((rc = launch_factor<CT>(c, x, i, LEFT, pl, ws, g, mcap))) return rc;
+        PTT_CUDA(ptt_launch(c, k_set_identity, dim3(32), dim3(256), 0, pl, ws));
         PTT_LAUNCHED(c);
         if ((rc = launch_apply<CT>(c, x, i, LEFT, pl, ws, &info->q, CT))) return rc;
-        k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i, -1, &info->q, info);
+        PTT_CUDA(ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i + 1, i, -1, (const int*)&info->q,
+                            (const Info*)info));
         PTT_LAUNCHED(c);
         return PTT_OK;
     }
     // left-to-right orthogonalisation
     for (int i = 0; i < d - 1 && (phases & 1); i++) {
-        Plan pl = mkplan((long long)rk[i] * x->n[i]);
-        if ((rc = launch_factor<CT>(c, x, i, LEFT, pl, ws))) return rc;
+        const long long mcap = (long long)rk[i] * x->n[i];
+        Plan pl = mkplan(mcap);
+        if ((rc = launch_factor<CT>(c, x, i, LEFT, pl, ws, g, mcap))) return rc;
         {
             const long long ncap = (long long)x->n[i + 1] * rk[i + 2];
             int gy = (int)((ncap + GT - 1) / GT);
             if (gy > 4096) gy = 4096;
-            k_gemm_rx<<<dim3((CT + GT - 1) / GT, gy), 256, 0, c->stream>>>(x->dd, i + 1, pl, ws);
+            PTT_CUDA(ptt_launch(c, k_gemm_rx, dim3((CT + GT - 1) / GT, gy), dim3(256), 0, dd, i + 1, pl, ws));
             PTT_LAUNCHED(c);
         }
-        k_set_identity<<<32, 256, 0, c->stream>>>(pl, ws);
+        PTT_CUDA(ptt_launch(c, k_set_identity, dim3(32), dim3(256), 0, pl, ws));
         PTT_LAUNCHED(c);
         if ((rc = launch_apply<CT>(c, x, i, LEFT, pl, ws, &info->q, CT))) return rc;
-        k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i + 1, i, i + 1, &info->q, info);
+        PTT_CUDA(ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i + 1, i, i + 1, (const int*)&info->q,
+                            (const Info*)info));
         PTT_LAUNCHED(c);
     }
     // right-to-left truncation
     for (int i = d - 1; i >= 1 && (phases & 2); i--) {
-        Plan pl = mkplan((long long)x->n[i] * rk[i + 1]);
-        if ((rc = launch_factor<CT>(c, x, i, RIGHT_T, pl, ws))) return rc;
+        const long long mcap = (long long)x->n[i] * rk[i + 1];
+        Plan pl = mkplan(mcap);
+        if ((rc = launch_factor<CT>(c, x, i, RIGHT_T, pl, ws, g, mcap))) return rc;
         const int mr = maxr ? maxr[i] : rk[i];
         ptt_time_begin(c, PTT_TIME_SVD);
-        k_svd_jacobi<CT><<<1, svd_nt<CT>(), svd_smem<CT>(), c->stream>>>(pl, ws, delta, mr, i, c->d_status);
-        ptt_time_end(c, PTT_TIME_SVD);
-        PTT_LAUNCHED(c);
-        k_svd_replay<<<(CT + 7) / 8, 256, replay_smem<CT>(), c->stream>>>(pl, ws);
-        PTT_LAUNCHED(c);
-        if ((rc = launch_apply<CT>(c, x, i, RIGHT_T, pl, ws, &info->rank, CT))) return rc;
-        {
-            const long long mcap = (long long)rk[i - 1] * x->n[i - 1];
-            int gx = (int)((mcap + GT - 1) / GT);
-            if (gx > 4096) gx = 4096;
-            k_gemm_xm<<<dim3(gx, (CT + GT - 1) / GT), 256, 0, c->stream>>>(x->dd, i - 1, pl, ws);
+        if (CT <= 64) {  // V accumulated in shared memory: V_r written by the SVD itself
+            PTT_CUDA(ptt_launch(c, k_svd_jacobi<CT, svd_nt<CT>(), 8, true>, dim3(1), dim3(svd_nt<CT>()),
+                                svd_smem_v<CT>(), pl, ws, delta, mr, i, c->d_status));
+            ptt_time_end(c, PTT_TIME_SVD);
+            PTT_LAUNCHED(c);
+        } else {
+            PTT_CUDA(ptt_launch(c, k_svd_jacobi<CT>, dim3(1), dim3(svd_nt<CT>()), svd_smem<CT>(), pl, ws, delta, mr,
+                                i, c->d_status));
+            ptt_time_end(c, PTT_TIME_SVD);
+            PTT_LAUNCHED(c);
+            PTT_CUDA(ptt_launch(c, k_svd_replay, dim3((CT + 7) / 8), dim3(256), replay_smem<CT>(), pl, ws));
             PTT_LAUNCHED(c);
         }
-        k_bond_finalize<<<1, 32, 0, c->stream>>>(x->dd, i, i, i - 1, &info->rank, info);
+        if ((rc = launch_apply<CT>(c, x, i, RIGHT_T, pl, ws, &info->rank, CT))) return rc;
+        if (g) {  // Q V_r for a bond the grid Cholesky QR finished
+            int gx = (int)((mcap + gq::WROWS - 1) / gq::WROWS);
+            gx = gx < 1 ? 1 : (gx > 2 * c->nsm ? 2 * c->nsm : gx);
+            PTT_CUDA(ptt_launch(c, gq::k_gq_write, dim3(gx), dim3(gq::NT), 0, dd, i, pl, *g, ws));
+            PTT_LAUNCHED(c);
+        }
+        {
+            const long long mcap2 = (long long)rk[i - 1] * x->n[i - 1];
+            int gx = (int)((mcap2 + GT - 1) / GT);
+            if (gx > 4096) gx = 4096;
+            PTT_CUDA(ptt_launch(c, k_gemm_xm, dim3(gx, (CT + GT - 1) / GT), dim3(256), 0, dd, i - 1, pl, ws));
+            PTT_LAUNCHED(c);
+        }
+        PTT_CUDA(ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i, i, i - 1, (const int*)&info->rank,
+                            (const Info*)info));
         PTT_LAUNCHED(c);
     }
     return PTT_OK;
 }
 
-#include "ptt_wtsqr.cuh"
-#include "ptt_cholqr.cuh"
 
 // Rounding of a train whose ranks stay <= 32 on the warp-level TSQR.
 // Per bond only the factorisation, the small product that moves R (or U S)

@@ -82,7 +82,18 @@ struct Plan {
     Info* info;       // device
     double* stats;    // device, per-bond records of the rounding (may be null)
     double* work;     // device accumulator of algorithmic bytes (may be null)
+    const int* gqstate;  // device state of the grid Cholesky QR of this bond (null: not used);
+                         // the Householder kernels skip a bond it finished
 };
+
+// The grid Cholesky QR (ptt_gridqr.cuh) finished this bond: its state word
+// is DONE (1) or FINISH (4).  Read from L2: it was written by an earlier
+// launch of the same stream.
+__device__ __forceinline__ bool gq_finished(const Plan& pl) {
+    if (!pl.gqstate) return false;
+    const int s = __ldcg(pl.gqstate);
+    return s == 1 || s == 4;
+}
 
 // Leaf row range (identical on host and device).  The non-empty leaves are
 // 0..Peff-1; the last one absorbs the tail so every non-empty leaf has at

@@ -49,6 +49,15 @@ class Replicas:
         self._td.all_reduce(t, op=self._td.ReduceOp.MAX)
         return float(t.item())
 
+    def gather(self, obj):
+        """Every rank's `obj` in rank order (on every rank; a picklable value).
+        Used to collect per-instance results (ranks, errors) on rank 0."""
+        if not self._td:
+            return [obj]
+        out = [None] * self.world
+        self._td.all_gather_object(out, obj)
+        return out
+
     def job_rate(self, units_per_rank: float, seconds_per_rank: float) -> float:
         """Whole-job throughput: the units all ranks processed over the
         slowest rank's time."""

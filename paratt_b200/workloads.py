@@ -81,20 +81,48 @@ def batch_shapes(count=64, seed=4):
     return out
 
 
-def batch_trains(ctx, count=64, seed=4):
+def rounding_cost(shape):
+    """Work of one rounding of a train of this (d, n, r, cap) shape, in
+    proportion to its flops: sum_k r_k n r_{k+1} max(r_k, r_{k+1}) (every
+    bond's QR, and the products around it, scale with the unfolding's size
+    times its column count)."""
+    d, n, r, _ = shape
+    return float(sum(r[k] * n * r[k + 1] * max(r[k], r[k + 1]) for k in range(d)))
+
+
+def shard_by_cost(costs, world):
+    """Split independent instances over `world` ranks so that the largest
+    per-rank total is small: longest first, each to the least loaded rank
+    (ties to the lower rank).  Deterministic, so every rank computes the same
+    split without communicating.  Returns one list of indices per rank."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    out = [[] for _ in range(world)]
+    for i in order:
+        w = min(range(world), key=lambda k: (load[k], k))
+        out[w].append(i)
+        load[w] += costs[i]
+    return [sorted(o) for o in out]
+
+
+def batch_trains(ctx, count=64, seed=4, only=None):
     """The batched-rounding workload as device trains: left-orthonormal
     random cores (QR of a Gaussian matrix) whose bond column j is scaled by
-    2^-j, so every bond's spectrum decays as 2^-j.  Generated on the GPU
-    with torch (input preparation only).  Returns [(TT, shape)]."""
+    2^-j, so every bond's spectrum decays as 2^-j.  Train i is generated
+    from its own seed (seed * 1000 + i), so any subset (`only`: indices) is
+    the same trains on any rank.  Generated on the GPU with torch (input
+    preparation only).  Returns [(TT, shape)] in index order."""
     import torch
 
     from . import TT
 
     dev = torch.device("cuda", ctx.device)
     g = torch.Generator(device=dev)
-    g.manual_seed(seed)
     trains = []
-    for d, n, r, cap in batch_shapes(count, seed):
+    for idx, (d, n, r, cap) in enumerate(batch_shapes(count, seed)):
+        if only is not None and idx not in only:
+            continue
+        g.manual_seed(seed * 1000 + idx)
         T = TT(ctx, [n] * d, r)
         cores = []
         for k in range(d):

@@ -196,3 +196,40 @@ def test_autotune(ctx):
     X.close()
     assert O.ranks_of(after) == O.ranks_of(before)
     assert O.rel_diff_exact(after, before) <= 1e-12
+
+
+@pytest.mark.parametrize("decay", [1e-3, 1e-9, 1e-14, 0.0])
+def test_grid_cholqr_matches_householder(ctx, decay):
+    """33 to 64 columns: the grid Cholesky QR (rows spread over all SMs, one
+    launch per Gram stage) against the Householder TSQR and the oracle, for
+    well separated, graded, near-singular and exactly rank-deficient
+    unfoldings; the Cholesky path is the one that ran."""
+    dims = [9, 16, 7, 12, 8]
+    if decay == 0.0:
+        full, keep = [1, 7, 30, 28, 20, 1], [1, 5, 12, 10, 6, 1]
+    else:
+        full, keep = [1, 9, 48, 60, 40, 1], [1, 5, 20, 24, 7, 1]
+    x = gapped_tt(dims, full, 23, keep, decay=decay)
+    if decay == 0.0:
+        x = O.axpby(1.0, x, 0.5, x)  # repeated columns: 40 to 60 per unfolding
+    assert 32 < max(O.ranks_of(x)) <= 64
+    tol = 1e-6 * O.norm(x)
+    got = {}
+    for on in (False, True):
+        ctx.cholqr(on)
+        before = ctx.qr_counts()
+        X = P.TT.from_cores(ctx, x)
+        X.round(tol, 64)
+        got[on] = X.get()
+        X.close()
+        after = ctx.qr_counts()
+        if on:
+            assert after[0] > before[0]
+        else:
+            assert after == before
+    ctx.cholqr(True)
+    ref = O.round_tt(x, tol, 10**6)
+    for on in (False, True):
+        assert O.ranks_of(got[on]) == O.ranks_of(ref)
+        assert O.rel_diff_exact(got[on], ref) <= 1e-12
+    assert O.rel_diff_exact(got[True], got[False]) <= 1e-12

@@ -60,3 +60,52 @@ def test_single_process_needs_no_group():
     assert r.max(4.0) == 4.0
     assert r.job_rate(10, 2.0) == 5.0
     r.close()
+
+
+def _batch_worker(rank, world, port, q):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    from paratt_b200 import workloads as W
+    from paratt_b200.replicas import Replicas
+
+    r = Replicas("gloo", timeout_s=60)
+    shapes = W.batch_shapes(64, 4)
+    shards = W.shard_by_cost([W.rounding_cost(s) for s in shapes], r.world)
+    mine = shards[r.rank]
+    # stand-in for the rounding of this rank's trains: the result of train i
+    # is its index and its rank caps (what the benchmark gathers per train)
+    results = [(i, list(shapes[i][3])) for i in mine]
+    allres = r.gather(results)
+    q.put((rank, shards, allres))
+    r.close()
+
+
+def test_batch_instances_sharded_over_two_ranks():
+    """The batched-rounding workload split over 2 gloo ranks by instance,
+    balanced by rounding cost: the shards are disjoint and cover all 64
+    trains, every rank computes the same split, the heavier shard carries at
+    most 10 % more than half the work, and rank 0 gathers every train's
+    result."""
+    from paratt_b200 import workloads as W
+
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_batch_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=180) for _ in range(world)), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in procs)
+    shards = res[0][1]
+    assert res[1][1] == shards
+    assert sorted(shards[0] + shards[1]) == list(range(64))
+    shapes = W.batch_shapes(64, 4)
+    cost = [W.rounding_cost(s) for s in shapes]
+    loads = [sum(cost[i] for i in sh) for sh in shards]
+    assert max(loads) <= 1.1 * sum(cost) / world
+    gathered = [t for part in res[0][2] for t in part]
+    assert sorted(i for i, _ in gathered) == list(range(64))
+    assert all(caps == list(shapes[i][3]) for i, caps in gathered)
