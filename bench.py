@@ -173,7 +173,9 @@ def autotune(ctx):
     kept), or the reason the tuning failed; the built-in rule stays in force
     then, so a failed tuning never stops the benchmark."""
     try:
-        return ctx.autotune().tolist()
+        table = ctx.autotune().tolist()
+        tm64, fill = ctx.autotune_gemm()
+        return {"cq_cluster_sizes": table, "gemm_tile64_from": tm64, "gemm_splitk_tiles": fill}
     except Exception as e:  # noqa: BLE001 -- reported in the JSON line
         return f"not tuned: {e}"
 
@@ -320,7 +322,7 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": learned_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "method": "learned-sketch (MLP-proposed sketch ranks, pad 4)",
-                   "autotune_cq_cluster_sizes": tuned,
+                   "autotune": tuned,
                    "l2": "flushed before every step (2 x L2 write, outside the events)",
                    "state_rank": max(UL.ranks()), "parallelism": f"replicas x{world}"},
         "plain": {"value": plain_value, "unit": "RK2 steps/s", "ms_per_step": plain_ms / args.steps},
@@ -459,7 +461,7 @@ def run_batch(args, rank, world, local_rank):
         "loop": {"value": 64e3 / tl, "unit": "roundings/s", "ms": tl},
         "batch_over_loop": tl / tb,
         "same_ranks_as_loop": bool(same),
-        "autotune_cq_cluster_sizes": tuned,
+        "autotune": tuned,
     }
     print(json.dumps(out))
     rep.close()
@@ -564,6 +566,73 @@ def run_round(args, rank, world, local_rank):
 
 
 # ---------------------------------------------------------------------------
+# formal kernels at full rank (--workload formal)
+# ---------------------------------------------------------------------------
+def run_formal(args, rank, world, local_rank):
+    """The HBM-bound formal kernels at the benchmark's full rank (d=40, n=256,
+    r=64 trains, outputs of rank 128): axpby, the all-modes stencil operator
+    (op_sum), one single-mode stencil, a Hadamard product of rank-8 trains and
+    a train copy.  Device time by events, L2 flushed before each launch
+    (outside the events); achieved = algorithmic bytes (reads + writes, the
+    zero blocks of formal cores included) / time, against the measured HBM
+    copy bandwidth.  W untimed launches of each, then the median of K."""
+    import paratt_b200 as P
+
+    if rank != 0:
+        return 0
+    d, n, r = args.formal_d, 256, 64
+    ctx = P.Context(local_rank)
+    rng = np.random.default_rng(1)
+    rr = [1] + [r] * (d - 1) + [1]
+    X = P.TT.from_cores(ctx, [rng.standard_normal((rr[k], n, rr[k + 1])) for k in range(d)])
+    Y = P.TT.from_cores(ctx, [rng.standard_normal((rr[k], n, rr[k + 1])) for k in range(d)])
+    cap2 = [1] + [2 * r] * (d - 1) + [1]
+    Z, W = P.TT(ctx, [n] * d, cap2), P.TT(ctx, [n] * d, cap2)
+    r8 = [1] + [8] * (d - 1) + [1]
+    X8 = P.TT.from_cores(ctx, [rng.standard_normal((r8[k], n, r8[k + 1])) for k in range(d)])
+    H = P.TT(ctx, [n] * d, [1] + [64] * (d - 1) + [1])
+    e_in = sum(rr[k] * n * rr[k + 1] for k in range(d))
+    e_out = sum(cap2[k] * n * cap2[k + 1] for k in range(d))
+    e8 = sum(r8[k] * n * r8[k + 1] for k in range(d))
+    sten = [0.3, -0.6, 0.3]
+    cases = [
+        ("k_axpby", lambda: P.axpby(1.0, X, 2.0, Y, Z), 8.0 * (2 * e_in + e_out)),
+        ("k_opsum", lambda: P.op_sum(X, sten, 1.0, W), 8.0 * (e_in + e_out)),
+        ("k_stencil (mode d/2)", lambda: X.stencil(d // 2, sten), 16.0 * r * n * r),
+        ("k_hadamard (rank 8 x 8)", lambda: P.hadamard(X8, X8, H), 8.0 * (2 * e8 + e_in)),
+        ("k_copy_tt", lambda: Z.copy_from(X), 16.0 * e_in),
+    ]
+    hbm, src = peaks()
+    out = {}
+    for name, fn, nbytes in cases:
+        for _ in range(args.warmup):
+            fn()
+        ts = []
+        for _ in range(args.steps):
+            ctx.flush_l2()
+            ctx.mark(0)
+            fn()
+            ctx.mark(1)
+            ctx.sync()
+            ts.append(ctx.elapsed_ms(0, 1))
+        t = statistics.median(ts)
+        out[name] = {"ms": t, "bytes": nbytes, "GBs": nbytes / (t / 1e3) / 1e9, "frac": nbytes / (t / 1e3) / 1e9 / hbm}
+    line = {
+        "metric": "formal TT kernels at full rank (d=40, n=256, r=64): HBM GB/s", "value": out["k_axpby"]["GBs"],
+        "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic", "peak": hbm, "peak_source": src,
+        "config": {"workload": f"axpby of two rank-64 trains (rank-128 output), all-modes stencil operator, one-mode "
+                               f"stencil, rank-8 Hadamard, copy; d={d}, n=256", "l2": "flushed before each launch"},
+        "kernels": out,
+    }
+    print(json.dumps(line))
+    for t_ in (X, Y, Z, W, X8, H):
+        t_.close()
+    ctx.close()
+    return 0
+
+
+# ---------------------------------------------------------------------------
 # one step for profilers (--one-step plain|learned)
 # ---------------------------------------------------------------------------
 def run_one_step(args, local_rank):
@@ -609,11 +678,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--formal-d", type=int, default=40, help="cores of the trains of --workload formal")
     ap.add_argument("--one-step", choices=["plain", "learned"], default=None,
                     help="profiling aid: W warm-up steps, then one step; prints the launch index to skip to")
-    ap.add_argument("--workload", default="rk2", choices=["rk2", "batch", "round"],
+    ap.add_argument("--workload", default="rk2", choices=["rk2", "batch", "round", "formal"],
                     help="rk2: the headline reaction-Burgers steps; batch: 64 independent roundings; "
-                         "round: one rank-64 -> 32 rounding")
+                         "round: one rank-64 -> 32 rounding; formal: the HBM-bound formal kernels at full rank")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -626,6 +696,8 @@ def main():
         return run_batch(args, rank, world, local_rank)
     if args.workload == "round":
         return run_round(args, rank, world, local_rank)
+    if args.workload == "formal":
+        return run_formal(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 
 

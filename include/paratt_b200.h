@@ -108,6 +108,13 @@ PTT_API int ptt_ctx_pdl(ptt_ctx* ctx, int on);
  * or 0 where the rule is kept (all 0 if not tuned). */
 PTT_API int ptt_ctx_autotune(ptt_ctx* ctx);
 PTT_API int ptt_ctx_autotune_table(const ptt_ctx* ctx, int* out18);
+/* The autotuner also times the sketch contractions: a batch of 48 x 48 x 48
+ * products with 64- or 32-wide tiles, and one 40 x 40 product over K = 8192
+ * split to fill 1, 2 or 4 times the SM count; a setting replaces the built-in
+ * one (64-wide tiles from M, N >= 48; split-K up to 2 x SMs tiles) only when
+ * it timed at least 10 % faster.  out2: [0] the smallest M, N of 64-wide
+ * tiles, [1] the split-K tile target in force. */
+PTT_API int ptt_ctx_autotune_gemm(const ptt_ctx* ctx, int* out2);
 PTT_API int ptt_ctx_qr_counts(ptt_ctx* ctx, long long* out3);
 /* Device memory held by the context's grow-on-demand workspaces (bytes), and
  * cudaMemGetInfo for the context's device (the caller's current device is

@@ -87,6 +87,7 @@ _SIGS = {
     "ptt_checkpoint_wait": (_i, [_p]),
     "ptt_tt_load_folder": (_i, [_p, C.c_char_p]),
     "ptt_ctx_autotune_table": (_i, [_p, C.POINTER(C.c_int)]),
+    "ptt_ctx_autotune_gemm": (_i, [_p, C.POINTER(C.c_int)]),
     "ptt_ctx_qr_counts": (_i, [_p, C.POINTER(C.c_longlong)]),
     "ptt_ctx_workspace_bytes": (_i, [_p, C.POINTER(C.c_ulonglong)]),
     "ptt_cdf_stencil": (_i, [_p, _i, _dp, _i]),
@@ -204,6 +205,12 @@ class Context:
         v = (C.c_int * 18)()
         _check(lib().ptt_ctx_autotune_table(self.h, v))
         return np.array(list(v)).reshape(3, 6)
+
+    def autotune_gemm(self):
+        """(smallest M, N of 64-wide contraction tiles, split-K tile target)."""
+        out = (C.c_int * 2)()
+        _check(lib().ptt_ctx_autotune_gemm(self.h, out))
+        return int(out[0]), int(out[1])
 
     def pdl(self, on=True):
         """Programmatic dependent launch of the rounding chain (default on)."""

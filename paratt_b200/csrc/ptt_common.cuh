@@ -85,6 +85,11 @@ struct ptt_ctx {
     unsigned char cq_cs[3][6];
     int cq_tuned;                 // generation of the table (0 = none)
     int cq_cs_force;              // cluster size while tuning (0 = table/heuristic)
+    // sketch contractions (ptt_sketch.cu): smallest M and N of a 64 x 64
+    // output tile, and the tile count split-K aims at when the tiles alone
+    // cannot fill the device (0 = built-in 48 / 2 x SMs; set by the autotuner)
+    int gemm_tm64;
+    int gemm_fill;
 };
 
 // Per-device one-time set-up (kernel attributes are per device): returns the
@@ -169,6 +174,9 @@ int ptt_ones(ptt_ctx* c, int n);  // make c->d_ones hold at least n ones
 // Device address of ptt_dot_noalloc's fixed scratch array on `device`
 // (looked up once per device; the caller's current device is kept).
 int ptt_dot_scratch_init(int device, double** out);
+// Autotuner of the sketch contractions' tile and split-K choices (sets
+// ctx->gemm_tm64 / gemm_fill; synchronises).
+int ptt_gemm_autotune(ptt_ctx* c);
 
 // Swap core[k] <-> alt[k] for k in [k0, k1).
 int ptt_swap(ptt_tt* t, int k0, int k1);

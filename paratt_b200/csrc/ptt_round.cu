@@ -270,12 +270,7 @@ __host__ __device__ constexpr int svd_nt() {
 // rotation chain and not the block barrier being the cost.)  Column norms
 // are tracked through the rotations (a_p' = a_p - t a_pq ...) and recomputed
 // at the start of a sweep.
-//
-// With VACC (CT <= 64) the rotations are also applied to V, kept column by
-// column in shared memory beside L, and V_r is written at the end: no
-// rotation log and no replay launch.  Each pair's positions in the circle
-// order advance by one per round (no division on the chain).
-template <int CT, int NTH = svd_nt<CT>(), int LP = 8, bool VACC = false>
+template <int CT, int NTH = svd_nt<CT>(), int LP = 8>
 __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double delta, int maxr, int bond,
                                                     int* status) {
     PTT_PDL_ENTRY();
@@ -284,7 +279,6 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
     constexpr int S = CT + 1;
     constexpr int NG = CT / LP;
     double* Lc = sm;                   // (CT+1) columns x S
-    double* Vc = sm + (CT + 2) * S;    // VACC: (CT+1) columns of V x S
     __shared__ double s_nrm[CT + 2];
     __shared__ double s_sig[CT + 2];
     __shared__ int s_ord[CT + 2];
@@ -301,7 +295,6 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
     for (int e = tid; e < qq * S; e += SVD_NT) {
         const int j = e / S, t = e - (e / S) * S;
         Lc[e] = (j < q && t < c) ? R[(long long)j * CT + t] : 0.0;
-        if (VACC) Vc[e] = (j == t) ? 1.0 : 0.0;
     }
     __syncthreads();
     double2* rot = (double2*)(ws + pl.o_rot);
@@ -337,21 +330,9 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
         __syncthreads();
         const double thr2 = s_thr2;
         int myrot = 0;
-        // circle positions of this group's pair (one pair per group when
-        // qq / 2 <= SVD_NT / LP, the case of every VACC launch): advanced
-        // by one per round
-        int tp = grp == 0 ? 0 : (grp - 1) % (qq - 1 > 0 ? qq - 1 : 1);
-        int tq = (qq - 2 - grp) >= 0 ? (qq - 2 - grp) % (qq - 1 > 0 ? qq - 1 : 1) : 0;
         for (int rd = 0; rd < qq - 1; rd++) {
             for (int i = grp; i < qq / 2; i += SVD_NT / LP) {
-                int pc, qc;
-                if (VACC) {
-                    pc = i == 0 ? 0 : 1 + tp;
-                    qc = 1 + tq;
-                } else {
-                    pc = circle_col(i, rd, qq);
-                    qc = circle_col(qq - 1 - i, rd, qq);
-                }
+                const int pc = circle_col(i, rd, qq), qc = circle_col(qq - 1 - i, rd, qq);
                 double* ap = Lc + pc * S;
                 double* aq = Lc + qc * S;
                 double xa[NG], xb[NG];
@@ -387,16 +368,6 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
                         ap[p + LP * v] = cs * xa[v] - sn * xb[v];
                         aq[p + LP * v] = sn * xa[v] + cs * xb[v];
                     }
-                    if (VACC) {  // the same rotation of V's columns (off the chain)
-                        double* vp = Vc + pc * S;
-                        double* vq = Vc + qc * S;
-#pragma unroll
-                        for (int v = 0; v < NG; v++) {
-                            const double ya = vp[p + LP * v], yb = vq[p + LP * v];
-                            vp[p + LP * v] = cs * ya - sn * yb;
-                            vq[p + LP * v] = sn * ya + cs * yb;
-                        }
-                    }
                     if (p == 0) {
                         s_nrm[pc] = al - t * ga;
                         s_nrm[qc] = be + t * ga;
@@ -404,11 +375,7 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
                     // bit 1: a rotation of a pair whose cosine exceeded 1e-8
                     myrot |= (ga * ga > 1e-16 * (al * be)) ? 3 : 1;
                 }
-                if (!VACC && p == 0) rot[((long long)sw * (CT + 1) + rd) * npair + i] = make_double2(cs, sn);
-            }
-            if (VACC) {
-                tp = (tp + 1 == qq - 1) ? 0 : tp + 1;
-                tq = (tq + 1 == qq - 1) ? 0 : tq + 1;
+                if (p == 0) rot[((long long)sw * (CT + 1) + rd) * npair + i] = make_double2(cs, sn);
             }
             __syncthreads();
         }
@@ -505,14 +472,278 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
         const int b = e / CT, t = e - (e / CT) * CT;
         US[e] = (b < rank && t < c) ? Lc[s_ord[b] * S + t] : 0.0;
     }
-    if (VACC) {  // V_r = V[:, order[0:rank]] into Bn[root] (row-major CT x KC)
-        double* B = ws + pl.o_Bn;
-        const int KC = pl.KC;
-        for (int e = tid; e < CT * KC; e += SVD_NT) {
-            const int row = e / KC, b = e - (e / KC) * KC;
-            B[e] = (row < q && b < rank) ? Vc[s_ord[b] * S + row] : 0.0;
+}
+
+// The same one-sided Jacobi with the columns kept in registers.  Group g of
+// LP lanes holds the two columns of pair g (rows p + LP v), and after each
+// round the columns move as the circle order moves them: pair g's top to
+// pair g - 1 (pair 0's top, column 0, stays; pair 1's top goes to pair 0's
+// bottom), pair g's bottom to pair g + 1 (the last pair's bottom becomes its
+// own top) -- warp shuffles between neighbouring groups, shared memory only
+// across warp boundaries (double-buffered, one block barrier per round).  The
+// tracked column norms travel with the columns.  Rotations are logged for
+// k_svd_replay(_b) exactly as by k_svd_jacobi, and after the last sweep the
+// columns are written to shared memory for the same epilogue (order, rank
+// rule, U S, statistics).
+template <int CT>
+__global__ void __launch_bounds__(svd_nt<CT>()) k_svd_ring(Plan pl, double* ws, double delta, int maxr, int bond,
+                                                          int* status) {
+    PTT_PDL_ENTRY();
+    constexpr int SVD_NT = svd_nt<CT>();
+    constexpr int LP = 8;
+    constexpr int NG = CT / LP;            // rows per lane
+    constexpr int NW = SVD_NT / 32;        // warps
+    constexpr int S = CT + 1;
+    extern __shared__ double sm[];
+    double* Lc = sm;                                  // (CT + 2) columns x S, written after the sweeps
+    double* xch = sm + (CT + 2) * S;                  // [2 buffers][NW][2 (top, bottom)][LP lanes][NG + 1]
+    __shared__ double s_nrm[CT + 2];
+    __shared__ double s_sig[CT + 2];
+    __shared__ int s_ord[CT + 2];
+    __shared__ int s_rot;
+    __shared__ double s_wmax[NW];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int grp = tid / LP, p = tid % LP;
+    const unsigned gm = group_mask<LP>(tid);
+    Info* info = pl.info;
+    if (info->status) return;
+    const int c = info->c, q = info->q;
+    const int qq = q + (q & 1);
+    const int G = qq / 2;  // active pairs (one per group)
+    const bool act = grp < G;
+    const double* R = ws + pl.o_Rn;  // root factor, row-major CT x CT; L = R^T: column j = row j of R
+    // round 0: pair g holds columns g (top) and qq - 1 - g (bottom)
+    double top[NG], bot[NG];
+    {
+        const int ct = grp, cb = qq - 1 - grp;
+#pragma unroll
+        for (int v = 0; v < NG; v++) {
+            const int t = p + LP * v;
+            top[v] = (act && ct < q && t < c) ? R[(long long)ct * CT + t] : 0.0;
+            bot[v] = (act && cb < q && cb >= 0 && t < c) ? R[(long long)cb * CT + t] : 0.0;
         }
     }
+    double2* rot = (double2*)(ws + pl.o_rot);
+    const int npair = (CT + 2) / 2;
+    const double tol = (double)(c < 16 ? 16 : c) * 2.220446049250313e-16;
+    const double tol2 = tol * tol;
+    int sweeps = 0, buf = 0;
+    bool conv = (qq < 2);
+    for (int sw = 0; sw < MAXSW && !conv; sw++) {
+        // exact column norms, and the noise threshold from the largest
+        double al = 0.0, be = 0.0;
+#pragma unroll
+        for (int v = 0; v < NG; v++) {
+            al = fma(top[v], top[v], al);
+            be = fma(bot[v], bot[v], be);
+        }
+        al = gsum_g<LP>(al, gm);
+        be = gsum_g<LP>(be, gm);
+        double mx = act ? fmax(al, be) : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) s_wmax[warp] = mx;
+        if (tid == 0) s_rot = 0;
+        __syncthreads();
+        mx = 0.0;
+#pragma unroll
+        for (int w = 0; w < NW; w++) mx = fmax(mx, s_wmax[w]);
+        const double thr2 = (double)q * 1.232595164407831e-32 * mx;  // (sqrt(q) 2^-53)^2 max |a_j|^2
+        int myrot = 0;
+        for (int rd = 0; rd < qq - 1; rd++) {
+            double cs = 1.0, sn = 0.0;
+            if (act) {
+                double g0 = 0.0, g1 = 0.0;
+#pragma unroll
+                for (int v = 0; v < NG; v += 2) {
+                    g0 = fma(top[v], bot[v], g0);
+                    g1 = fma(top[v + 1], bot[v + 1], g1);
+                }
+                const double ga = gsum_g<LP>(g0 + g1, gm);
+                if (ga != 0.0 && al > thr2 && be > thr2 && ga * ga > tol2 * (al * be)) {
+                    const double dd = be - al, g2 = 2.0 * ga;
+                    const double ri = rsqrt(fma(dd, dd, g2 * g2));
+                    const double hc = fma(0.5 * fabs(dd), ri, 0.5);
+                    const double ic = rsqrt(hc);
+                    cs = hc * ic;
+                    sn = 0.5 * copysign(1.0, dd) * g2 * ri * ic;
+                    const double t = sn * ic;
+#pragma unroll
+                    for (int v = 0; v < NG; v++) {
+                        const double xa = top[v], xb = bot[v];
+                        top[v] = cs * xa - sn * xb;
+                        bot[v] = sn * xa + cs * xb;
+                    }
+                    al = al - t * ga;
+                    be = be + t * ga;
+                    myrot |= (ga * ga > 1e-16 * (al * be)) ? 3 : 1;
+                }
+                if (p == 0) rot[((long long)sw * (CT + 1) + rd) * npair + grp] = make_double2(cs, sn);
+            }
+            // move the columns to the next round's pairs
+            double* xb0 = xch + (long long)buf * NW * 2 * LP * (NG + 1);
+            const int gw = lane / LP;  // group within the warp (0 .. 3)
+            if (gw == 0) {             // this warp's first top: to the previous warp's last group
+                double* d = xb0 + ((warp * 2 + 0) * LP + p) * (NG + 1);
+#pragma unroll
+                for (int v = 0; v < NG; v++) d[v] = top[v];
+                d[NG] = al;
+            }
+            if (gw == 3) {  // this warp's last bottom: to the next warp's first group
+                double* d = xb0 + ((warp * 2 + 1) * LP + p) * (NG + 1);
+#pragma unroll
+                for (int v = 0; v < NG; v++) d[v] = bot[v];
+                d[NG] = be;
+            }
+            double rt[NG], rb[NG];
+#pragma unroll
+            for (int v = 0; v < NG; v++) {
+                rt[v] = __shfl_down_sync(0xffffffffu, top[v], LP);  // top of group + 1
+                rb[v] = __shfl_up_sync(0xffffffffu, bot[v], LP);    // bottom of group - 1
+            }
+            double rta = __shfl_down_sync(0xffffffffu, al, LP);
+            double rbb = __shfl_up_sync(0xffffffffu, be, LP);
+            __syncthreads();
+            if (gw == 3 && warp + 1 < NW) {
+                const double* sx = xb0 + (((warp + 1) * 2 + 0) * LP + p) * (NG + 1);
+#pragma unroll
+                for (int v = 0; v < NG; v++) rt[v] = sx[v];
+                rta = sx[NG];
+            }
+            if (gw == 0 && warp > 0) {
+                const double* sx = xb0 + (((warp - 1) * 2 + 1) * LP + p) * (NG + 1);
+#pragma unroll
+                for (int v = 0; v < NG; v++) rb[v] = sx[v];
+                rbb = sx[NG];
+            }
+            buf ^= 1;
+            if (G == 1) {
+                // one pair: both positions are fixed points of the circle order
+            } else if (grp == 0) {  // top fixed, bottom <- top of pair 1
+#pragma unroll
+                for (int v = 0; v < NG; v++) bot[v] = rt[v];
+                be = rta;
+            } else if (grp == G - 1) {  // top <- own bottom, bottom <- bottom of pair G - 2
+#pragma unroll
+                for (int v = 0; v < NG; v++) {
+                    top[v] = bot[v];
+                    bot[v] = rb[v];
+                }
+                al = be;
+                be = rbb;
+            } else if (act) {
+#pragma unroll
+                for (int v = 0; v < NG; v++) {
+                    top[v] = rt[v];
+                    bot[v] = rb[v];
+                }
+                al = rta;
+                be = rbb;
+            }
+        }
+        if (myrot) atomicOr(&s_rot, myrot);
+        __syncthreads();
+        if (s_rot == 0) {
+            conv = true;
+        } else {
+            sweeps = sw + 1;
+            if (!(s_rot & 2)) conv = true;
+        }
+        __syncthreads();  // s_rot is reset at the next sweep's start
+    }
+    if (!conv && tid == 0) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
+    // the columns back to shared memory: after R rounds of a sweep (R = qq - 1
+    // per sweep) the pairs hold circle_col(g, 0) again, i.e. g and qq - 1 - g
+    if (act) {
+#pragma unroll
+        for (int v = 0; v < NG; v++) {
+            Lc[grp * S + p + LP * v] = top[v];
+            Lc[(qq - 1 - grp) * S + p + LP * v] = bot[v];
+        }
+    }
+    __syncthreads();
+    // singular values (column norms) and descending order
+    for (int j = tid / LP; j < qq; j += SVD_NT / LP) {
+        double s2 = 0.0;
+#pragma unroll
+        for (int v = 0; v < NG; v++) {
+            const double x = Lc[j * S + p + LP * v];
+            s2 += x * x;
+        }
+        s2 = gsum_g<LP>(s2, gm);
+        if (p == 0) {
+            const bool nan = !(s2 == s2);
+            if (nan && j < q) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
+            s_sig[j] = (j < q && !nan) ? sqrt(s2) : -1.0;
+        }
+    }
+    __syncthreads();
+    for (int j = tid; j < qq; j += SVD_NT) {
+        const double sj = s_sig[j];
+        int pos = 0;
+        for (int i = 0; i < qq; i++) {
+            const double si = s_sig[i];
+            pos += (si > sj) || (si == sj && i < j);
+        }
+        s_ord[pos] = j;
+    }
+    __syncthreads();
+    double* sig_out = ws + pl.o_sig;
+    if (tid == 0) {
+        const double s0 = q > 0 ? s_sig[s_ord[0]] : 0.0;
+        const double thr = sqrt((double)q) * 1.1102230246251565e-16 * s0;
+        int nsv = q > 0 ? 1 : 0;
+        while (nsv < q && s_sig[s_ord[nsv]] >= thr) nsv++;
+        if (!(s0 == s0)) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
+        double ssum = 0.0;
+        int rank = nsv;
+        for (int j = nsv - 1; j >= 0; j--) {
+            const double sj = s_sig[s_ord[j]];
+            ssum += sj * sj;
+            if (sqrt(ssum) < delta)
+                rank = j;
+            else
+                break;
+        }
+        if (rank > q) rank = q;
+        if (rank > maxr) rank = maxr;
+        if (rank < 1) rank = 1;
+        info->rank = rank;
+        info->nsv = nsv;
+        info->sweeps = sweeps;
+        double tail = 0.0;
+        for (int j = rank; j < q; j++) tail += s_sig[s_ord[j]] * s_sig[s_ord[j]];
+        info->tail = tail;
+        if (pl.stats) {
+            double* st = pl.stats + (long long)bond * PTT_STAT_LEN;
+            st[0] = rank;
+            st[1] = nsv;
+            st[2] = sweeps;
+            st[3] = q;
+            st[4] = c;
+            st[5] = tail;
+            st[6] = delta;
+            st[7] = 0.0;
+            for (int j = 0; j < PTT_STAT_NSIG; j++) st[8 + j] = j < q ? s_sig[s_ord[j]] : 0.0;
+        }
+    }
+    for (int j = tid; j < CT; j += SVD_NT) {
+        sig_out[j] = j < q ? s_sig[s_ord[j]] : 0.0;
+        ((int*)(sig_out + CT))[j] = j < qq ? s_ord[j] : 0;
+    }
+    __syncthreads();
+    const int rank = info->rank;
+    double* US = ws + pl.o_US;  // c x rank, column-major ld CT
+    for (int e = tid; e < CT * CT; e += SVD_NT) {
+        const int b = e / CT, t = e - (e / CT) * CT;
+        US[e] = (b < rank && t < c) ? Lc[s_ord[b] * S + t] : 0.0;
+    }
+}
+
+template <int CT>
+static size_t ring_smem() {
+    constexpr int NW = svd_nt<CT>() / 32;
+    return sizeof(double) * ((size_t)(CT + 2) * (CT + 1) + 2ull * NW * 2 * 8 * (CT / 8 + 1));
 }
 
 // Rebuild rows of V (q x q, V = product of the recorded rotations) and write
@@ -750,11 +981,7 @@ template <int CT>
 static size_t svd_smem() {
     return sizeof(double) * (size_t)(CT + 2) * (CT + 1);
 }
-// the same with V kept in shared memory beside L (k_svd_jacobi VACC)
-template <int CT>
-static size_t svd_smem_v() {
-    return 2 * svd_smem<CT>();
-}
+
 // 8 V rows + one sweep's rotation table ((CT+1) rounds x (CT+2)/2 pairs)
 template <int CT>
 static size_t replay_smem() {
@@ -775,8 +1002,8 @@ static int set_attrs() {
     PTT_CUDA(cudaFuncSetAttribute(k_svd_jacobi<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)svd_smem<CT>()));
     if (CT <= 64)
-        PTT_CUDA(cudaFuncSetAttribute(k_svd_jacobi<CT, svd_nt<CT>(), 8, true>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)svd_smem_v<CT>()));
+        PTT_CUDA(cudaFuncSetAttribute(k_svd_ring<CT <= 64 ? CT : 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)ring_smem<CT <= 64 ? CT : 64>()));
     PTT_CUDA(cudaFuncSetAttribute(k_svd_replay, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)replay_smem<128>()));
     PTT_CUDA(cudaFuncSetAttribute(gq::k_gq_stage, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gq::SMEM));
@@ -939,19 +1166,16 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
         if ((rc = launch_factor<CT>(c, x, i, RIGHT_T, pl, ws, g, mcap))) return rc;
         const int mr = maxr ? maxr[i] : rk[i];
         ptt_time_begin(c, PTT_TIME_SVD);
-        if (CT <= 64) {  // V accumulated in shared memory: V_r written by the SVD itself
-            PTT_CUDA(ptt_launch(c, k_svd_jacobi<CT, svd_nt<CT>(), 8, true>, dim3(1), dim3(svd_nt<CT>()),
-                                svd_smem_v<CT>(), pl, ws, delta, mr, i, c->d_status));
-            ptt_time_end(c, PTT_TIME_SVD);
-            PTT_LAUNCHED(c);
-        } else {
+        if (CT <= 64)  // columns in registers
+            PTT_CUDA(ptt_launch(c, k_svd_ring<CT <= 64 ? CT : 64>, dim3(1), dim3(svd_nt<CT>()),
+                                ring_smem<CT <= 64 ? CT : 64>(), pl, ws, delta, mr, i, c->d_status));
+        else
             PTT_CUDA(ptt_launch(c, k_svd_jacobi<CT>, dim3(1), dim3(svd_nt<CT>()), svd_smem<CT>(), pl, ws, delta, mr,
                                 i, c->d_status));
-            ptt_time_end(c, PTT_TIME_SVD);
-            PTT_LAUNCHED(c);
-            PTT_CUDA(ptt_launch(c, k_svd_replay, dim3((CT + 7) / 8), dim3(256), replay_smem<CT>(), pl, ws));
-            PTT_LAUNCHED(c);
-        }
+        ptt_time_end(c, PTT_TIME_SVD);
+        PTT_LAUNCHED(c);
+        PTT_CUDA(ptt_launch(c, k_svd_replay, dim3((CT + 7) / 8), dim3(256), replay_smem<CT>(), pl, ws));
+        PTT_LAUNCHED(c);
         if ((rc = launch_apply<CT>(c, x, i, RIGHT_T, pl, ws, &info->rank, CT))) return rc;
         if (g) {  // Q V_r for a bond the grid Cholesky QR finished
             int gx = (int)((mcap + gq::WROWS - 1) / gq::WROWS);
@@ -1240,7 +1464,7 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
                 Wmax = Wr[i] > Wmax ? Wr[i] : Wmax;
                 const int mr = maxr ? maxr[i] : rk[i];
                 ptt_time_begin(c, PTT_TIME_SVD);
-                PTT_CUDA(ptt_launch(c, k_svd_jacobi<32>, dim3(1), dim3(svd_nt<32>()), svd_smem<32>(), pl, wsb, delta, mr, i,
+                PTT_CUDA(ptt_launch(c, k_svd_ring<32>, dim3(1), dim3(svd_nt<32>()), ring_smem<32>(), pl, wsb, delta, mr, i,
                                     c->d_status));
                 ptt_time_end(c, PTT_TIME_SVD);
                 PTT_LAUNCHED(c);
@@ -1424,6 +1648,7 @@ extern "C" int ptt_ctx_autotune(ptt_ctx* c) {
     c->tkind = tkind;
     if (rc) return rc;
     c->cq_tuned++;
+    if ((rc = ptt_gemm_autotune(c))) return rc;
     return ptt_ctx_synchronize(c);
 }
 

@@ -314,14 +314,16 @@ int gemm(ptt_ctx* c, const GemmB& g) {
         ptt_time_end(c, PTT_TIME_GEMM);
         return PTT_OK;
     }
-    const bool big = g.M >= 48 && g.N >= 48;
+    const int tm64 = c->gemm_tm64 > 0 ? c->gemm_tm64 : 48;
+    const long long fill = c->gemm_fill > 0 ? c->gemm_fill : 2LL * c->nsm;
+    const bool big = g.M >= tm64 && g.N >= tm64;
     const int TM = big ? 64 : 32;
     dim3 grid((g.M + TM - 1) / TM, (g.N + TM - 1) / TM, 1);
     // split K when the tiles alone cannot fill the GPU and K is long
     const long long tiles = (long long)grid.x * grid.y * nb;
     int ns = 1, kper = g.K;
-    if (tiles < 2 * 148 && g.K >= 512) {
-        long long want = (2 * 148 + tiles - 1) / tiles;
+    if (tiles < fill && g.K >= 512) {
+        long long want = (fill + tiles - 1) / tiles;
         const long long kmax = (g.K + 255) / 256;
         ns = (int)(want < kmax ? want : kmax);
         if (ns > 64) ns = 64;
@@ -638,5 +640,98 @@ extern "C" int ptt_round_sketch(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, con
     for (int k = 0; k <= x->d; k++) full[k] = rx[k] * ry[k];
     if ((rc = sketch_round(x, y, z, ell, seed, tol, maxrank, used))) return rc;
     if (accepted) return check_sketch(z, used, full, pad, accepted);
+    return PTT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// autotuner of the contractions' tile width and split-K target: times the
+// shapes the sketch rounding meets (a batch of 48 x 48 x 48 products, tiles
+// of 32 or 64; one 40 x 40 product over K = 8192, split to fill 1, 2 or 4
+// times the SM count) and keeps a setting only when it is >= 10 % faster
+// than the built-in one.  Allocates its own operands; synchronises.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void k_tune_val(double* p, long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        p[e] = 1.0 / (double)(1 + (e * 7919) % 1021) - 0.0005;
+}
+}  // namespace
+
+int ptt_gemm_autotune(ptt_ctx* c) {
+    const int tm0 = c->gemm_tm64, fill0 = c->gemm_fill, tk = c->tkind;
+    c->tkind = 0;
+    double* buf = nullptr;
+    const long long nA = 48LL * 48 * 256 * 3, nB = 40LL * 8192 * 2 + 40 * 40;
+    const long long tot = nA > nB ? nA : nB;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = PTT_OK;
+    PTT_CUDA(cudaMalloc(&buf, sizeof(double) * (size_t)tot));
+    if ((rc = ptt_cuda_check(cudaEventCreate(&e0), "event")) || (rc = ptt_cuda_check(cudaEventCreate(&e1), "event"))) {
+        cudaFree(buf);
+        return rc;
+    }
+    k_tune_val<<<296, 256, 0, c->stream>>>(buf, tot);
+    auto time_it = [&](const GemmB& g, float* best) -> int {
+        float tmin = 1e30f;
+        for (int rep = 0; rep < 6; rep++) {
+            PTT_CUDA(cudaEventRecord(e0, c->stream));
+            int r2 = gemm(c, g);
+            if (r2) return r2;
+            PTT_CUDA(cudaEventRecord(e1, c->stream));
+            PTT_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            PTT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (rep > 0 && ms < tmin) tmin = ms;
+        }
+        *best = tmin;
+        return PTT_OK;
+    };
+    // (1) a batch of 256 products of 48 x 48 x 48: 64-wide tiles from 48 on, or 32-wide
+    GemmB ga = {};
+    ga.A = buf; ga.ars = 1; ga.acs = 48; ga.ab1 = 48 * 48; ga.ab2 = 0;
+    ga.B = buf + 48LL * 48 * 256; ga.brs = 1; ga.bcs = 48; ga.bb1 = 48 * 48; ga.bb2 = 0;
+    ga.C = buf + 2LL * 48 * 48 * 256; ga.crs = 1; ga.ccs = 48; ga.cb1 = 48 * 48; ga.cb2 = 0;
+    ga.M = ga.N = ga.K = 48; ga.nb1 = 256; ga.nb2 = 1; ga.alpha = 1.0; ga.beta = 0.0;
+    float t64 = 0.f, t32 = 0.f;
+    c->gemm_tm64 = 48;
+    if (!rc) rc = time_it(ga, &t64);
+    c->gemm_tm64 = 65;  // 48-wide products take 32-wide tiles
+    if (!rc) rc = time_it(ga, &t32);
+    const int tm_best = (t32 < 0.9f * t64) ? 65 : 48;
+    // (2) one 40 x 40 product over K = 8192: split-K fill targets
+    GemmB gb = {};
+    gb.A = buf; gb.ars = 8192; gb.acs = 1;  // A row-major 40 x 8192
+    gb.B = buf + 40LL * 8192; gb.brs = 1; gb.bcs = 8192;  // B column-major 8192 x 40
+    gb.C = buf + 80LL * 8192; gb.crs = 40; gb.ccs = 1;
+    gb.M = gb.N = 40; gb.K = 8192; gb.nb1 = gb.nb2 = 1; gb.alpha = 1.0; gb.beta = 0.0;
+    const int fills[3] = {2 * c->nsm, c->nsm, 4 * c->nsm};
+    float tf[3] = {1e30f, 1e30f, 1e30f};
+    c->gemm_tm64 = tm_best;
+    for (int i = 0; i < 3 && !rc; i++) {
+        c->gemm_fill = fills[i];
+        rc = time_it(gb, &tf[i]);
+    }
+    int fbest = 0;
+    for (int i = 1; i < 3; i++)
+        if (tf[i] < 0.9f * tf[0] && tf[i] < tf[fbest]) fbest = i;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(buf);
+    c->tkind = tk;
+    if (rc) {
+        c->gemm_tm64 = tm0;
+        c->gemm_fill = fill0;
+        return rc;
+    }
+    c->gemm_tm64 = tm_best;
+    c->gemm_fill = fills[fbest];
+    return PTT_OK;
+}
+
+extern "C" int ptt_ctx_autotune_gemm(const ptt_ctx* c, int* out2) {
+    if (!c || !out2) return ptt_set_error(PTT_ERR_ARG, "ptt_ctx_autotune_gemm: bad arguments");
+    out2[0] = c->gemm_tm64 > 0 ? c->gemm_tm64 : 48;
+    out2[1] = c->gemm_fill > 0 ? c->gemm_fill : 2 * c->nsm;
     return PTT_OK;
 }

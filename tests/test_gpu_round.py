@@ -190,6 +190,8 @@ def test_autotune(ctx):
     table = ctx.autotune()
     assert table.shape == (3, 6)
     assert all(v in (0, 1, 2, 4, 8, 16) for v in table.ravel())  # 0: the row-count rule is kept
+    tm64, fill = ctx.autotune_gemm()  # contraction tiles and split-K target
+    assert tm64 in (48, 65) and fill in (74, 148, 296, 592)
     X = P.TT.from_cores(ctx, x)
     X.round(tol, 64)
     after = X.get()
