@@ -80,11 +80,12 @@ PTT_API int ptt_ctx_kernel_work(ptt_ctx* ctx, double* work);
  * destroyed and recreated at the same address reuses its graph, which is
  * correct because the graph reads the descriptor at run time. */
 PTT_API int ptt_ctx_graphs(ptt_ctx* ctx, int on);
-/* Factorisation used for unfoldings with at most 32 columns (no counterpart
+/* Factorisation used for unfoldings with at most 64 columns (no counterpart
  * in the reference, whose TSQR is Householder throughout): with on != 0 (the
- * default) a shifted/repeated Cholesky-QR sequence, which falls back to the
- * Householder TSQR for a bond it cannot make orthonormal; with on == 0 the
- * Householder TSQR only.  ptt_ctx_qr_counts returns, summed over the context
+ * default) a shifted/repeated Cholesky-QR sequence -- by one thread-block
+ * cluster up to 32 columns, by all SMs (one launch per Gram stage) for 33 to
+ * 64 -- which falls back to the Householder TSQR for a bond it cannot make
+ * orthonormal; with on == 0 the Householder TSQR only.  ptt_ctx_qr_counts returns, summed over the context
  * and its batch workers: [0] factorisations finished by Cholesky QR, [1] fell
  * back, [2] Gram stages of the finished ones (synchronises). */
 PTT_API int ptt_ctx_cholqr(ptt_ctx* ctx, int on);

@@ -49,7 +49,9 @@ constexpr int NG = 7;                  // row groups of the Gram threads (36 til
 constexpr int GROUP = 8;               // CTAs summed by the first level
 constexpr int RPB_MAX = 112;           // rows per CTA
 constexpr int RPB_MIN = 16;
-constexpr int MAXST = 6;               // stage launches per factorisation
+constexpr int MAXST = 8;               // stage launches per factorisation: an unfolding of condition ~1e16
+                                       // (numerically rank-deficient) takes three shifted stages, a plain
+                                       // one and a first-order finish -- seven launches
 constexpr int LTRI = CB * (CB + 1) / 2;
 constexpr int EPT = (LTRI + NT - 1) / NT;  // lower-triangle entries per thread of the Cholesky
 constexpr double TAU = 1e-13;
@@ -242,9 +244,15 @@ __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int
     const View& src = (stage <= 1) ? A : Qv;
     // this CTA's rows (zero beyond c), every element in flight by cp.async
     for (int e = tid; e < h * XP; e += NT) Xs[e] = 0.0;
-    if (stage >= 1) {  // the factor of the previous stage
+    if (stage >= 1) {  // the factor of the previous stage (all loads in flight first)
         const double* F = g.rec + O_FAC;
-        for (int e = tid; e < CB * RP + CB; e += NT) sScr[e] = ldcg(F + e);
+        constexpr int FL = CB * RP + CB, FPT = (FL + NT - 1) / NT;
+        double f[FPT];
+#pragma unroll
+        for (int k = 0; k < FPT; k++) f[k] = (tid + k * NT < FL) ? ldcg(F + tid + k * NT) : 0.0;
+#pragma unroll
+        for (int k = 0; k < FPT; k++)
+            if (tid + k * NT < FL) sScr[tid + k * NT] = f[k];
     }
     __syncthreads();
     {
@@ -340,12 +348,25 @@ __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int
     if (tid == 0) g.cnt[grp] = 0;
     __threadfence();
     {
+        // every load of the thread's entries in flight before the sums (in
+        // CTA order; absent CTAs add exact zeros)
         const double* P = g.part + (long long)grp * GROUP * UP;
         double* Gp = g.gpart + (long long)grp * UP;
-        for (int u = tid; u < UP; u += NT) {
-            double v = 0.0;
-            for (int t = 0; t < gsize; t++) v += ldcg(P + (long long)t * UP + u);
-            Gp[u] = v;
+        constexpr int UPT = (UP + NT - 1) / NT;
+        double v[UPT][GROUP];
+#pragma unroll
+        for (int k = 0; k < UPT; k++) {
+            const int u = tid + k * NT;
+#pragma unroll
+            for (int t = 0; t < GROUP; t++) v[k][t] = (u < UP && t < gsize) ? ldcg(P + (long long)t * UP + u) : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < UPT; k++) {
+            const int u = tid + k * NT;
+            double a = 0.0;
+#pragma unroll
+            for (int t = 0; t < GROUP; t++) a += v[k][t];
+            if (u < UP) Gp[u] = a;
         }
     }
     __threadfence();
@@ -365,8 +386,15 @@ __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int
     if (tid == 0) s_flags = 0;
     __syncthreads();
     for (int u = tid; u < UP; u += NT) {
+        // the groups' sums in order, eight loads in flight at a time
         double v = 0.0;
-        for (int t = 0; t < ngroups; t++) v += ldcg(g.gpart + (long long)t * UP + u);
+        for (int t0 = 0; t0 < ngroups; t0 += 8) {
+            double w8[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) w8[t] = (t0 + t < ngroups) ? ldcg(g.gpart + (long long)(t0 + t) * UP + u) : 0.0;
+#pragma unroll
+            for (int t = 0; t < 8; t++) v += w8[t];
+        }
         const int qq = u / (TS * TS), w = u - qq * (TS * TS);
         int a0, b0;
         cq::upper_tile(qq, &a0, &b0);
@@ -376,9 +404,20 @@ __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int
             sG[gj * GP + gi] = v;
         }
     }
-    for (int e = tid; e < CB * GP; e += NT) {
-        const int i = e / GP, j = e - (e / GP) * GP;
-        sT[e] = (stage == 0) ? ((i == j && i < c) ? 1.0 : 0.0) : ((j < CB) ? ldcg(g.rec + O_T + i * CB + j) : 0.0);
+    {
+        constexpr int TPT = (CB * GP + NT - 1) / NT;
+        double tv[TPT];
+#pragma unroll
+        for (int k = 0; k < TPT; k++) {
+            const int e = tid + k * NT;
+            const int i = e / GP, j = e - (e / GP) * GP;
+            tv[k] = (e >= CB * GP) ? 0.0
+                    : (stage == 0) ? ((i == j && i < c) ? 1.0 : 0.0)
+                    : ((j < CB) ? ldcg(g.rec + O_T + i * CB + j) : 0.0);
+        }
+#pragma unroll
+        for (int k = 0; k < TPT; k++)
+            if (tid + k * NT < CB * GP) sT[tid + k * NT] = tv[k];
     }
     __syncthreads();
     // trace, max |G - I|, NaN, zero column

@@ -485,12 +485,19 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
 // k_svd_replay(_b) exactly as by k_svd_jacobi, and after the last sweep the
 // columns are written to shared memory for the same epilogue (order, rank
 // rule, U S, statistics).
-template <int CT>
-__global__ void __launch_bounds__(svd_nt<CT>()) k_svd_ring(Plan pl, double* ws, double delta, int maxr, int bond,
-                                                          int* status) {
+// LP lanes per column pair (4: a round's rotation math, the same instructions
+// for every group of a warp, serves eight pairs per warp; the SVD is bound by
+// the instructions it issues on its one SM).
+template <int CT, int LP = 4>
+__host__ __device__ constexpr int ring_nt() {
+    return (CT / 2) * LP;
+}
+template <int CT, int LP = 4>
+__global__ void __launch_bounds__(ring_nt<CT, LP>()) k_svd_ring(Plan pl, double* ws, double delta, int maxr, int bond,
+                                                               int* status) {
     PTT_PDL_ENTRY();
-    constexpr int SVD_NT = svd_nt<CT>();
-    constexpr int LP = 8;
+    constexpr int SVD_NT = ring_nt<CT, LP>();
+    constexpr int GPW = 32 / LP;           // groups per warp
     constexpr int NG = CT / LP;            // rows per lane
     constexpr int NW = SVD_NT / 32;        // warps
     constexpr int S = CT + 1;
@@ -582,14 +589,14 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_ring(Plan pl, double* ws, 
             }
             // move the columns to the next round's pairs
             double* xb0 = xch + (long long)buf * NW * 2 * LP * (NG + 1);
-            const int gw = lane / LP;  // group within the warp (0 .. 3)
+            const int gw = lane / LP;  // group within the warp (0 .. GPW - 1)
             if (gw == 0) {             // this warp's first top: to the previous warp's last group
                 double* d = xb0 + ((warp * 2 + 0) * LP + p) * (NG + 1);
 #pragma unroll
                 for (int v = 0; v < NG; v++) d[v] = top[v];
                 d[NG] = al;
             }
-            if (gw == 3) {  // this warp's last bottom: to the next warp's first group
+            if (gw == GPW - 1) {  // this warp's last bottom: to the next warp's first group
                 double* d = xb0 + ((warp * 2 + 1) * LP + p) * (NG + 1);
 #pragma unroll
                 for (int v = 0; v < NG; v++) d[v] = bot[v];
@@ -604,7 +611,7 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_ring(Plan pl, double* ws, 
             double rta = __shfl_down_sync(0xffffffffu, al, LP);
             double rbb = __shfl_up_sync(0xffffffffu, be, LP);
             __syncthreads();
-            if (gw == 3 && warp + 1 < NW) {
+            if (gw == GPW - 1 && warp + 1 < NW) {
                 const double* sx = xb0 + (((warp + 1) * 2 + 0) * LP + p) * (NG + 1);
 #pragma unroll
                 for (int v = 0; v < NG; v++) rt[v] = sx[v];
@@ -740,10 +747,10 @@ __global__ void __launch_bounds__(svd_nt<CT>()) k_svd_ring(Plan pl, double* ws, 
     }
 }
 
-template <int CT>
+template <int CT, int LP = 4>
 static size_t ring_smem() {
-    constexpr int NW = svd_nt<CT>() / 32;
-    return sizeof(double) * ((size_t)(CT + 2) * (CT + 1) + 2ull * NW * 2 * 8 * (CT / 8 + 1));
+    constexpr int NW = ring_nt<CT, LP>() / 32;
+    return sizeof(double) * ((size_t)(CT + 2) * (CT + 1) + 2ull * NW * 2 * LP * (CT / LP + 1));
 }
 
 // Rebuild rows of V (q x q, V = product of the recorded rotations) and write
@@ -1068,7 +1075,7 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
     const int KC = (CT + KG - 1) / KG * KG;
     int PMAX = 1, KLMAX = 1, NBMAX = 1;
     long long MQMAX = 1;
-    const int pmax = use_gq ? 8 : 512;
+    const int pmax = use_gq ? 32 : 512;
     for (int i = 0; i < d; i++) {
         Plan t;
         long long ml = (long long)rk[i] * x->n[i], mr = (long long)x->n[i] * rk[i + 1];
@@ -1167,7 +1174,7 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
         const int mr = maxr ? maxr[i] : rk[i];
         ptt_time_begin(c, PTT_TIME_SVD);
         if (CT <= 64)  // columns in registers
-            PTT_CUDA(ptt_launch(c, k_svd_ring<CT <= 64 ? CT : 64>, dim3(1), dim3(svd_nt<CT>()),
+            PTT_CUDA(ptt_launch(c, k_svd_ring<CT <= 64 ? CT : 64>, dim3(1), dim3(ring_nt<CT <= 64 ? CT : 64>()),
                                 ring_smem<CT <= 64 ? CT : 64>(), pl, ws, delta, mr, i, c->d_status));
         else
             PTT_CUDA(ptt_launch(c, k_svd_jacobi<CT>, dim3(1), dim3(svd_nt<CT>()), svd_smem<CT>(), pl, ws, delta, mr,
@@ -1464,7 +1471,7 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
                 Wmax = Wr[i] > Wmax ? Wr[i] : Wmax;
                 const int mr = maxr ? maxr[i] : rk[i];
                 ptt_time_begin(c, PTT_TIME_SVD);
-                PTT_CUDA(ptt_launch(c, k_svd_ring<32>, dim3(1), dim3(svd_nt<32>()), ring_smem<32>(), pl, wsb, delta, mr, i,
+                PTT_CUDA(ptt_launch(c, k_svd_ring<32>, dim3(1), dim3(ring_nt<32>()), ring_smem<32>(), pl, wsb, delta, mr, i,
                                     c->d_status));
                 ptt_time_end(c, PTT_TIME_SVD);
                 PTT_LAUNCHED(c);
