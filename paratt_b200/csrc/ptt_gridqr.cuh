@@ -52,17 +52,17 @@ constexpr int RPB_MIN = 16;
 constexpr int MAXST = 8;               // stage launches per factorisation: an unfolding of condition ~1e16
                                        // (numerically rank-deficient) takes three shifted stages, a plain
                                        // one and a first-order finish -- seven launches
-constexpr int LTRI = CB * (CB + 1) / 2;
-constexpr int EPT = (LTRI + NT - 1) / NT;  // lower-triangle entries per thread of the Cholesky
 constexpr double TAU = 1e-13;
 constexpr double FIRST = 1e-7;
 constexpr double FIRST_DONE = 1e-8;
 constexpr double U = 1.1102230246251565e-16;
 constexpr size_t SMEM = sizeof(double) * ((size_t)RPB_MAX * XP + (size_t)NG * UP);
-static_assert(CB * GP + CB * RP + CB + CB * GP + 2 * CB <= NG * UP, "decision arrays fit the Gram scratch");
+constexpr int FSZ = CB * RP + CB;      // a factor and its inverse pivots
+static_assert(CB * GP + 2 * FSZ + 64 <= NG * UP, "decision arrays fit the Gram scratch");
+static_assert(CB * GP <= FSZ, "the accumulated R fits a factor buffer");
 static_assert(CB * RP + CB <= NG * UP, "factor fits the Gram scratch");
 
-enum { RUN = 0, DONE = 1, FALLBACK = 2, FINISH = 4 };
+enum { RUN = 0, DONE = 1, FALLBACK = 2, FINISH = 4, CHOL = 8 };
 
 __host__ __device__ __forceinline__ bool finished(int s) { return s == DONE || s == FINISH; }
 
@@ -129,66 +129,88 @@ __device__ __forceinline__ void row_solve(double* xs, const double* R, const dou
     for (int j = 0; j < CB; j += 2) *(double2*)(xs + j) = make_double2(x[j], x[j + 1]);
 }
 
-// lower-triangle entry e (row-major packing) -> (i, l), l <= i
-__device__ __forceinline__ void tri_index(int e, int* i, int* l) {
-    int r = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
-    while ((r + 1) * (r + 2) / 2 <= e) r++;
-    while (r * (r + 1) / 2 > e) r--;
-    *i = r;
-    *l = e - r * (r + 1) / 2;
-}
-
-// Cholesky factor of G + shift I (c x c, pitch GP) by all NT threads:
-// right-looking, every thread keeps its lower-triangle entries in registers,
-// and the column of the next step is published through a double buffer, so
-// each step costs one block barrier.  Result: R = L^T (row-major, pitch RP,
-// zero outside the upper c x c triangle) and inverse pivots iv[j].  Returns
-// false when a pivot is not positive (NaN included); *ratio = min/max pivot.
-__device__ bool block_chol(const double* G, int c, double shift, double* R, double* iv, double* col2, double* ratio) {
-    const int tid = threadIdx.x;
-    double a[EPT];
-    int ii[EPT], ll[EPT];
+// Cholesky of one 32-column panel by one warp, lane = column: g[t] holds
+// entry (t, lane) of the panel's symmetric block (rows t < 32); row j of the
+// factor is broadcast through sRow.  Writes R[off + j][off + lane] (pitch RP)
+// and iv[off + j] = 1 / R[off + j][off + j] for j < cc; tracks the pivots.
+__device__ __forceinline__ void chol_panel(double (&g)[32], int cc, int off, double* R, double* iv, double* sRow,
+                                           bool& ok, double& dmin, double& dmax) {
+    const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int s = 0; s < EPT; s++) {
-        const int e = tid + NT * s;
-        int i = CB, l = CB;
-        if (e < LTRI) tri_index(e, &i, &l);
-        ii[s] = i;
-        ll[s] = l;
-        a[s] = (i < c && l < c) ? G[i * GP + l] + (i == l ? shift : 0.0) : 0.0;
-    }
-    for (int e = tid; e < CB * RP; e += NT) R[e] = 0.0;
-    for (int e = tid; e < CB; e += NT) iv[e] = 0.0;
-#pragma unroll
-    for (int s = 0; s < EPT; s++)
-        if (ll[s] == 0 && ii[s] < CB) col2[ii[s]] = a[s];
-    bool ok = true;
-    double dmin = 1.0 / 0.0, dmax = 0.0;
-    for (int j = 0; j < c; j++) {
-        __syncthreads();
-        const double* col = col2 + (j & 1) * CB;
-        double* nxt = col2 + ((j + 1) & 1) * CB;
-        const double d = col[j];
-        ok = ok && (d > 0.0);
+    for (int j = 0; j < 32; j++) {
+        if (j >= cc) continue;
+        const double d = __shfl_sync(0xffffffffu, g[j], j);
+        ok = ok && (d > 0.0);  // false for NaN
         dmin = fmin(dmin, d);
         dmax = fmax(dmax, d);
         const double dd = d > 0.0 ? d : 1.0;
         const double inv = rsqrt(dd);
-        const double piv = dd * inv;
+        const double rj = (lane == j) ? dd * inv : ((lane > j && lane < cc) ? g[j] * inv : 0.0);
+        sRow[lane] = rj;
+        __syncwarp();
+        if (lane > j && lane < cc) {
 #pragma unroll
-        for (int s = 0; s < EPT; s++) {
-            const int i = ii[s], l = ll[s];
-            if (i >= c) continue;
-            if (l == j) {
-                R[j * RP + i] = (i == j) ? piv : a[s] * inv;
-            } else if (l > j) {
-                a[s] = fma(-(col[i] * inv), col[l] * inv, a[s]);
-                if (l == j + 1) nxt[i] = a[s];
+            for (int t = j + 1; t < 32; t++) g[t] = fma(-sRow[t], rj, g[t]);
+        }
+        if (lane >= j && lane < cc) R[(off + j) * RP + off + lane] = rj;
+        if (lane == j) iv[off + j] = inv;
+        __syncwarp();
+    }
+}
+
+// Cholesky factor of G + shift I (c x c, pitch GP) by ONE warp in two
+// 32-column panels: R11 = chol(G11); R12 = R11^{-T} G12 (forward
+// substitution, lane = column); S = G22 - R12^T R12 (lane = column, in
+// registers); R22 = chol(S).  Result R (row-major, pitch RP, zero outside the
+// upper c x c triangle), iv[j] = 1 / R[j][j].  Returns false when a pivot is
+// not positive (NaN included); *ratio = min/max pivot.  Two warps can form
+// the plain and the shifted factor at once into different R buffers.
+__device__ bool warp_chol64(const double* G, int c, double shift, double* R, double* iv, double* sRow, double* ratio) {
+    const int lane = threadIdx.x & 31;
+    for (int e = lane; e < CB * RP; e += 32) R[e] = 0.0;
+    for (int e = lane; e < CB; e += 32) iv[e] = 0.0;
+    __syncwarp();
+    bool ok = true;
+    double dmin = 1.0 / 0.0, dmax = 0.0;
+    const int c1 = c < 32 ? c : 32;
+    double g[32];
+#pragma unroll
+    for (int t = 0; t < 32; t++) g[t] = (t < c1 && lane < c1) ? G[t * GP + lane] + (t == lane ? shift : 0.0) : 0.0;
+    chol_panel(g, c1, 0, R, iv, sRow, ok, dmin, dmax);
+    if (c > 32) {
+        const int c2 = c - 32, k = 32 + lane;
+        const bool mine = lane < c2;
+        // R12[:, k]: R11^T y = G[0:32, k]
+        double y[32];
+#pragma unroll
+        for (int i = 0; i < 32; i++) y[i] = mine ? G[i * GP + k] : 0.0;
+#pragma unroll
+        for (int i = 0; i < 32; i++) {
+            const double yi = y[i] * iv[i];
+            y[i] = yi;
+#pragma unroll
+            for (int t = i + 1; t < 32; t++) y[t] = fma(-R[i * RP + t], yi, y[t]);
+        }
+        if (mine) {
+#pragma unroll
+            for (int i = 0; i < 32; i++) R[i * RP + k] = y[i];
+        }
+        __syncwarp();
+        // S[32 + t][k] = G[32 + t][k] + shift [t == lane] - sum_i R[i][32 + t] R[i][k]
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+            double acc = 0.0;
+            if (mine && t < c2) {
+#pragma unroll
+                for (int i = 0; i < 32; i++) acc = fma(R[i * RP + 32 + t], y[i], acc);
+                g[t] = G[(32 + t) * GP + k] + (t == lane ? shift : 0.0) - acc;
+            } else {
+                g[t] = 0.0;
             }
         }
-        if (tid == 0) iv[j] = inv;
+        chol_panel(g, c2, 32, R, iv, sRow, ok, dmin, dmax);
     }
-    __syncthreads();
+    __syncwarp();
     *ratio = dmax > 0.0 ? dmin / dmax : 0.0;
     return ok;
 }
@@ -201,7 +223,8 @@ __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int
     extern __shared__ double gsm[];
     double* Xs = gsm;                     // rpb x XP rows
     double* sScr = Xs + RPB_MAX * XP;     // factor; Gram partials; decision arrays
-    __shared__ int s_state, s_fin, s_ticket, s_flags;
+    __shared__ int s_state, s_fin, s_ticket, s_flags, s_cok[2];
+    __shared__ double s_cratio[2];
     __shared__ double s_red[NT / 32][2];
     State* st = (State*)g.rec;
     const View A = make_view(D, k, mode, false);
@@ -378,46 +401,46 @@ __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int
     __threadfence();
     // ---- the deciding CTA: G = sum of the groups in order --------------------
     double* sG = sScr;              // CB x GP
-    double* sF = sG + CB * GP;      // CB x RP factor
-    double* sIv = sF + CB * RP;     // CB inverse pivots
-    double* sT = sIv + CB;          // CB x GP accumulated R (the factors applied so far)
-    double* sCol = sT + CB * GP;    // 2 x CB
+    double* sFa = sG + CB * GP;     // CB x RP factor + CB inverse pivots: plain Cholesky (or first order)
+    double* sFb = sFa + FSZ;        // the same for the shifted Cholesky
+    double* sRow = sFb + FSZ;       // 2 x 32 row broadcasts of the two Cholesky warps
     for (int e = tid; e < CB * GP; e += NT) sG[e] = 0.0;
     if (tid == 0) s_flags = 0;
     __syncthreads();
-    for (int u = tid; u < UP; u += NT) {
-        // the groups' sums in order, eight loads in flight at a time
-        double v = 0.0;
-        for (int t0 = 0; t0 < ngroups; t0 += 8) {
-            double w8[8];
-#pragma unroll
-            for (int t = 0; t < 8; t++) w8[t] = (t0 + t < ngroups) ? ldcg(g.gpart + (long long)(t0 + t) * UP + u) : 0.0;
-#pragma unroll
-            for (int t = 0; t < 8; t++) v += w8[t];
-        }
-        const int qq = u / (TS * TS), w = u - qq * (TS * TS);
-        int a0, b0;
-        cq::upper_tile(qq, &a0, &b0);
-        const int gi = a0 * TS + w / TS, gj = b0 * TS + w % TS;
-        if (gi < c && gj < c) {
-            sG[gi * GP + gj] = v;
-            sG[gj * GP + gi] = v;
-        }
-    }
     {
-        constexpr int TPT = (CB * GP + NT - 1) / NT;
-        double tv[TPT];
+        // the groups' sums in order, all of a thread's entries of eight groups
+        // in flight at a time
+        constexpr int UPT = (UP + NT - 1) / NT;
+        double vs[UPT];
 #pragma unroll
-        for (int k = 0; k < TPT; k++) {
-            const int e = tid + k * NT;
-            const int i = e / GP, j = e - (e / GP) * GP;
-            tv[k] = (e >= CB * GP) ? 0.0
-                    : (stage == 0) ? ((i == j && i < c) ? 1.0 : 0.0)
-                    : ((j < CB) ? ldcg(g.rec + O_T + i * CB + j) : 0.0);
+        for (int k = 0; k < UPT; k++) vs[k] = 0.0;
+        for (int t0 = 0; t0 < ngroups; t0 += 8) {
+            double w8[UPT][8];
+#pragma unroll
+            for (int k = 0; k < UPT; k++) {
+                const int u = tid + k * NT;
+#pragma unroll
+                for (int t = 0; t < 8; t++)
+                    w8[k][t] = (u < UP && t0 + t < ngroups) ? ldcg(g.gpart + (long long)(t0 + t) * UP + u) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < UPT; k++)
+#pragma unroll
+                for (int t = 0; t < 8; t++) vs[k] += w8[k][t];
         }
 #pragma unroll
-        for (int k = 0; k < TPT; k++)
-            if (tid + k * NT < CB * GP) sT[tid + k * NT] = tv[k];
+        for (int k = 0; k < UPT; k++) {
+            const int u = tid + k * NT;
+            if (u >= UP) continue;
+            const int qq = u / (TS * TS), w = u - qq * (TS * TS);
+            int a0, b0;
+            cq::upper_tile(qq, &a0, &b0);
+            const int gi = a0 * TS + w / TS, gj = b0 * TS + w % TS;
+            if (gi < c && gj < c) {
+                sG[gi * GP + gj] = vs[k];
+                sG[gj * GP + gi] = vs[k];
+            }
+        }
     }
     __syncthreads();
     // trace, max |G - I|, NaN, zero column
@@ -470,33 +493,94 @@ __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int
                 else if (l == j)
                     v = 1.0 + 0.5 * (sG[j * GP + j] - 1.0);
             }
-            sF[e] = v;
+            sFa[e] = v;
         }
-        for (int j = tid; j < CB; j += NT) sIv[j] = j < c ? 1.0 / (1.0 + 0.5 * (sG[j * GP + j] - 1.0)) : 0.0;
+        for (int j = tid; j < CB; j += NT) sFa[CB * RP + j] = j < c ? 1.0 / (1.0 + 0.5 * (sG[j * GP + j] - 1.0)) : 0.0;
         dec = emax <= FIRST_DONE ? FINISH : RUN;
     } else if (stage == MAXST - 1) {
         dec = FALLBACK;
     } else {
-        double ratio;
-        bool ok = block_chol(sG, c, 0.0, sF, sIv, sCol, &ratio);
-        if (!ok || ratio < 1e-12) {
-            const double sigma = 11.0 * ((double)m * c + (double)c * (c + 1)) * U * tr;
-            ok = block_chol(sG, c, sigma, sF, sIv, sCol, &ratio);
-            nshift++;
+        // plain (warp 0) and shifted (warp 1) Cholesky at once; the plain one
+        // is kept when its pivots span less than 12 decades
+        if (tid < 64) {
+            const int w = tid >> 5;
+            const double sigma = w ? 11.0 * ((double)m * c + (double)c * (c + 1)) * U * tr : 0.0;
+            double ratio;
+            double* F = w ? sFb : sFa;
+            const bool ok = warp_chol64(sG, c, sigma, F, F + CB * RP, sRow + 32 * w, &ratio);
+            if ((tid & 31) == 0) {
+                s_cok[w] = ok;
+                s_cratio[w] = ratio;
+            }
         }
-        dec = ok ? RUN : FALLBACK;
+        dec = CHOL;
+    }
+    __syncthreads();
+    bool use_b = false;
+    if (dec == CHOL) {
+        if (s_cok[0] && s_cratio[0] >= 1e-12) {
+            dec = RUN;
+        } else if (s_cok[1]) {
+            dec = RUN;
+            use_b = true;
+            nshift++;
+        } else {
+            dec = FALLBACK;
+        }
     }
     if (stage == MAXST - 1 && (dec == RUN || dec == FINISH)) dec = FALLBACK;  // no launch left to apply it
+    double* sF = use_b ? sFb : sFa;  // the factor applied next
+    double* sT = use_b ? sFa : sFb;  // the accumulated R of the factors applied so far
+    {
+        constexpr int TPT = (CB * GP + NT - 1) / NT;
+        double tv[TPT];
+#pragma unroll
+        for (int k = 0; k < TPT; k++) {
+            const int e = tid + k * NT;
+            const int i = e / GP, j = e - (e / GP) * GP;
+            tv[k] = (e >= CB * GP) ? 0.0
+                    : (stage == 0) ? ((i == j && i < c) ? 1.0 : 0.0)
+                    : ((j < CB) ? ldcg(g.rec + O_T + i * CB + j) : 0.0);
+        }
+#pragma unroll
+        for (int k = 0; k < TPT; k++)
+            if (tid + k * NT < CB * GP) sT[tid + k * NT] = tv[k];
+    }
     __syncthreads();
     if (dec == RUN || dec == FINISH) {
-        // new accumulated R = F T (both upper triangular), into sG (no longer needed)
-        for (int e = tid; e < CB * CB; e += NT) {
-            const int i = e / CB, j = e - (e / CB) * CB;
-            double v = 0.0;
-            if (j >= i && j < c) {
-                for (int t = i; t <= j; t++) v = fma(sF[i * RP + t], sT[t * GP + j], v);
+        // new accumulated R = F T (both upper triangular) into sG: each thread
+        // a 4 x 4 block; at stage 0 T = I and it is F itself
+        {
+            const int bi = (tid >> 4) * 4, bj = (tid & 15) * 4;
+            double acc[4][4];
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+            if (stage == 0) {
+#pragma unroll
+                for (int a = 0; a < 4; a++)
+#pragma unroll
+                    for (int b = 0; b < 4; b++) acc[a][b] = sF[(bi + a) * RP + bj + b];
+            } else if (bj + 3 >= bi) {
+                for (int t = bi; t <= bj + 3 && t < CB; t++) {
+                    double fa[4], tb[4];
+#pragma unroll
+                    for (int a = 0; a < 4; a++) fa[a] = sF[(bi + a) * RP + t];
+#pragma unroll
+                    for (int b = 0; b < 4; b++) tb[b] = sT[t * GP + bj + b];
+#pragma unroll
+                    for (int a = 0; a < 4; a++)
+#pragma unroll
+                        for (int b = 0; b < 4; b++) acc[a][b] = fma(fa[a], tb[b], acc[a][b]);
+                }
             }
-            sG[i * GP + j] = v;
+            // F and T are upper triangular and zero beyond c: the products
+            // outside the upper c x c triangle are exact zeros
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int b = 0; b < 4; b++) sG[(bi + a) * GP + bj + b] = (bj + b >= bi + a) ? acc[a][b] : 0.0;
         }
         __syncthreads();
         double* F = g.rec + O_FAC;
