@@ -196,7 +196,7 @@ def run_ours(args, rank, world, local_rank):
 
     d, n, maxr, dt = CFG["d"], CFG["n"], CFG["maxrank"], CFG["dt"]
     ctx = P.Context(local_rank)
-    tuned = autotune(ctx)  # Cholesky-QR cluster sizes, timed once per context
+    tuned = autotune(ctx) if not args.no_autotune else "not tuned (--no-autotune)"
     u0 = Wl.initial_condition(d, n, CFG["ngauss"], CFG["seed"] + rank)
     tol = CFG["tol"] * Wl.rms_norm(u0)
     cap = [1] + [2 * maxr] * (d - 1) + [1]
@@ -392,7 +392,7 @@ def run_batch(args, rank, world, local_rank):
 
     rep = Replicas("nccl")
     ctx = P.Context(local_rank)
-    tuned = autotune(ctx)  # Cholesky-QR cluster sizes, timed once per context
+    tuned = autotune(ctx) if not args.no_autotune else "not tuned (--no-autotune)"
     shapes = Wl.batch_shapes(64, 4)
     costs = [Wl.rounding_cost(sh) for sh in shapes]
     shards = Wl.shard_by_cost(costs, world)
@@ -544,7 +544,8 @@ def run_round(args, rank, world, local_rank):
     if rank != 0:
         return 0
     ctx = P.Context(local_rank)
-    autotune(ctx)  # Cholesky-QR cluster sizes, timed once per context
+    if not args.no_autotune:
+        autotune(ctx)  # Cholesky-QR cluster sizes, timed once per context
     c1 = config1_rounding(P, ctx, args.steps, args.warmup)
     t = c1["ms"]
     out = {
@@ -645,7 +646,7 @@ def run_one_step(args, local_rank):
 
     d, n, maxr, dt = CFG["d"], CFG["n"], CFG["maxrank"], CFG["dt"]
     ctx = P.Context(local_rank)
-    tuned = autotune(ctx)  # Cholesky-QR cluster sizes, timed once per context
+    tuned = autotune(ctx) if not args.no_autotune else "not tuned (--no-autotune)"
     u0 = Wl.initial_condition(d, n, CFG["ngauss"], CFG["seed"])
     tol = CFG["tol"] * Wl.rms_norm(u0)
     plain = P.RxnBurgers(ctx, d, n, maxrank=maxr, dt=dt, tol=tol, seed=7)
@@ -678,6 +679,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the built-in cluster-size and tile rules (short runs under a profiler)")
     ap.add_argument("--formal-d", type=int, default=40, help="cores of the trains of --workload formal")
     ap.add_argument("--one-step", choices=["plain", "learned"], default=None,
                     help="profiling aid: W warm-up steps, then one step; prints the launch index to skip to")

@@ -255,6 +255,24 @@ __device__ __forceinline__ int circle_col(int pos, int round, int qq) {
     return pos == 0 ? 0 : 1 + (pos - 1 + round) % (qq - 1);
 }
 
+// Stationary-ring order, for G = qq / 2 a power of two.  Level l (block size
+// hb = G >> l groups, rounds [2G - 2hb, 2G - hb)): block b of hb consecutive
+// pairs owns columns [2 hb b, 2 hb (b + 1)); pair i of the block keeps column
+// 2 hb b + i and meets 2 hb b + hb + (i + s) mod hb at shift s, so the second
+// columns move one pair along a ring of hb pairs per round while the first
+// ones stay.  Between levels each block splits in two: the first half pairs
+// its first columns among themselves, the second half its second columns
+// (a swap of one column between pairs i and i + hb / 2).  Every pair of
+// columns meets once in 2G - 1 rounds.
+__device__ __forceinline__ void stat_cols(int i, int rd, int G, int* pc, int* qc) {
+    const int x = 2 * G - 1 - rd;  // in [hb, 2 hb - 1]
+    const int hb = 1 << (31 - __clz(x));
+    const int s = rd - (2 * G - 2 * hb);
+    const int b = i / hb, ii = i - b * hb;
+    *pc = 2 * hb * b + ii;
+    *qc = 2 * hb * b + hb + (ii + s) % hb;
+}
+
 // threads of the SVD block: 8 lanes for each of the (CT+2)/2 column pairs
 // of a round, rounded to a power of two (idle threads only slow the barriers)
 template <int CT>
@@ -445,6 +463,7 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
         info->rank = rank;
         info->nsv = nsv;
         info->sweeps = sweeps;
+        info->order = 0;
         double tail = 0.0;
         for (int j = rank; j < q; j++) tail += s_sig[s_ord[j]] * s_sig[s_ord[j]];
         info->tail = tail;
@@ -493,7 +512,7 @@ __host__ __device__ constexpr int ring_nt() {
     return (CT / 2) * LP;
 }
 template <int CT, int LP = 4>
-__global__ void __launch_bounds__(ring_nt<CT, LP>()) k_svd_ring(Plan pl, double* ws, double delta, int maxr, int bond,
+__global__ void __launch_bounds__(ring_nt<CT, LP>(), 1) k_svd_ring(Plan pl, double* ws, double delta, int maxr, int bond,
                                                                int* status) {
     PTT_PDL_ENTRY();
     constexpr int SVD_NT = ring_nt<CT, LP>();
@@ -519,10 +538,14 @@ __global__ void __launch_bounds__(ring_nt<CT, LP>()) k_svd_ring(Plan pl, double*
     const int G = qq / 2;  // active pairs (one per group)
     const bool act = grp < G;
     const double* R = ws + pl.o_Rn;  // root factor, row-major CT x CT; L = R^T: column j = row j of R
-    // round 0: pair g holds columns g (top) and qq - 1 - g (bottom)
+    // stationary-ring order when the pair count is a power of two (one column
+    // of each pair moves per round), circle order otherwise
+    const bool stat = G >= 2 && (G & (G - 1)) == 0;
+    // round 0: pair g holds columns g (top) and qq - 1 - g (circle) or G + g
+    // (stationary ring) (bottom)
     double top[NG], bot[NG];
     {
-        const int ct = grp, cb = qq - 1 - grp;
+        const int ct = grp, cb = stat ? G + grp : qq - 1 - grp;
 #pragma unroll
         for (int v = 0; v < NG; v++) {
             const int t = p + LP * v;
@@ -534,6 +557,7 @@ __global__ void __launch_bounds__(ring_nt<CT, LP>()) k_svd_ring(Plan pl, double*
     const int npair = (CT + 2) / 2;
     const double tol = (double)(c < 16 ? 16 : c) * 2.220446049250313e-16;
     const double tol2 = tol * tol;
+    const int gw = lane / LP;  // group within the warp (0 .. GPW - 1)
     int sweeps = 0, buf = 0;
     bool conv = (qq < 2);
     for (int sw = 0; sw < MAXSW && !conv; sw++) {
@@ -557,95 +581,182 @@ __global__ void __launch_bounds__(ring_nt<CT, LP>()) k_svd_ring(Plan pl, double*
         for (int w = 0; w < NW; w++) mx = fmax(mx, s_wmax[w]);
         const double thr2 = (double)q * 1.232595164407831e-32 * mx;  // (sqrt(q) 2^-53)^2 max |a_j|^2
         int myrot = 0;
-        for (int rd = 0; rd < qq - 1; rd++) {
+        // rotate the pair (top, bot) of this group; log it as pair grp of round rd
+        auto rotate = [&](int rd) {
             double cs = 1.0, sn = 0.0;
-            if (act) {
-                double g0 = 0.0, g1 = 0.0;
+            double g0 = 0.0, g1 = 0.0;
 #pragma unroll
-                for (int v = 0; v < NG; v += 2) {
-                    g0 = fma(top[v], bot[v], g0);
-                    g1 = fma(top[v + 1], bot[v + 1], g1);
+            for (int v = 0; v < NG; v += 2) {
+                g0 = fma(top[v], bot[v], g0);
+                g1 = fma(top[v + 1], bot[v + 1], g1);
+            }
+            const double ga = gsum_g<LP>(g0 + g1, gm);
+            if (ga != 0.0 && al > thr2 && be > thr2 && ga * ga > tol2 * (al * be)) {
+                const double dd = be - al, g2 = 2.0 * ga;
+                const double ri = rsqrt(fma(dd, dd, g2 * g2));
+                const double hc = fma(0.5 * fabs(dd), ri, 0.5);
+                const double ic = rsqrt(hc);
+                cs = hc * ic;
+                sn = 0.5 * copysign(1.0, dd) * g2 * ri * ic;
+                const double t = sn * ic;
+#pragma unroll
+                for (int v = 0; v < NG; v++) {
+                    const double xa = top[v], xb = bot[v];
+                    top[v] = cs * xa - sn * xb;
+                    bot[v] = sn * xa + cs * xb;
                 }
-                const double ga = gsum_g<LP>(g0 + g1, gm);
-                if (ga != 0.0 && al > thr2 && be > thr2 && ga * ga > tol2 * (al * be)) {
-                    const double dd = be - al, g2 = 2.0 * ga;
-                    const double ri = rsqrt(fma(dd, dd, g2 * g2));
-                    const double hc = fma(0.5 * fabs(dd), ri, 0.5);
-                    const double ic = rsqrt(hc);
-                    cs = hc * ic;
-                    sn = 0.5 * copysign(1.0, dd) * g2 * ri * ic;
-                    const double t = sn * ic;
+                al = al - t * ga;
+                be = be + t * ga;
+                myrot |= (ga * ga > 1e-16 * (al * be)) ? 3 : 1;
+            }
+            if (p == 0) rot[((long long)sw * (CT + 1) + rd) * npair + grp] = make_double2(cs, sn);
+        };
+        if (stat) {
+            // levels of block size hb = G, G / 2, ..., 1 (see stat_cols)
+            int rd = 0;
+            for (int hb = G; hb >= 1; hb >>= 1) {
+                const int i = grp & (hb - 1);
+                const bool cross = hb > GPW;  // the ring of hb pairs spans warps
+                const int wpb = cross ? hb / GPW : 1, wbase = warp - warp % wpb;
+                const int src = cross ? ((lane + LP) & 31) : ((i + 1 == hb) ? lane - (hb - 1) * LP : lane + LP);
+                for (int s = 0; s < hb; s++, rd++) {
+                    if (act) rotate(rd);
+                    if (hb == 1) continue;
+                    // second columns one pair back along the ring: within the
+                    // warp by shuffles, across warps through shared memory
+                    double* xb0 = xch + (long long)buf * NW * 2 * LP * (NG + 1);
+                    if (cross && gw == 0) {
+                        double* d = xb0 + (warp * 2 * LP + p) * (NG + 1);
+#pragma unroll
+                        for (int v = 0; v < NG; v++) d[v] = bot[v];
+                        d[NG] = be;
+                    }
+                    double nb[NG];
+#pragma unroll
+                    for (int v = 0; v < NG; v++) nb[v] = __shfl_sync(0xffffffffu, bot[v], src);
+                    double nbe = __shfl_sync(0xffffffffu, be, src);
+                    if (cross) {
+                        __syncthreads();
+                        if (gw == GPW - 1) {
+                            const int wn = wbase + (warp - wbase + 1) % wpb;
+                            const double* sx = xb0 + (wn * 2 * LP + p) * (NG + 1);
+#pragma unroll
+                            for (int v = 0; v < NG; v++) nb[v] = sx[v];
+                            nbe = sx[NG];
+                        }
+                        buf ^= 1;
+                    }
+#pragma unroll
+                    for (int v = 0; v < NG; v++) bot[v] = nb[v];
+                    be = nbe;
+                }
+                if (hb >= 2) {
+                    // split: pair i < h takes the first column of pair i + h
+                    // as its second, pair i + h the second column of pair i
+                    // as its first (h = hb / 2), through shared memory
+                    const int h = hb >> 1;
+                    const bool lo = i < h;
+                    double* d = Lc + ((long long)grp * LP + p) * (NG + 1);
+                    if (act) {
+#pragma unroll
+                        for (int v = 0; v < NG; v++) d[v] = lo ? bot[v] : top[v];
+                        d[NG] = lo ? be : al;
+                    }
+                    __syncthreads();
+                    if (act) {
+                        const double* sx = Lc + ((long long)(grp ^ h) * LP + p) * (NG + 1);
+                        if (lo) {
+#pragma unroll
+                            for (int v = 0; v < NG; v++) bot[v] = sx[v];
+                            be = sx[NG];
+                        } else {
+#pragma unroll
+                            for (int v = 0; v < NG; v++) top[v] = sx[v];
+                            al = sx[NG];
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+            // back to the first arrangement: pair g holds columns 2g, 2g + 1
+            // after the last level; it starts the next sweep with g, G + g
+            if (act) {
+#pragma unroll
+                for (int v = 0; v < NG; v++) {
+                    Lc[(2 * grp) * S + p + LP * v] = top[v];
+                    Lc[(2 * grp + 1) * S + p + LP * v] = bot[v];
+                }
+            }
+            __syncthreads();
+            if (act) {
+#pragma unroll
+                for (int v = 0; v < NG; v++) {
+                    top[v] = Lc[grp * S + p + LP * v];
+                    bot[v] = Lc[(G + grp) * S + p + LP * v];
+                }
+            }
+        } else {
+            for (int rd = 0; rd < qq - 1; rd++) {
+                if (act) rotate(rd);
+                // move the columns to the next round's pairs
+                double* xb0 = xch + (long long)buf * NW * 2 * LP * (NG + 1);
+                if (gw == 0) {  // this warp's first top: to the previous warp's last group
+                    double* d = xb0 + ((warp * 2 + 0) * LP + p) * (NG + 1);
+#pragma unroll
+                    for (int v = 0; v < NG; v++) d[v] = top[v];
+                    d[NG] = al;
+                }
+                if (gw == GPW - 1) {  // this warp's last bottom: to the next warp's first group
+                    double* d = xb0 + ((warp * 2 + 1) * LP + p) * (NG + 1);
+#pragma unroll
+                    for (int v = 0; v < NG; v++) d[v] = bot[v];
+                    d[NG] = be;
+                }
+                double rt[NG], rb[NG];
+#pragma unroll
+                for (int v = 0; v < NG; v++) {
+                    rt[v] = __shfl_down_sync(0xffffffffu, top[v], LP);  // top of group + 1
+                    rb[v] = __shfl_up_sync(0xffffffffu, bot[v], LP);    // bottom of group - 1
+                }
+                double rta = __shfl_down_sync(0xffffffffu, al, LP);
+                double rbb = __shfl_up_sync(0xffffffffu, be, LP);
+                __syncthreads();
+                if (gw == GPW - 1 && warp + 1 < NW) {
+                    const double* sx = xb0 + (((warp + 1) * 2 + 0) * LP + p) * (NG + 1);
+#pragma unroll
+                    for (int v = 0; v < NG; v++) rt[v] = sx[v];
+                    rta = sx[NG];
+                }
+                if (gw == 0 && warp > 0) {
+                    const double* sx = xb0 + (((warp - 1) * 2 + 1) * LP + p) * (NG + 1);
+#pragma unroll
+                    for (int v = 0; v < NG; v++) rb[v] = sx[v];
+                    rbb = sx[NG];
+                }
+                buf ^= 1;
+                if (G == 1) {
+                    // one pair: both positions are fixed points of the circle order
+                } else if (grp == 0) {  // top fixed, bottom <- top of pair 1
+#pragma unroll
+                    for (int v = 0; v < NG; v++) bot[v] = rt[v];
+                    be = rta;
+                } else if (grp == G - 1) {  // top <- own bottom, bottom <- bottom of pair G - 2
 #pragma unroll
                     for (int v = 0; v < NG; v++) {
-                        const double xa = top[v], xb = bot[v];
-                        top[v] = cs * xa - sn * xb;
-                        bot[v] = sn * xa + cs * xb;
+                        top[v] = bot[v];
+                        bot[v] = rb[v];
                     }
-                    al = al - t * ga;
-                    be = be + t * ga;
-                    myrot |= (ga * ga > 1e-16 * (al * be)) ? 3 : 1;
+                    al = be;
+                    be = rbb;
+                } else if (act) {
+#pragma unroll
+                    for (int v = 0; v < NG; v++) {
+                        top[v] = rt[v];
+                        bot[v] = rb[v];
+                    }
+                    al = rta;
+                    be = rbb;
                 }
-                if (p == 0) rot[((long long)sw * (CT + 1) + rd) * npair + grp] = make_double2(cs, sn);
-            }
-            // move the columns to the next round's pairs
-            double* xb0 = xch + (long long)buf * NW * 2 * LP * (NG + 1);
-            const int gw = lane / LP;  // group within the warp (0 .. GPW - 1)
-            if (gw == 0) {             // this warp's first top: to the previous warp's last group
-                double* d = xb0 + ((warp * 2 + 0) * LP + p) * (NG + 1);
-#pragma unroll
-                for (int v = 0; v < NG; v++) d[v] = top[v];
-                d[NG] = al;
-            }
-            if (gw == GPW - 1) {  // this warp's last bottom: to the next warp's first group
-                double* d = xb0 + ((warp * 2 + 1) * LP + p) * (NG + 1);
-#pragma unroll
-                for (int v = 0; v < NG; v++) d[v] = bot[v];
-                d[NG] = be;
-            }
-            double rt[NG], rb[NG];
-#pragma unroll
-            for (int v = 0; v < NG; v++) {
-                rt[v] = __shfl_down_sync(0xffffffffu, top[v], LP);  // top of group + 1
-                rb[v] = __shfl_up_sync(0xffffffffu, bot[v], LP);    // bottom of group - 1
-            }
-            double rta = __shfl_down_sync(0xffffffffu, al, LP);
-            double rbb = __shfl_up_sync(0xffffffffu, be, LP);
-            __syncthreads();
-            if (gw == GPW - 1 && warp + 1 < NW) {
-                const double* sx = xb0 + (((warp + 1) * 2 + 0) * LP + p) * (NG + 1);
-#pragma unroll
-                for (int v = 0; v < NG; v++) rt[v] = sx[v];
-                rta = sx[NG];
-            }
-            if (gw == 0 && warp > 0) {
-                const double* sx = xb0 + (((warp - 1) * 2 + 1) * LP + p) * (NG + 1);
-#pragma unroll
-                for (int v = 0; v < NG; v++) rb[v] = sx[v];
-                rbb = sx[NG];
-            }
-            buf ^= 1;
-            if (G == 1) {
-                // one pair: both positions are fixed points of the circle order
-            } else if (grp == 0) {  // top fixed, bottom <- top of pair 1
-#pragma unroll
-                for (int v = 0; v < NG; v++) bot[v] = rt[v];
-                be = rta;
-            } else if (grp == G - 1) {  // top <- own bottom, bottom <- bottom of pair G - 2
-#pragma unroll
-                for (int v = 0; v < NG; v++) {
-                    top[v] = bot[v];
-                    bot[v] = rb[v];
-                }
-                al = be;
-                be = rbb;
-            } else if (act) {
-#pragma unroll
-                for (int v = 0; v < NG; v++) {
-                    top[v] = rt[v];
-                    bot[v] = rb[v];
-                }
-                al = rta;
-                be = rbb;
             }
         }
         if (myrot) atomicOr(&s_rot, myrot);
@@ -659,13 +770,14 @@ __global__ void __launch_bounds__(ring_nt<CT, LP>()) k_svd_ring(Plan pl, double*
         __syncthreads();  // s_rot is reset at the next sweep's start
     }
     if (!conv && tid == 0) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
-    // the columns back to shared memory: after R rounds of a sweep (R = qq - 1
-    // per sweep) the pairs hold circle_col(g, 0) again, i.e. g and qq - 1 - g
+    // the columns back to shared memory: each sweep ends with pair g holding
+    // columns g and qq - 1 - g (circle) or g and G + g (stationary ring)
     if (act) {
+        const int cb = stat ? G + grp : qq - 1 - grp;
 #pragma unroll
         for (int v = 0; v < NG; v++) {
             Lc[grp * S + p + LP * v] = top[v];
-            Lc[(qq - 1 - grp) * S + p + LP * v] = bot[v];
+            Lc[cb * S + p + LP * v] = bot[v];
         }
     }
     __syncthreads();
@@ -718,6 +830,7 @@ __global__ void __launch_bounds__(ring_nt<CT, LP>()) k_svd_ring(Plan pl, double*
         info->rank = rank;
         info->nsv = nsv;
         info->sweeps = sweeps;
+        info->order = stat ? 1 : 0;
         double tail = 0.0;
         for (int j = rank; j < q; j++) tail += s_sig[s_ord[j]] * s_sig[s_ord[j]];
         info->tail = tail;
@@ -766,7 +879,7 @@ __device__ void svd_replay_body(const Plan& pl, double* ws, const Info* info, in
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int row = bx * 8 + warp;
     if (info->status) return;
-    const int q = info->q, qq = q + (q & 1), sweeps = info->sweeps, rank = info->rank;
+    const int q = info->q, qq = q + (q & 1), sweeps = info->sweeps, rank = info->rank, order = info->order;
     for (int j = lane; j < SR; j += 32) vrow[j] = (j == row) ? 1.0 : 0.0;
     const double2* rot = (const double2*)(ws + pl.o_rot);
     for (int sw = 0; sw < sweeps; sw++) {
@@ -780,7 +893,13 @@ __device__ void svd_replay_body(const Plan& pl, double* ws, const Info* info, in
                 for (int i = lane; i < qq / 2; i += 32) {
                     const double2 r = tab[rd * npair + i];
                     if (r.y != 0.0) {
-                        const int pc = circle_col(i, rd, qq), qc = circle_col(qq - 1 - i, rd, qq);
+                        int pc, qc;
+                        if (order == 1) {
+                            stat_cols(i, rd, qq / 2, &pc, &qc);
+                        } else {
+                            pc = circle_col(i, rd, qq);
+                            qc = circle_col(qq - 1 - i, rd, qq);
+                        }
                         const double x = vrow[pc], y = vrow[qc];
                         vrow[pc] = r.x * x - r.y * y;
                         vrow[qc] = r.y * x + r.x * y;

@@ -61,7 +61,7 @@ struct Info {
     int sweeps;       // Jacobi sweeps
     int nsv;          // numerical rank kept by the SVD stage
     int status;
-    int pad;
+    int order;        // Jacobi pair order of the recorded rotations (0 circle, 1 stationary ring)
     double tail;      // retained tail sum (diagnostic)
 };
 
