@@ -40,12 +40,12 @@ namespace gq {
 
 constexpr int NT = 256;
 constexpr int CB = 64;                 // column bound
-constexpr int XP = CB + 2;             // pitch of the rows in shared memory (even: 16-byte pairs)
+constexpr int XP = CB + 8;             // pitch of the rows in shared memory: 8 mod 16 doubles, so the
+                                       // four rows of an mma fragment load fall in the two halves of the banks
 constexpr int RP = CB + 2;             // pitch of a factor R (row-major, upper triangular)
 constexpr int GP = CB + 1;             // pitch of the Gram matrix of the deciding CTA
 constexpr int TS = CB / 8;             // Gram tiles are TS x TS, 8 x 8 of them
 constexpr int UP = 36 * TS * TS;       // entries of the 36 upper tiles
-constexpr int NG = 7;                  // row groups of the Gram threads (36 tiles x 7 = 252)
 constexpr int GROUP = 8;               // CTAs summed by the first level
 constexpr int RPB_MAX = 112;           // rows per CTA
 constexpr int RPB_MIN = 16;
@@ -56,11 +56,11 @@ constexpr double TAU = 1e-13;
 constexpr double FIRST = 1e-7;
 constexpr double FIRST_DONE = 1e-8;
 constexpr double U = 1.1102230246251565e-16;
-constexpr size_t SMEM = sizeof(double) * ((size_t)RPB_MAX * XP + (size_t)NG * UP);
 constexpr int FSZ = CB * RP + CB;      // a factor and its inverse pivots
-static_assert(CB * GP + 2 * FSZ + 64 <= NG * UP, "decision arrays fit the Gram scratch");
+constexpr int SCR = CB * GP + 2 * FSZ + 64;  // Gram, two candidate factors, row broadcasts of the deciding CTA
+constexpr size_t SMEM = sizeof(double) * ((size_t)RPB_MAX * XP + (size_t)SCR);
 static_assert(CB * GP <= FSZ, "the accumulated R fits a factor buffer");
-static_assert(CB * RP + CB <= NG * UP, "factor fits the Gram scratch");
+static_assert(CB * RP + CB <= SCR, "factor fits the scratch");
 
 enum { RUN = 0, DONE = 1, FALLBACK = 2, FINISH = 4, CHOL = 8 };
 
@@ -280,19 +280,35 @@ __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int
     __syncthreads();
     {
         const unsigned xs0 = (unsigned)__cvta_generic_to_shared(Xs);
-        const int tot = h * c;
-        for (int f = tid; f < tot; f += NT) {
-            int row, col;
-            if (src.rs == 1) {  // column-major: a column's rows are contiguous
-                col = f / h;
-                row = f - col * h;
-            } else {  // row-major rows of c
-                row = f / c;
-                col = f - row * c;
+        if (src.rs == 1) {
+            // column-major: a warp copies 4 rows x 8 columns at a time (32
+            // contiguous bytes of each column; the 4 rows fall in different
+            // bank halves)
+            const int nrb = (h + 3) / 4, ncb = (c + 7) / 8;
+            const int lr = (tid & 31) & 3, lc = (tid & 31) >> 2;
+            for (int t = tid >> 5; t < nrb * ncb; t += NT / 32) {
+                const int cb = t / nrb, rb = t - cb * nrb;
+                const int row = rb * 4 + lr, col = cb * 8 + lc;
+                if (row < h && col < c) {
+                    const double* gp = src.p + (long long)(r0 + row) + (long long)col * src.cs;
+                    const unsigned sa = xs0 + 8u * (unsigned)(row * XP + col);
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gp) : "memory");
+                }
             }
-            const double* gp = src.p + (long long)(r0 + row) * src.rs + (long long)col * src.cs;
-            const unsigned sa = xs0 + 8u * (unsigned)(row * XP + col);
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gp) : "memory");
+        } else {  // row-major rows of c: element f = row c + col, stepped without divisions
+            const int dq = NT / c, dr = NT - dq * c;
+            int row = tid / c, col = tid - row * c;
+            for (; row < h;) {
+                const double* gp = src.p + (long long)(r0 + row) * src.rs + (long long)col * src.cs;
+                const unsigned sa = xs0 + 8u * (unsigned)(row * XP + col);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gp) : "memory");
+                row += dq;
+                col += dr;
+                if (col >= c) {
+                    col -= c;
+                    row++;
+                }
+            }
         }
         asm volatile("cp.async.wait_all;\n" ::: "memory");
     }
@@ -300,64 +316,68 @@ __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int
     if (stage >= 1) {
         if (tid < h) row_solve(Xs + tid * XP, sScr, sScr + CB * RP, c);
         __syncthreads();
-        const int tot = h * c;
-        for (int f = tid; f < tot; f += NT) {
-            int row, col;
-            if (Qv.rs == 1) {
-                col = f / h;
-                row = f - col * h;
-            } else {
-                row = f / c;
-                col = f - row * c;
+        if (Qv.rs == 1) {  // column-major, in the load's 4 x 8 warp tiles
+            const int nrb = (h + 3) / 4, ncb = (c + 7) / 8;
+            const int lr = (tid & 31) & 3, lc = (tid & 31) >> 2;
+            for (int t = tid >> 5; t < nrb * ncb; t += NT / 32) {
+                const int cb = t / nrb, rb = t - cb * nrb;
+                const int row = rb * 4 + lr, col = cb * 8 + lc;
+                if (row < h && col < c) Qv.p[(long long)(r0 + row) + (long long)col * Qv.cs] = Xs[row * XP + col];
             }
-            Qv.p[(long long)(r0 + row) * Qv.rs + (long long)col * Qv.cs] = Xs[row * XP + col];
+        } else {
+            const int dq = NT / c, dr = NT - dq * c;
+            int row = tid / c, col = tid - row * c;
+            for (; row < h;) {
+                Qv.p[(long long)(r0 + row) * Qv.rs + (long long)col * Qv.cs] = Xs[row * XP + col];
+                row += dq;
+                col += dr;
+                if (col >= c) {
+                    col -= c;
+                    row++;
+                }
+            }
         }
         if (s_state == FINISH) return;  // the last factor is applied: Q is final
     }
-    // partial Gram matrix (upper tiles) of this CTA's rows
+    // partial Gram matrix (upper 8 x 8 tiles) of this CTA's rows on the FP64
+    // tensor cores: warp w accumulates tiles w, w + 8, ... over all rows, four
+    // rows per mma.m8n8k4 (A = the tile's row-block columns transposed, B =
+    // its column-block columns), and writes them straight to its partial
     {
-        const int q = tid % 36, grp = tid / 36;
-        int ti, tj;
-        cq::upper_tile(q, &ti, &tj);
-        ti *= TS;
-        tj *= TS;
-        if (grp < NG) {
-            double acc[TS][TS];
+        const int warp = tid >> 5, lane = tid & 31;
+        const int li = lane >> 2, lk = lane & 3;
+        constexpr int NWP = NT / 32, TPW = (36 + NWP - 1) / NWP;
+        double c0[TPW], c1[TPW];
+        int oa[TPW], ob[TPW];
 #pragma unroll
-            for (int a = 0; a < TS; a++)
+        for (int t = 0; t < TPW; t++) {
+            int ti = 0, tj = 0;
+            if (warp + NWP * t < 36) cq::upper_tile(warp + NWP * t, &ti, &tj);
+            oa[t] = ti * TS + li;
+            ob[t] = tj * TS + li;
+            c0[t] = 0.0;
+            c1[t] = 0.0;
+        }
+        for (int r = 0; r < h; r += 4) {
+            const int row = r + lk;
+            const double* xr = Xs + row * XP;
+            const bool ok = row < h;
 #pragma unroll
-                for (int bb = 0; bb < TS; bb++) acc[a][bb] = 0.0;
-            for (int r = grp; r < h; r += NG) {
-                double xa[TS], xb[TS];
-#pragma unroll
-                for (int a = 0; a < TS; a += 2) {
-                    const double2 va = *(const double2*)(Xs + r * XP + ti + a);
-                    const double2 vb = *(const double2*)(Xs + r * XP + tj + a);
-                    xa[a] = va.x;
-                    xa[a + 1] = va.y;
-                    xb[a] = vb.x;
-                    xb[a + 1] = vb.y;
+            for (int t = 0; t < TPW; t++) {
+                if (warp + NWP * t < 36) {
+                    const double av = ok ? xr[oa[t]] : 0.0;
+                    const double bv = ok ? xr[ob[t]] : 0.0;
+                    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                                 : "+d"(c0[t]), "+d"(c1[t])
+                                 : "d"(av), "d"(bv));
                 }
-#pragma unroll
-                for (int a = 0; a < TS; a++)
-#pragma unroll
-                    for (int bb = 0; bb < TS; bb++) acc[a][bb] = fma(xa[a], xb[bb], acc[a][bb]);
             }
-#pragma unroll
-            for (int a = 0; a < TS; a++)
-#pragma unroll
-                for (int bb = 0; bb < TS; bb++) sScr[grp * UP + q * TS * TS + a * TS + bb] = acc[a][bb];
         }
-    }
-    __syncthreads();
-    {
         double* P = g.part + (long long)b * UP;
-        for (int u = tid; u < UP; u += NT) {
-            double v = sScr[u];
 #pragma unroll
-            for (int g2 = 1; g2 < NG; g2++) v += sScr[g2 * UP + u];
-            P[u] = v;
-        }
+        for (int t = 0; t < TPW; t++)
+            if (warp + NWP * t < 36)
+                *(double2*)(P + (warp + NWP * t) * TS * TS + li * TS + 2 * lk) = make_double2(c0[t], c1[t]);
     }
     // first level: the last CTA of each group sums the group's partials
     const int ngroups = (nb + GROUP - 1) / GROUP;

@@ -535,17 +535,19 @@ __global__ void __launch_bounds__(ring_nt<CT, LP>(), 1) k_svd_ring(Plan pl, doub
     if (info->status) return;
     const int c = info->c, q = info->q;
     const int qq = q + (q & 1);
-    const int G = qq / 2;  // active pairs (one per group)
-    const bool act = grp < G;
+    const int G = qq / 2;  // pairs of a round
     const double* R = ws + pl.o_Rn;  // root factor, row-major CT x CT; L = R^T: column j = row j of R
-    // stationary-ring order when the pair count is a power of two (one column
-    // of each pair moves per round), circle order otherwise
-    const bool stat = G >= 2 && (G & (G - 1)) == 0;
-    // round 0: pair g holds columns g (top) and qq - 1 - g (circle) or G + g
+    // stationary-ring order (one column of each pair moves per round) over G2
+    // pairs, G rounded up to a power of two (the extra columns are zero and
+    // never rotated); circle order for a single pair
+    const bool stat = G >= 2;
+    const int G2 = stat ? 1 << (32 - __clz(G - 1)) : G;
+    const bool act = grp < G2;
+    // round 0: pair g holds columns g (top) and qq - 1 - g (circle) or G2 + g
     // (stationary ring) (bottom)
     double top[NG], bot[NG];
     {
-        const int ct = grp, cb = stat ? G + grp : qq - 1 - grp;
+        const int ct = grp, cb = stat ? G2 + grp : qq - 1 - grp;
 #pragma unroll
         for (int v = 0; v < NG; v++) {
             const int t = p + LP * v;
@@ -612,9 +614,9 @@ __global__ void __launch_bounds__(ring_nt<CT, LP>(), 1) k_svd_ring(Plan pl, doub
             if (p == 0) rot[((long long)sw * (CT + 1) + rd) * npair + grp] = make_double2(cs, sn);
         };
         if (stat) {
-            // levels of block size hb = G, G / 2, ..., 1 (see stat_cols)
+            // levels of block size hb = G2, G2 / 2, ..., 1 (see stat_cols)
             int rd = 0;
-            for (int hb = G; hb >= 1; hb >>= 1) {
+            for (int hb = G2; hb >= 1; hb >>= 1) {
                 const int i = grp & (hb - 1);
                 const bool cross = hb > GPW;  // the ring of hb pairs spans warps
                 const int wpb = cross ? hb / GPW : 1, wbase = warp - warp % wpb;
@@ -679,7 +681,7 @@ __global__ void __launch_bounds__(ring_nt<CT, LP>(), 1) k_svd_ring(Plan pl, doub
                 }
             }
             // back to the first arrangement: pair g holds columns 2g, 2g + 1
-            // after the last level; it starts the next sweep with g, G + g
+            // after the last level; it starts the next sweep with g, G2 + g
             if (act) {
 #pragma unroll
                 for (int v = 0; v < NG; v++) {
@@ -692,7 +694,7 @@ __global__ void __launch_bounds__(ring_nt<CT, LP>(), 1) k_svd_ring(Plan pl, doub
 #pragma unroll
                 for (int v = 0; v < NG; v++) {
                     top[v] = Lc[grp * S + p + LP * v];
-                    bot[v] = Lc[(G + grp) * S + p + LP * v];
+                    bot[v] = Lc[(G2 + grp) * S + p + LP * v];
                 }
             }
         } else {
@@ -771,9 +773,9 @@ __global__ void __launch_bounds__(ring_nt<CT, LP>(), 1) k_svd_ring(Plan pl, doub
     }
     if (!conv && tid == 0) PTT_STATUS_SET(status, PTT_ERR_NUMERIC);
     // the columns back to shared memory: each sweep ends with pair g holding
-    // columns g and qq - 1 - g (circle) or g and G + g (stationary ring)
+    // columns g and qq - 1 - g (circle) or g and G2 + g (stationary ring)
     if (act) {
-        const int cb = stat ? G + grp : qq - 1 - grp;
+        const int cb = stat ? G2 + grp : qq - 1 - grp;
 #pragma unroll
         for (int v = 0; v < NG; v++) {
             Lc[grp * S + p + LP * v] = top[v];
@@ -880,22 +882,26 @@ __device__ void svd_replay_body(const Plan& pl, double* ws, const Info* info, in
     const int row = bx * 8 + warp;
     if (info->status) return;
     const int q = info->q, qq = q + (q & 1), sweeps = info->sweeps, rank = info->rank, order = info->order;
+    // pairs and rounds of a sweep: the stationary ring runs over qq / 2
+    // rounded up to a power of two
+    const int npr = (order == 1 && qq >= 4) ? 1 << (32 - __clz(qq / 2 - 1)) : qq / 2;
+    const int nrd = 2 * npr - 1;
     for (int j = lane; j < SR; j += 32) vrow[j] = (j == row) ? 1.0 : 0.0;
     const double2* rot = (const double2*)(ws + pl.o_rot);
     for (int sw = 0; sw < sweeps; sw++) {
         __syncthreads();
         const long long base = (long long)sw * (CT + 1) * npair;
-        const int cnt = (qq - 1) * npair;
+        const int cnt = nrd * npair;
         for (int e = threadIdx.x; e < cnt; e += blockDim.x) tab[e] = rot[base + e];
         __syncthreads();
         if (row < q) {
-            for (int rd = 0; rd < qq - 1; rd++) {
-                for (int i = lane; i < qq / 2; i += 32) {
+            for (int rd = 0; rd < nrd; rd++) {
+                for (int i = lane; i < npr; i += 32) {
                     const double2 r = tab[rd * npair + i];
                     if (r.y != 0.0) {
                         int pc, qc;
                         if (order == 1) {
-                            stat_cols(i, rd, qq / 2, &pc, &qc);
+                            stat_cols(i, rd, npr, &pc, &qc);
                         } else {
                             pc = circle_col(i, rd, qq);
                             qc = circle_col(qq - 1 - i, rd, qq);
