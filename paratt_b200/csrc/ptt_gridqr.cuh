@@ -100,33 +100,48 @@ __host__ __forceinline__ int ctas(long long mcap, int rpb) {
     return (int)(b < 1 ? 1 : b);
 }
 
-// x <- x R^{-1} for one row held in shared memory (R upper triangular, pitch
-// RP, zero below the diagonal and beyond c; inverse pivots in iv).  The row
-// lives in registers; each R entry is a broadcast 16-byte load.
-__device__ __forceinline__ void row_solve(double* xs, const double* R, const double* iv, int c) {
-    double x[CB];
-#pragma unroll
-    for (int j = 0; j < CB; j += 2) {
-        const double2 v = *(const double2*)(xs + j);
-        x[j] = v.x;
-        x[j + 1] = v.y;
-    }
-#pragma unroll
-    for (int j = 0; j < CB; j++) {
-        if (j < c) {
-            const double y = x[j] * iv[j];
-            x[j] = y;
-            const double* Rj = R + j * RP;
-#pragma unroll
-            for (int l = (j + 1) & ~1; l < CB; l += 2) {
-                const double2 r2 = *(const double2*)(Rj + l);
-                if (l > j) x[l] = fma(-y, r2.x, x[l]);
-                x[l + 1] = fma(-y, r2.y, x[l + 1]);
+// x <- x R^{-1} for the CTA's rows (h of them, zero rows up to a multiple of
+// 8), one warp per 8-row tile, by 8-column blocks in order: the update of
+// block J by the solved blocks, X_J - Y_{<J} R_{<J,J}, on the FP64 tensor
+// cores (mma.m8n8k4, four columns of Y a step), then forward substitution in
+// the 8 x 8 diagonal block, the row's four lanes passing each solved entry by
+// a shuffle.  Rows are independent, so a warp needs no barrier.  R upper
+// triangular (pitch RP), zero outside the c x c triangle; iv = inverse
+// pivots, zero beyond c.
+__device__ __forceinline__ void tile_solve(double* Xs, int h, const double* R, const double* iv, int c) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int li = lane >> 2, lk = lane & 3;
+    const int ntile = (h + 7) >> 3, nb = (c + 7) >> 3;
+    for (int t = warp; t < ntile; t += NT / 32) {
+        double* xr = Xs + (t * 8 + li) * XP;  // this lane's row
+        for (int J = 0; J < nb; J++) {
+            const double2 cv = *(const double2*)(xr + 8 * J + 2 * lk);
+            double c0 = cv.x, c1 = cv.y;  // columns 8J + 2lk, 8J + 2lk + 1
+            for (int kk = 0; kk < 2 * J; kk++) {
+                const double av = -xr[4 * kk + lk];
+                const double bv = R[(4 * kk + lk) * RP + 8 * J + li];
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                             : "+d"(c0), "+d"(c1)
+                             : "d"(av), "d"(bv));
             }
+            const double* Rb = R + 8 * J * RP + 8 * J;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int own = j >> 1;
+                if (lk == own) {
+                    if (j & 1)
+                        c1 *= iv[8 * J + j];
+                    else
+                        c0 *= iv[8 * J + j];
+                }
+                const double y = __shfl_sync(0xffffffffu, (j & 1) ? c1 : c0, (lane & ~3) | own);
+                if (2 * lk > j) c0 = fma(-y, Rb[j * RP + 2 * lk], c0);
+                if (2 * lk + 1 > j) c1 = fma(-y, Rb[j * RP + 2 * lk + 1], c1);
+            }
+            *(double2*)(xr + 8 * J + 2 * lk) = make_double2(c0, c1);
+            __syncwarp();
         }
     }
-#pragma unroll
-    for (int j = 0; j < CB; j += 2) *(double2*)(xs + j) = make_double2(x[j], x[j + 1]);
 }
 
 // Cholesky of one 32-column panel by one warp, lane = column: g[t] holds
@@ -266,7 +281,7 @@ __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int
     }
     const View& src = (stage <= 1) ? A : Qv;
     // this CTA's rows (zero beyond c), every element in flight by cp.async
-    for (int e = tid; e < h * XP; e += NT) Xs[e] = 0.0;
+    for (int e = tid; e < ((h + 7) & ~7) * XP; e += NT) Xs[e] = 0.0;  // whole 8-row tiles
     if (stage >= 1) {  // the factor of the previous stage (all loads in flight first)
         const double* F = g.rec + O_FAC;
         constexpr int FL = CB * RP + CB, FPT = (FL + NT - 1) / NT;
@@ -314,7 +329,7 @@ __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int
     }
     __syncthreads();
     if (stage >= 1) {
-        if (tid < h) row_solve(Xs + tid * XP, sScr, sScr + CB * RP, c);
+        tile_solve(Xs, h, sScr, sScr + CB * RP, c);
         __syncthreads();
         if (Qv.rs == 1) {  // column-major, in the load's 4 x 8 warp tiles
             const int nrb = (h + 3) / 4, ncb = (c + 7) / 8;
