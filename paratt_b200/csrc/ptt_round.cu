@@ -862,6 +862,12 @@ __global__ void __launch_bounds__(ring_nt<CT, LP>(), 1) k_svd_ring(Plan pl, doub
     }
 }
 
+// The ring Jacobi is used for bonds of more than SVD_RING_MIN columns; below
+// that the shared-memory Jacobi was faster on one B200 (the reaction-Burgers
+// steps, whose bonds have <= ~40 columns: 105 vs 101 ms per plain step),
+// above it the ring (64 columns: 13.2 vs 21.7 ms for 39 bonds).
+constexpr int SVD_RING_MIN = 48;
+
 template <int CT, int LP = 4>
 static size_t ring_smem() {
     constexpr int NW = ring_nt<CT, LP>() / 32;
@@ -870,7 +876,8 @@ static size_t ring_smem() {
 
 // Rebuild rows of V (q x q, V = product of the recorded rotations) and write
 // V_r = V[:, order[0:rank]] into Bn[root].  One warp per row; each sweep's
-// rotation table is staged in shared memory once per block.
+// rotation table is staged in shared memory once per block, the column pair
+// of each (round, pair) slot is tabulated once for all sweeps.
 __device__ void svd_replay_body(const Plan& pl, double* ws, const Info* info, int bx) {
     extern __shared__ double sm[];
     const int CT = pl.CT, KC = pl.KC;
@@ -886,6 +893,21 @@ __device__ void svd_replay_body(const Plan& pl, double* ws, const Info* info, in
     // rounded up to a power of two
     const int npr = (order == 1 && qq >= 4) ? 1 << (32 - __clz(qq / 2 - 1)) : qq / 2;
     const int nrd = 2 * npr - 1;
+    // the column pair of every (round, pair) slot, once for all sweeps
+    unsigned char* pcol = (unsigned char*)(tab + (CT + 1) * npair);
+    unsigned char* qcol = pcol + (CT + 1) * npair;
+    for (int e = threadIdx.x; e < nrd * npr; e += blockDim.x) {
+        const int rd = e / npr, i = e - (e / npr) * npr;
+        int pc, qc;
+        if (order == 1) {
+            stat_cols(i, rd, npr, &pc, &qc);
+        } else {
+            pc = circle_col(i, rd, qq);
+            qc = circle_col(qq - 1 - i, rd, qq);
+        }
+        pcol[rd * npair + i] = (unsigned char)pc;
+        qcol[rd * npair + i] = (unsigned char)qc;
+    }
     for (int j = lane; j < SR; j += 32) vrow[j] = (j == row) ? 1.0 : 0.0;
     const double2* rot = (const double2*)(ws + pl.o_rot);
     for (int sw = 0; sw < sweeps; sw++) {
@@ -899,13 +921,7 @@ __device__ void svd_replay_body(const Plan& pl, double* ws, const Info* info, in
                 for (int i = lane; i < npr; i += 32) {
                     const double2 r = tab[rd * npair + i];
                     if (r.y != 0.0) {
-                        int pc, qc;
-                        if (order == 1) {
-                            stat_cols(i, rd, npr, &pc, &qc);
-                        } else {
-                            pc = circle_col(i, rd, qq);
-                            qc = circle_col(qq - 1 - i, rd, qq);
-                        }
+                        const int pc = pcol[rd * npair + i], qc = qcol[rd * npair + i];
                         const double x = vrow[pc], y = vrow[qc];
                         vrow[pc] = r.x * x - r.y * y;
                         vrow[qc] = r.y * x + r.x * y;
@@ -1117,7 +1133,9 @@ static size_t svd_smem() {
 // 8 V rows + one sweep's rotation table ((CT+1) rounds x (CT+2)/2 pairs)
 template <int CT>
 static size_t replay_smem() {
-    return sizeof(double) * (8 * (size_t)(CT + 2) + 2 * (size_t)(CT + 1) * ((CT + 2) / 2));
+    // 8 rows of V, one sweep's rotations, the two column tables (bytes)
+    return sizeof(double) * (8 * (size_t)(CT + 2) + 2 * (size_t)(CT + 1) * ((CT + 2) / 2)) +
+           2 * (size_t)(CT + 1) * ((CT + 2) / 2);
 }
 
 template <int CT>
@@ -1298,7 +1316,7 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
         if ((rc = launch_factor<CT>(c, x, i, RIGHT_T, pl, ws, g, mcap))) return rc;
         const int mr = maxr ? maxr[i] : rk[i];
         ptt_time_begin(c, PTT_TIME_SVD);
-        if (CT <= 64)  // columns in registers
+        if (CT <= 64 && rk[i] > SVD_RING_MIN)  // columns in registers
             PTT_CUDA(ptt_launch(c, k_svd_ring<CT <= 64 ? CT : 64>, dim3(1), dim3(ring_nt<CT <= 64 ? CT : 64>()),
                                 ring_smem<CT <= 64 ? CT : 64>(), pl, ws, delta, mr, i, c->d_status));
         else
@@ -1596,7 +1614,7 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
                 Wmax = Wr[i] > Wmax ? Wr[i] : Wmax;
                 const int mr = maxr ? maxr[i] : rk[i];
                 ptt_time_begin(c, PTT_TIME_SVD);
-                PTT_CUDA(ptt_launch(c, k_svd_ring<32>, dim3(1), dim3(ring_nt<32>()), ring_smem<32>(), pl, wsb, delta, mr, i,
+                PTT_CUDA(ptt_launch(c, k_svd_jacobi<32>, dim3(1), dim3(svd_nt<32>()), svd_smem<32>(), pl, wsb, delta, mr, i,
                                     c->d_status));
                 ptt_time_end(c, PTT_TIME_SVD);
                 PTT_LAUNCHED(c);
