@@ -264,49 +264,79 @@ __global__ void __launch_bounds__(NT, 1) k_cq_factor(const DevDesc* D, int k, in
         asm volatile("cp.async.wait_all;\n" ::: "memory");
     }
     __syncthreads();
-    // Gram threads: upper tile q of the 8 x 8 grid, row group grp
-    const int q = tid % 36, grp = tid / 36;
-    int ti, tj;
-    upper_tile(q, &ti, &tj);
-    ti *= TS;
-    tj *= TS;
+    // Gram warps: rows [4 ks0, 4 ks1) of this CTA, every 8 x 8 tile of the
+    // NB column blocks (mma.m8n8k4: four rows a step, the block's fragment
+    // serves as A and as B)
+    constexpr int NB = CB / 8, NTL = NB * (NB + 1) / 2;
+    static_assert(4 * NTL * 64 <= NG * UP, "the warp tiles fit the Gram scratch");
+    const int warp = tid >> 5, lane = tid & 31, li = lane >> 2, lk = lane & 3;
+    const int nks = (h + 3) / 4;
+    const int ks0 = (nks * warp) / (NT / 32), ks1 = (nks * (warp + 1)) / (NT / 32);
     int dec = RUN, nst = 0, nshift = 0, stage = 0;
     for (stage = 0; stage < MAXST; stage++) {
         if (stage > 0) {  // Q_stage = Q_{stage-1} R_stage^{-1}
             for (int r = tid; r < h; r += 2 * NT) row_solve2<CB>(Xs + r * XP, Xs + (r + NT) * XP, r + NT < h, sR, c);
             __syncthreads();
         }
-        // partial Gram (upper tiles) of this CTA's rows
-        if (grp < NG) {
-            double acc[TS][TS];
+        // partial Gram of this CTA's rows on the FP64 tensor cores: each warp
+        // its rows, all tiles; warps w and w + 4 are added in shared memory,
+        // then the four sums in warp order into the grid layout of myP
+        {
+            double c0[NTL], c1[NTL];
 #pragma unroll
-            for (int a = 0; a < TS; a++)
-#pragma unroll
-                for (int b = 0; b < TS; b++) acc[a][b] = 0.0;
-            for (int r = grp; r < h; r += NG) {
-                double xa[TS], xb[TS];
-#pragma unroll
-                for (int a = 0; a < TS; a++) {
-                    xa[a] = Xs[r * XP + ti + a];
-                    xb[a] = Xs[r * XP + tj + a];
-                }
-#pragma unroll
-                for (int a = 0; a < TS; a++)
-#pragma unroll
-                    for (int b = 0; b < TS; b++) acc[a][b] = fma(xa[a], xb[b], acc[a][b]);
+            for (int t = 0; t < NTL; t++) {
+                c0[t] = 0.0;
+                c1[t] = 0.0;
             }
+            for (int ks = ks0; ks < ks1; ks++) {
+                const int row = 4 * ks + lk;
+                double f[NB];
 #pragma unroll
-            for (int a = 0; a < TS; a++)
+                for (int bb = 0; bb < NB; bb++) f[bb] = row < h ? Xs[row * XP + 8 * bb + li] : 0.0;
+                int t = 0;
 #pragma unroll
-                for (int b = 0; b < TS; b++) sScr[grp * UP + q * TS * TS + a * TS + b] = acc[a][b];
+                for (int I = 0; I < NB; I++)
+#pragma unroll
+                    for (int J = I; J < NB; J++, t++)
+                        asm volatile(
+                            "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                            : "+d"(c0[t]), "+d"(c1[t])
+                            : "d"(f[I]), "d"(f[J]));
+            }
+            double* slot = sScr + (warp & 3) * NTL * 64 + li * 8 + 2 * lk;
+            if (warp < 4) {
+#pragma unroll
+                for (int t = 0; t < NTL; t++) {
+                    slot[t * 64] = c0[t];
+                    slot[t * 64 + 1] = c1[t];
+                }
+            }
+            __syncthreads();
+            if (warp >= 4) {
+#pragma unroll
+                for (int t = 0; t < NTL; t++) {
+                    slot[t * 64] += c0[t];
+                    slot[t * 64 + 1] += c1[t];
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
         double* myP = sP + (stage & 1) * UP;
         for (int u = tid; u < UP; u += NT) {
-            double v = sScr[u];
-#pragma unroll
-            for (int g2 = 1; g2 < NG; g2++) v += sScr[g2 * UP + u];
-            myP[u] = v;
+            // entry (gi, gj) of upper grid tile qq, from the 8 x 8 tile of its
+            // column blocks (the symmetric entry when gi's block is the later)
+            const int qq = u / (TS * TS), w = u - qq * (TS * TS);
+            int a0, b0;
+            upper_tile(qq, &a0, &b0);
+            int gi = a0 * TS + w / TS, gj = b0 * TS + w % TS;
+            if ((gi >> 3) > (gj >> 3)) {
+                const int tmp = gi;
+                gi = gj;
+                gj = tmp;
+            }
+            const int I = gi >> 3, J = gj >> 3;
+            const int e = (I * NB - (I * (I - 1)) / 2 + (J - I)) * 64 + (gi & 7) * 8 + (gj & 7);
+            myP[u] = ((sScr[e] + sScr[NTL * 64 + e]) + sScr[2 * NTL * 64 + e]) + sScr[3 * NTL * 64 + e];
         }
         cl.sync();  // every CTA's partial is complete and visible
         // sum the CTAs' partials in CTA order (distributed shared memory),
@@ -395,21 +425,28 @@ __global__ void __launch_bounds__(NT, 1) k_cq_factor(const DevDesc* D, int k, in
         }
         if (dec == DONE || dec == FALLBACK) break;
         nst = stage + 1;
-        // R <- R_{stage+1} R (both upper triangular), into the other buffer;
-        // the entries below the diagonal of sTn stay zero from the start
-        for (int e = tid; e < 32 * 32; e += NT) {
-            const int i = e >> 5, j = e & 31;
-            if (j < i) continue;
-            double a0 = 0.0, a1 = 0.0;
-            if (j < c) {
-                int t = i;
-                for (; t + 1 <= j; t += 2) {
-                    a0 = fma(sR[i * 33 + t], sT[t * 33 + j], a0);
-                    a1 = fma(sR[i * 33 + t + 1], sT[(t + 1) * 33 + j], a1);
-                }
-                if (t <= j) a0 = fma(sR[i * 33 + t], sT[t * 33 + j], a0);
+        // R <- R_{stage+1} R (both upper triangular, zero beyond c) into the
+        // other buffer on the FP64 tensor cores: warp w forms 8 x 8 tiles w and
+        // w + 8 of the 10 upper tiles, k over the tile's triangle band; the
+        // tiles below the diagonal of sTn stay zero from the start, the lower
+        // halves of the diagonal tiles come out as exact zeros
+        for (int t = warp; t < 10; t += NT / 32) {
+            int I = 0, J = t;
+            while (J >= 4 - I) {
+                J -= 4 - I;
+                I++;
             }
-            sTn[i * 33 + j] = a0 + a1;
+            J += I;
+            double d0 = 0.0, d1 = 0.0;
+            for (int k0 = 8 * I; k0 < 8 * J + 8; k0 += 4) {
+                const double av = sR[(8 * I + li) * 33 + k0 + lk];
+                const double bv = sT[(k0 + lk) * 33 + 8 * J + li];
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                             : "+d"(d0), "+d"(d1)
+                             : "d"(av), "d"(bv));
+            }
+            sTn[(8 * I + li) * 33 + 8 * J + 2 * lk] = d0;
+            sTn[(8 * I + li) * 33 + 8 * J + 2 * lk + 1] = d1;
         }
         {
             double* t2 = sT;
