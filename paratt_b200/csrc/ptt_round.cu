@@ -1009,34 +1009,70 @@ __device__ void gemm_tile(GV A, GV B, double* C, long long crs, long long ccs, i
     }
 }
 
-// core[i+1] <- R * core[i+1]   (R = root factor, q x c, row-major CT)
-__global__ void __launch_bounds__(256) k_gemm_rx(const DevDesc* D, int i1, Plan pl, double* ws) {
-    PTT_PDL_ENTRY();
-    if (pl.info->status) return;
-    const int q = pl.info->q, c = pl.info->c;
-    const int N = D->n[i1] * D->r[i1 + 1];
-    const int tm = blockIdx.x, tn = blockIdx.y;
-    if (tm * GT >= q) return;
-    for (int t = tn; t * GT < N; t += gridDim.y) {
-        GV A{ws + pl.o_Rn, pl.CT, 1};
-        GV B{D->core[i1], 1, c};
-        gemm_tile(A, B, D->alt[i1], 1, q, q, N, c, tm, t);
+// The bookkeeping that follows a bond's contraction: publish the bond's new
+// rank (D->r[kq] = *val) and swap core[ka] with the buffer just written.
+// With a ticket (a zero-initialised counter) the last block of the
+// contraction does it, so it needs no launch of its own; without one the
+// caller launches k_bond_finalize.
+struct Fin {
+    int* ticket;
+    int kq, ka;
+    const int* val;
+};
+
+__device__ __forceinline__ void fin_last_block(DevDesc* D, const Fin& f, const Info* info) {
+    if (!f.ticket) return;
+    __shared__ int s_last;
+    __syncthreads();
+    __threadfence();  // this block's output is visible before its ticket
+    if (threadIdx.x == 0) s_last = atomicAdd(f.ticket, 1) == (int)(gridDim.x * gridDim.y) - 1;
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        *f.ticket = 0;
+        __threadfence();
+        if (info->status == 0) {
+            D->r[f.kq] = *f.val;
+            double* t = D->core[f.ka];
+            D->core[f.ka] = D->alt[f.ka];
+            D->alt[f.ka] = t;
+        }
     }
 }
 
-// core[i-1] <- core[i-1] * US   (US = c x rank, column-major ld CT)
-__global__ void __launch_bounds__(256) k_gemm_xm(const DevDesc* D, int im1, Plan pl, double* ws) {
+// core[i+1] <- R * core[i+1]   (R = root factor, q x c, row-major CT)
+__global__ void __launch_bounds__(256) k_gemm_rx(DevDesc* D, int i1, Plan pl, double* ws, Fin fin) {
     PTT_PDL_ENTRY();
-    if (pl.info->status) return;
-    const int c = pl.info->c, rank = pl.info->rank;
-    const int M = D->r[im1] * D->n[im1];
-    const int tn = blockIdx.y;
-    if (tn * GT >= rank) return;
-    for (int t = blockIdx.x; t * GT < M; t += gridDim.x) {
-        GV A{D->core[im1], 1, M};
-        GV B{ws + pl.o_US, 1, pl.CT};
-        gemm_tile(A, B, D->alt[im1], 1, M, M, rank, c, t, tn);
+    const int tm = blockIdx.x, tn = blockIdx.y;
+    if (pl.info->status == 0) {
+        const int q = pl.info->q, c = pl.info->c;
+        const int N = D->n[i1] * D->r[i1 + 1];
+        if (tm * GT < q) {
+            for (int t = tn; t * GT < N; t += gridDim.y) {
+                GV A{ws + pl.o_Rn, pl.CT, 1};
+                GV B{D->core[i1], 1, c};
+                gemm_tile(A, B, D->alt[i1], 1, q, q, N, c, tm, t);
+            }
+        }
     }
+    fin_last_block(D, fin, pl.info);
+}
+
+// core[i-1] <- core[i-1] * US   (US = c x rank, column-major ld CT)
+__global__ void __launch_bounds__(256) k_gemm_xm(DevDesc* D, int im1, Plan pl, double* ws, Fin fin) {
+    PTT_PDL_ENTRY();
+    const int tn = blockIdx.y;
+    if (pl.info->status == 0) {
+        const int c = pl.info->c, rank = pl.info->rank;
+        const int M = D->r[im1] * D->n[im1];
+        if (tn * GT < rank) {
+            for (int t = blockIdx.x; t * GT < M; t += gridDim.x) {
+                GV A{D->core[im1], 1, M};
+                GV B{ws + pl.o_US, 1, pl.CT};
+                gemm_tile(A, B, D->alt[im1], 1, M, M, rank, c, t, tn);
+            }
+        }
+    }
+    fin_last_block(D, fin, pl.info);
 }
 
 // publish a bond's new rank and swap the two rewritten cores
@@ -1299,7 +1335,7 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
             const long long ncap = (long long)x->n[i + 1] * rk[i + 2];
             int gy = (int)((ncap + GT - 1) / GT);
             if (gy > 4096) gy = 4096;
-            PTT_CUDA(ptt_launch(c, k_gemm_rx, dim3((CT + GT - 1) / GT, gy), dim3(256), 0, dd, i + 1, pl, ws));
+            PTT_CUDA(ptt_launch(c, k_gemm_rx, dim3((CT + GT - 1) / GT, gy), dim3(256), 0, x->dd, i + 1, pl, ws, Fin{}));
             PTT_LAUNCHED(c);
         }
         PTT_CUDA(ptt_launch(c, k_set_identity, dim3(32), dim3(256), 0, pl, ws));
@@ -1337,7 +1373,7 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
             const long long mcap2 = (long long)rk[i - 1] * x->n[i - 1];
             int gx = (int)((mcap2 + GT - 1) / GT);
             if (gx > 4096) gx = 4096;
-            PTT_CUDA(ptt_launch(c, k_gemm_xm, dim3(gx, (CT + GT - 1) / GT), dim3(256), 0, dd, i - 1, pl, ws));
+            PTT_CUDA(ptt_launch(c, k_gemm_xm, dim3(gx, (CT + GT - 1) / GT), dim3(256), 0, x->dd, i - 1, pl, ws, Fin{}));
             PTT_LAUNCHED(c);
         }
         PTT_CUDA(ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i, i, i - 1, (const int*)&info->rank,
@@ -1447,6 +1483,7 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
     double* ws = (double*)c->ws;
     wp.cnt = c->d_counters;
     base.cnt = c->d_counters;
+    int* fin_ticket = c->d_counters + (long long)Pcap * d;  // past the bonds' tree counters
     base.qn = nullptr;
     base.pass = nullptr;
     base.stats = c->d_stats;
@@ -1593,9 +1630,9 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
                 const long long ncap = (long long)x->n[i + 1] * rk[i + 2];
                 int gy = (int)((ncap + GT - 1) / GT);
                 if (gy > 4096) gy = 4096;
-                PTT_CUDA(ptt_launch(c, k_gemm_rx, dim3(dim3(1, gy)), dim3(256), 0, x->dd, i + 1, pl, wsb));
-                PTT_LAUNCHED(c);
-                PTT_CUDA(ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i + 1, i + 1, -1, &pl.info->q, pl.info));
+                // the contraction's last block publishes the rank and swaps the core
+                PTT_CUDA(ptt_launch(c, k_gemm_rx, dim3(dim3(1, gy)), dim3(256), 0, x->dd, i + 1, pl, wsb,
+                                    Fin{fin_ticket, i + 1, i + 1, &pl.info->q}));
                 PTT_LAUNCHED(c);
             }
             if (d > 1) {
@@ -1621,9 +1658,8 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
                 const long long mcap = (long long)rk[i - 1] * x->n[i - 1];
                 int gx = (int)((mcap + GT - 1) / GT);
                 if (gx > 4096) gx = 4096;
-                PTT_CUDA(ptt_launch(c, k_gemm_xm, dim3(dim3(gx, 1)), dim3(256), 0, x->dd, i - 1, pl, wsb));
-                PTT_LAUNCHED(c);
-                PTT_CUDA(ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i, i - 1, -1, &pl.info->rank, pl.info));
+                PTT_CUDA(ptt_launch(c, k_gemm_xm, dim3(dim3(gx, 1)), dim3(256), 0, x->dd, i - 1, pl, wsb,
+                                    Fin{fin_ticket, i, i - 1, &pl.info->rank}));
                 PTT_LAUNCHED(c);
             }
             if (d > 1) {
