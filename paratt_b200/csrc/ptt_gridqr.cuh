@@ -211,18 +211,52 @@ __device__ bool warp_chol64(const double* G, int c, double shift, double* R, dou
             for (int i = 0; i < 32; i++) R[i * RP + k] = y[i];
         }
         __syncwarp();
-        // S[32 + t][k] = G[32 + t][k] + shift [t == lane] - sum_i R[i][32 + t] R[i][k]
+        // P = R12^T R12 on the FP64 tensor cores (the 10 upper 8 x 8 tiles, k
+        // over the 32 rows of R12), parked in the lower-left quarter of R,
+        // which is zero in the result; S[32 + t][k] = G[32 + t][k] + shift
+        // [t == lane] - P[t][lane] (only the upper entries t <= lane are used)
+        {
+            const int li = lane >> 2, lk = lane & 3;
+            double p0[10], p1[10];
+#pragma unroll
+            for (int q = 0; q < 10; q++) {
+                p0[q] = 0.0;
+                p1[q] = 0.0;
+            }
+#pragma unroll
+            for (int k0 = 0; k0 < 32; k0 += 4) {
+                double f[4];
+#pragma unroll
+                for (int bb = 0; bb < 4; bb++) f[bb] = R[(k0 + lk) * RP + 32 + 8 * bb + li];
+                int q = 0;
+#pragma unroll
+                for (int I = 0; I < 4; I++)
+#pragma unroll
+                    for (int J = I; J < 4; J++, q++)
+                        asm volatile(
+                            "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                            : "+d"(p0[q]), "+d"(p1[q])
+                            : "d"(f[I]), "d"(f[J]));
+            }
+            int q = 0;
+#pragma unroll
+            for (int I = 0; I < 4; I++)
+#pragma unroll
+                for (int J = I; J < 4; J++, q++) {
+                    R[(32 + 8 * I + li) * RP + 8 * J + 2 * lk] = p0[q];
+                    R[(32 + 8 * I + li) * RP + 8 * J + 2 * lk + 1] = p1[q];
+                }
+        }
+        __syncwarp();
 #pragma unroll
         for (int t = 0; t < 32; t++) {
-            double acc = 0.0;
-            if (mine && t < c2) {
-#pragma unroll
-                for (int i = 0; i < 32; i++) acc = fma(R[i * RP + 32 + t], y[i], acc);
-                g[t] = G[(32 + t) * GP + k] + (t == lane ? shift : 0.0) - acc;
-            } else {
-                g[t] = 0.0;
-            }
+            const double pt = R[(32 + t) * RP + lane];
+            g[t] = (mine && t < c2) ? G[(32 + t) * GP + k] + (t == lane ? shift : 0.0) - pt : 0.0;
         }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < 32; t++) R[(32 + t) * RP + lane] = 0.0;
+        __syncwarp();
         chol_panel(g, c2, 32, R, iv, sRow, ok, dmin, dmax);
     }
     __syncwarp();
