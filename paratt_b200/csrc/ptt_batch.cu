@@ -24,7 +24,10 @@ static int lane_ctx(ptt_ctx* c, int i, ptt_ctx** out) {
         c->lanes[c->nlanes++] = l;
     }
     c->lanes[i]->no_cholqr = c->no_cholqr;
-    c->lanes[i]->no_pdl = c->no_pdl;
+    // no programmatic dependent launch on the lanes: a dependent grid's CTAs
+    // occupy SMs while they wait for their predecessor, which on concurrent
+    // lanes takes those SMs from the other lanes' ready kernels
+    c->lanes[i]->no_pdl = 1;
     memcpy(c->lanes[i]->cq_cs, c->cq_cs, sizeof(c->cq_cs));
     c->lanes[i]->cq_tuned = c->cq_tuned;
     *out = c->lanes[i];
