@@ -310,7 +310,7 @@ def run_ours(args, rank, world, local_rank):
             "frac": achieved / hbm,
             # DRAM read + write of one k_cq_factor<16> launch of this step
             # (an ~3072 x <= 16 unfolding), from an ncu --set full capture
-            "traffic": 376576.0,
+            "traffic": 372480.0,
             "traffic_source": "ncu: one k_cq_factor<16> launch of the learned step (m ~3072, c <= 16)",
             "kernel": "factorisation: k_cq_factor (cluster Cholesky QR), k_wfactor/k_tsqr_factor fallback",
             "launches": klaunch, "avg_launch_us": 1e3 * ktime_ms / max(klaunch, 1),
