@@ -27,7 +27,7 @@
 // 1e20 and exactly repeated columns converge within six stages.
 //
 // One thread-block cluster factors one unfolding: CTA b of the cluster keeps
-// rows [b rpb, (b+1) rpb) in shared memory for all stages, every CTA writes
+// rows [b h, (b+1) h) (h = ceil(m / CS)) in shared memory for all stages, every CTA writes
 // the partial Gram matrix of its rows into its shared memory, and after a
 // cluster barrier every CTA sums all partials (distributed shared memory, CTA
 // order 0..CS-1) and runs the same Cholesky -- identical data and arithmetic,
@@ -199,7 +199,8 @@ __device__ __forceinline__ void warp_first_order(const double* sG, int c, double
 }
 
 // Factor core k's unfolding (mode) by the Cholesky sequence above.  Launched
-// as one cluster of CS CTAs with rpb rows each (m <= CS rpb, else fallback).
+// as one cluster of CS CTAs with room for rpb rows each (m <= CS rpb, else
+// fallback); CTA b takes rows [b ceil(m / CS), ...).
 template <int CB>
 __global__ void __launch_bounds__(NT, 1) k_cq_factor(const DevDesc* D, int k, int mode, Plan pl, wt::WP wp,
                                                   double* wsb, int rpb, long long* qstat) {
@@ -234,8 +235,12 @@ __global__ void __launch_bounds__(NT, 1) k_cq_factor(const DevDesc* D, int k, in
         return;
     }
     if (pl.work && crank == 0 && tid == 0) atomicAdd(pl.work, 16.0 * (double)m * (double)c);
-    const int r0 = crank * rpb;
-    const int h = (m - r0) < rpb ? ((m - r0) > 0 ? (m - r0) : 0) : rpb;
+    // the actual rows spread evenly: the host sized rpb (and the shared
+    // memory) from a bound on m, which the truncation sweep's shrinking
+    // ranks leave well above the rows a bond has
+    const int rpbd = (m + CS - 1) / CS;  // <= rpb
+    const int r0 = crank * rpbd;
+    const int h = (m - r0) < rpbd ? ((m - r0) > 0 ? (m - r0) : 0) : rpbd;
     // this CTA's rows: zero, then every element by cp.async (all in flight)
     for (int e = tid; e < h * XP; e += NT) Xs[e] = 0.0;
     for (int e = tid; e < 32 * 33; e += NT) {
