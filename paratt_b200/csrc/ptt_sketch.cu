@@ -39,7 +39,6 @@ template <int TM>
 __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, long long zoff, int kper, double* part) {
     PTT_PDL_ENTRY();
     constexpr int BK = 32;
-    constexpr int RT = TM / 16;
     constexpr int NL = TM * BK / 256;  // elements of each operand tile per thread
     __shared__ double sA[BK][TM + 1];
     __shared__ double sB[BK][TM + 1];
@@ -53,15 +52,21 @@ __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, long long zoff, int kpe
     const double* A = g.A + b1 * g.ab1 + b2 * g.ab2;
     const double* B = g.B + b1 * g.bb1 + b2 * g.bb2;
     double* C = g.C + b1 * g.cb1 + b2 * g.cb2;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int tid = threadIdx.x;
     const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TM;
     const bool a_colmajor = (g.ars == 1);
     const bool b_rowfast = (g.bcs == 1);
-    double acc[RT][RT];
+    // the product on the FP64 tensor cores: warp w owns TPW of the
+    // (TM / 8)^2 8 x 8 output tiles, all in one tile row (shared A fragment)
+    constexpr int TD = TM / 8, TPW = TD * TD / 8;
+    const int warp = tid >> 5, lane = tid & 31, li = lane >> 2, lk = lane & 3;
+    const int t0 = warp * TPW, tr = t0 / TD, tc0 = t0 - tr * TD;
+    double d0[TPW], d1[TPW];
 #pragma unroll
-    for (int i = 0; i < RT; i++)
-#pragma unroll
-        for (int j = 0; j < RT; j++) acc[i][j] = 0.0;
+    for (int t = 0; t < TPW; t++) {
+        d0[t] = 0.0;
+        d1[t] = 0.0;
+    }
     for (int k0 = kbeg; k0 < kend; k0 += BK) {
         // every element of both tiles is requested before the first store
         double va[NL], vb[NL];
@@ -103,33 +108,34 @@ __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, long long zoff, int kpe
         }
         __syncthreads();
 #pragma unroll
-        for (int kk = 0; kk < BK; kk++) {
-            double a[RT], b[RT];
+        for (int k4 = 0; k4 < BK; k4 += 4) {
+            const double av = sA[k4 + lk][8 * tr + li];
 #pragma unroll
-            for (int i = 0; i < RT; i++) a[i] = sA[kk][ty + 16 * i];
-#pragma unroll
-            for (int j = 0; j < RT; j++) b[j] = sB[kk][tx + 16 * j];
-#pragma unroll
-            for (int i = 0; i < RT; i++)
-#pragma unroll
-                for (int j = 0; j < RT; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+            for (int t = 0; t < TPW; t++) {
+                const double bv = sB[k4 + lk][8 * (tc0 + t) + li];
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                             : "+d"(d0[t]), "+d"(d1[t])
+                             : "d"(av), "d"(bv));
+            }
         }
         __syncthreads();
     }
+    const int gr = m0 + 8 * tr + li;
+    if (gr < g.M) {
 #pragma unroll
-    for (int i = 0; i < RT; i++) {
-        const int gr = m0 + ty + 16 * i;
-        if (gr >= g.M) continue;
+        for (int t = 0; t < TPW; t++) {
 #pragma unroll
-        for (int j = 0; j < RT; j++) {
-            const int gc = n0 + tx + 16 * j;
-            if (gc >= g.N) continue;
-            if (part) {
-                part[(((long long)sl * nb + bz) * g.M + gr) * g.N + gc] = acc[i][j];
-                continue;
+            for (int h = 0; h < 2; h++) {
+                const int gc = n0 + 8 * (tc0 + t) + 2 * lk + h;
+                if (gc >= g.N) continue;
+                const double v = h ? d1[t] : d0[t];
+                if (part) {
+                    part[(((long long)sl * nb + bz) * g.M + gr) * g.N + gc] = v;
+                    continue;
+                }
+                double* cp = C + (long long)gr * g.crs + (long long)gc * g.ccs;
+                *cp = (g.beta != 0.0) ? fma(g.alpha, v, g.beta * *cp) : g.alpha * v;
             }
-            double* cp = C + (long long)gr * g.crs + (long long)gc * g.ccs;
-            *cp = (g.beta != 0.0) ? fma(g.alpha, acc[i][j], g.beta * *cp) : g.alpha * acc[i][j];
         }
     }
 }
