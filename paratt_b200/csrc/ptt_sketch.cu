@@ -376,13 +376,32 @@ __device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
     return z ^ (z >> 31);
 }
 
-__global__ void k_gauss(double* G, long long cnt, unsigned long long seed, int core) {
+// The Gaussian sketch cores G_1 .. G_{d-1} in one launch: core k fills
+// [off[k], off[k+1]) of G from its own counter-based stream (splitmix64 of
+// the seed and the core index, Box-Muller), so a core's values do not
+// depend on the other cores or on the launch shape.
+struct GaussOff {
+    long long off[PTT_MAX_DIM + 1];
+};
+__global__ void k_gauss_all(double* G, GaussOff o, int k0, int k1, unsigned long long seed) {
     PTT_PDL_ENTRY();
-    const unsigned long long base = splitmix64(seed ^ (0xD1B54A32D192ED03ull * (unsigned long long)(core + 1)));
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt;
-         e += (long long)gridDim.x * blockDim.x) {
-        const unsigned long long h1 = splitmix64(base + 2ull * (unsigned long long)e);
-        const unsigned long long h2 = splitmix64(base + 2ull * (unsigned long long)e + 1ull);
+    const long long tot = o.off[k1] - o.off[k0];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < tot;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long e = o.off[k0] + i;
+        int lo = k0, hi = k1;  // the core: largest k with off[k] <= e
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (o.off[mid] <= e)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const int k = lo;
+        const unsigned long long base = splitmix64(seed ^ (0xD1B54A32D192ED03ull * (unsigned long long)(k + 1)));
+        const long long el = e - o.off[k];
+        const unsigned long long h1 = splitmix64(base + 2ull * (unsigned long long)el);
+        const unsigned long long h2 = splitmix64(base + 2ull * (unsigned long long)el + 1ull);
         const double u1 = ((double)(h1 >> 11) + 0.5) * 1.1102230246251565e-16;  // (0,1)
         const double u2 = (double)(h2 >> 11) * 1.1102230246251565e-16;          // [0,1)
         G[e] = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
@@ -479,9 +498,12 @@ static int sketch_round(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* 
         yc = yones;
     }
 
-    for (int k = 1; k < d; k++) {
-        const long long cnt = (long long)L[k] * n[k] * L[k + 1];
-        PTT_CUDA(ptt_launch(c, k_gauss, dim3(blocks_for(cnt)), dim3(256), 0, ws + oG[k], cnt, seed, k));
+    if (d > 1) {  // G_k at ws + oG[k], contiguous from oG[1] = 0
+        GaussOff go;
+        for (int k = 1; k < d; k++) go.off[k] = oG[k];
+        go.off[d] = oG[d - 1] + (long long)L[d - 1] * n[d - 1] * L[d];
+        PTT_CUDA(ptt_launch(c, k_gauss_all, dim3(blocks_for(go.off[d] - go.off[1])), dim3(256), 0, ws, go, 1, d,
+                            seed));
         PTT_LAUNCHED(c);
     }
     PTT_CUDA(ptt_launch(c, k_fill, dim3(1), dim3(32), 0, ws + oW[d], 1, 1.0));
