@@ -1554,15 +1554,15 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
         PTT_LAUNCHED(c);
         return PTT_OK;
     };
-    auto apply = [&](int k0, int nb, int mode, int Wmax, int cmax) -> int {
+    auto apply = [&](int k0, int nb, int mode, int Wmax, int cmax, Fin fin = Fin{}) -> int {
         const int cb = cbound(cmax);
         const dim3 g((Wmax + WPB - 1) / WPB, nb), b(32 * WPB);
         if (cb == 16)
-            PTT_CUDA(ptt_launch(c, k_wapply<16>, dim3(g), dim3(b), 0, x->dd, k0, mode, base, wp, ws, use_cq));
+            PTT_CUDA(ptt_launch(c, k_wapply<16>, dim3(g), dim3(b), 0, x->dd, k0, mode, base, wp, ws, use_cq, fin));
         else if (cb == 24)
-            PTT_CUDA(ptt_launch(c, k_wapply<24>, dim3(g), dim3(b), 0, x->dd, k0, mode, base, wp, ws, use_cq));
+            PTT_CUDA(ptt_launch(c, k_wapply<24>, dim3(g), dim3(b), 0, x->dd, k0, mode, base, wp, ws, use_cq, fin));
         else
-            PTT_CUDA(ptt_launch(c, k_wapply<32>, dim3(g), dim3(b), 0, x->dd, k0, mode, base, wp, ws, use_cq));
+            PTT_CUDA(ptt_launch(c, k_wapply<32>, dim3(g), dim3(b), 0, x->dd, k0, mode, base, wp, ws, use_cq, fin));
         PTT_LAUNCHED(c);
         if (use_cq && mode == RIGHT_T) {  // LEFT: the cluster wrote Q already
             long long gx = ((long long)Wmax * 32 + cq::NT - 1) / cq::NT;
@@ -1614,9 +1614,8 @@ static int round_impl_w(ptt_tt* x, const int* rk, double delta, const int* maxr,
             double* wsb;
             Plan pl = bond(i, &wsb);
             if ((rc = factor(i, LEFT, Wl[i], pl, wsb))) return rc;
-            if ((rc = apply(i, 1, LEFT, Wl[i], rk[i + 1]))) return rc;
-            PTT_CUDA(ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i + 1, i, -1, &pl.info->q, pl.info));
-            PTT_LAUNCHED(c);
+            // the apply's last block publishes the rank and swaps the core
+            if ((rc = apply(i, 1, LEFT, Wl[i], rk[i + 1], Fin{fin_ticket, i + 1, i, &pl.info->q}))) return rc;
             return PTT_OK;
         }
         if (phases & 1) {

@@ -303,9 +303,8 @@ __global__ void __launch_bounds__(32 * FPB) k_wfactor(const DevDesc* D, int k, i
 //   LEFT:    B = I_q;                       out (m x q, column-major) -> alt[k]
 //   RIGHT_T: B = V_r (Bn, row-major 32 x KC); out(row, col) -> alt[k][row * rank + col]
 template <int CB>
-__global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, int mode, Plan pl, WP wp, double* ws,
-                                                     int use_cq) {
-    PTT_PDL_ENTRY();
+__device__ __forceinline__ void wapply_body(const DevDesc* D, int k0, int mode, const Plan& pl, const WP& wp,
+                                            double* ws, int use_cq) {
     __shared__ double sh[WPB][32 * 33];
     __shared__ double stau[WPB][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -413,6 +412,16 @@ __global__ void __launch_bounds__(32 * WPB) k_wapply(const DevDesc* D, int k0, i
         w_store(out, 1, m, r0, h, qB, X, sw);
     else
         w_store(out, qB, 1, r0, h, qB, X, sw);
+}
+
+// With a ticket (fin.ticket) the last block also publishes the bond's rank
+// and swaps its core, as k_bond_finalize would after it (one bond, k0).
+template <int CB>
+__global__ void __launch_bounds__(32 * WPB) k_wapply(DevDesc* D, int k0, int mode, Plan pl, WP wp, double* ws,
+                                                     int use_cq, Fin fin) {
+    PTT_PDL_ENTRY();
+    wapply_body<CB>(D, k0, mode, pl, wp, ws, use_cq);
+    fin_last_block(D, fin, (const Info*)(ws + (long long)k0 * wp.stride + pl.o_info_d));
 }
 
 // swap core and alt of cores [k0, k1) unless an error was recorded
