@@ -15,6 +15,7 @@
 // structure, so no r_x r_y x n x r_x r_y core is ever stored.
 #include "ptt_common.cuh"
 
+#include <stddef.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -29,7 +30,19 @@ struct GemmB {
     long long crs, ccs, cb1, cb2;
     int M, N, K, nb1, nb2;
     double alpha, beta;
+    // optional: the first kernel of the product also writes the ranks
+    // rset[rk0] = rv0, rset[rk0 + 1] = rv1 (a train's device descriptor), so
+    // that bookkeeping needs no launch of its own
+    int* rset;
+    int rk0, rv0, rv1;
 };
+
+__device__ __forceinline__ void gemm_set_ranks(const GemmB& g, bool first) {
+    if (g.rset && first && threadIdx.x == 0) {
+        g.rset[g.rk0] = g.rv0;
+        g.rset[g.rk0 + 1] = g.rv1;
+    }
+}
 
 // C[b] = alpha * A[b] B[b] + beta * C[b]; batch b = b1 + nb1 * b2.
 // With split-K (part != NULL) grid z runs over (batch, slice): slice s sums
@@ -38,6 +51,7 @@ struct GemmB {
 template <int TM>
 __global__ void __launch_bounds__(256) k_gemm_b(GemmB g, long long zoff, int kper, double* part) {
     PTT_PDL_ENTRY();
+    gemm_set_ranks(g, blockIdx.x == 0 && blockIdx.y == 0 && zoff + blockIdx.z == 0);
     constexpr int BK = 32;
     constexpr int NL = TM * BK / 256;  // elements of each operand tile per thread
     __shared__ double sA[BK][TM + 1];
@@ -149,6 +163,7 @@ constexpr size_t SKINNY_SMEM = sizeof(double) * 2 * KS * 33;
 
 __global__ void __launch_bounds__(256) k_gemm_skinny(GemmB g, int ns, double* part) {
     PTT_PDL_ENTRY();
+    gemm_set_ranks(g, blockIdx.x == 0 && blockIdx.y == 0);
     extern __shared__ double ssm[];
     double* sA = ssm;            // [KS][33]: sA[k][i] = A(i, k0 + k)
     double* sB = ssm + KS * 33;  // [KS][33]: sB[k][j] = B(k0 + k, j)
@@ -292,7 +307,15 @@ __global__ void k_gemm_red(GemmB g, int ns, const double* part) {
 }
 
 int gemm(ptt_ctx* c, const GemmB& g) {
-    if (g.M <= 0 || g.N <= 0 || g.nb1 <= 0 || g.nb2 <= 0) return PTT_OK;
+    if (g.M <= 0 || g.N <= 0 || g.nb1 <= 0 || g.nb2 <= 0) {  // nothing to multiply; the ranks still go out
+        if (!g.rset) return PTT_OK;
+        GemmB h = g;
+        h.M = h.N = h.K = 0;
+        h.nb1 = h.nb2 = 1;
+        PTT_CUDA(ptt_launch(c, k_gemm_b<32>, dim3(1, 1, 1), dim3(256), 0, h, 0LL, 0, (double*)nullptr));
+        PTT_LAUNCHED(c);
+        return PTT_OK;
+    }
     const long long nb = (long long)g.nb1 * g.nb2;
     if (c->tkind == PTT_TIME_GEMM) c->hwork[PTT_TIME_GEMM] += 2.0 * g.M * (double)g.N * g.K * (double)nb;
     if (g.M <= 32 && g.N <= 32 && g.K >= 2 * KS) {
@@ -594,13 +617,13 @@ static int sketch_round(const ptt_tt* x, const ptt_tt* y, ptt_tt* z, const int* 
         }
         const int Lp = L[k + 1];
         // Y = Z W_{k+1} into z core k, then QR in place (core k <- Q)
+        // its first kernel also sets z's ranks r_k = r, r_{k+1} = Lp for the QR
         g = GemmB{ws + oZ, 1, (long long)r * nk, 0, 0,
                   ws + oW[k + 1], 1, Rp, 0, 0,
                   z->hd.core[k], 1, (long long)r * nk, 0, 0,
-                  r * nk, Lp, (int)Rp, 1, 1, 1.0, 0.0};
+                  r * nk, Lp, (int)Rp, 1, 1, 1.0, 0.0,
+                  (int*)((char*)z->dd + offsetof(DevDesc, r)), k, r, Lp};
         if ((rc = gemm(c, g))) return rc;
-        int rr[2] = {r, Lp};
-        if ((rc = ptt_set_ranks_async(z, k, rr, 2))) return rc;
         {
             // QR of core k: ranks known here (no read-back); the QR swaps
             // core k with its second buffer, mirrored in the host shadow
