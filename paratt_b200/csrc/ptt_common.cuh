@@ -36,6 +36,7 @@ struct ptt_ctx {
     cudaStream_t stream;
     cudaStream_t side;            // second stream for overlapped work
     cudaEvent_t ev_fork, ev_join;
+    cudaEvent_t ev_svd[2], ev_tail[2];  // truncation sweep: a bond's SVD done / its tail done, per slot
     int* d_status;                // device status word (first error wins)
     int fixed_plans;              // 1: size rounding plans by capacity (no rank read-back)
     long long launches;

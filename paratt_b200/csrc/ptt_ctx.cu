@@ -67,6 +67,10 @@ extern "C" ptt_ctx* ptt_ctx_create(int device) {
         ptt_cuda_check(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking), "stream") ||
         ptt_cuda_check(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming), "event") ||
         ptt_cuda_check(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming), "event") ||
+        ptt_cuda_check(cudaEventCreateWithFlags(&c->ev_svd[0], cudaEventDisableTiming), "event") ||
+        ptt_cuda_check(cudaEventCreateWithFlags(&c->ev_svd[1], cudaEventDisableTiming), "event") ||
+        ptt_cuda_check(cudaEventCreateWithFlags(&c->ev_tail[0], cudaEventDisableTiming), "event") ||
+        ptt_cuda_check(cudaEventCreateWithFlags(&c->ev_tail[1], cudaEventDisableTiming), "event") ||
         ptt_cuda_check(cudaMalloc(&c->d_status, sizeof(int)), "cudaMalloc status") ||
         ptt_cuda_check(cudaMemset(c->d_status, 0, sizeof(int)), "memset") ||
         ptt_cuda_check(cudaMalloc(&c->d_scalars, 512 * sizeof(double)), "cudaMalloc scalars") ||
@@ -202,6 +206,10 @@ extern "C" void ptt_ctx_destroy(ptt_ctx* c) {
     cudaFree(c->flush);
     cudaEventDestroy(c->ev_fork);
     cudaEventDestroy(c->ev_join);
+    for (int i = 0; i < 2; i++) {
+        cudaEventDestroy(c->ev_svd[i]);
+        cudaEventDestroy(c->ev_tail[i]);
+    }
     cudaStreamDestroy(c->stream);
     cudaStreamDestroy(c->side);
     free(c);

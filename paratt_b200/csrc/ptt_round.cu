@@ -180,7 +180,15 @@ __global__ void __launch_bounds__(NT) k_apply_leaf(const DevDesc* D, int kcore, 
     if (pl.info->status || kg0 >= kk) return;
     const int tid = threadIdx.x, col = tid >> 3, part = tid & 7;
     const int m = pl.info->m, c = pl.info->c;
-    const View A = make_view(D, kcore, mode, false);
+    // the unfolding the factorisation recorded (m x c), not the descriptor's
+    // ranks: in the truncation sweep this runs on the side stream while the
+    // main stream has already published the bond's new rank
+    View A;
+    A.p = D->core[kcore];
+    A.m = m;
+    A.c = c;
+    A.rs = (mode == LEFT) ? 1 : c;
+    A.cs = (mode == LEFT) ? m : 1;
     double* outp = D->alt[kcore];
     const long long ors = (mode == LEFT) ? 1 : kk;
     const long long ocs = (mode == LEFT) ? m : 1;
@@ -1275,38 +1283,43 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
     const int NGMAX = (NBMAX + gq::GROUP - 1) / gq::GROUP;
     long long o_gq = (total + 31) / 32 * 32, gq_len = 0;
     if (use_gq) gq_len = gq::REC + (long long)(NBMAX + NGMAX) * gq::UP + MQMAX * gq::CB + 64;
-    size_t bytes = (size_t)(o_gq + gq_len) * sizeof(double) + 256;
+    // two slots of the whole region (bond parity): the truncation sweep runs
+    // the tail of bond i (V replay, Q V_r, swap of core i) on the side stream
+    // while bond i - 1 is factored in the other slot
+    const long long SLOT = (o_gq + gq_len + 31) / 32 * 32;
+    size_t bytes = (size_t)(2 * SLOT) * sizeof(double) + 256;
     if ((rc = ptt_ws_reserve(c, bytes))) return rc;
     const size_t cnt_tree = (size_t)PMAX * 4 + 64;
     if ((rc = ptt_counters_reserve(c, cnt_tree + NGMAX + 2))) return rc;
-    double* ws = (double*)c->ws;
+    double* const ws0 = (double*)c->ws;
     // ints live after the doubles: qn [2P-1], pass [P], Info
     // Tree counters live alone in ctx->d_counters (zero between launches,
     // reset by the combining block); node ranks and pass flags in ws.
-    int* ints = (int*)(ws + base.o_nodes);
-    Info* info = (Info*)(ws + base.o_info_d);
-    gq::GQ gqs{};
-    gq::GQ* g = nullptr;
-    if (use_gq) {
-        gqs.rec = ws + o_gq;
-        gqs.part = gqs.rec + (gq::REC + 31) / 32 * 32;
-        gqs.gpart = gqs.part + (long long)NBMAX * gq::UP;
-        gqs.qscr = gqs.gpart + (long long)NGMAX * gq::UP;
-        gqs.cnt = c->d_counters + cnt_tree;
-        g = &gqs;
+    double* wss[2] = {ws0, ws0 + SLOT};
+    gq::GQ gqs[2] = {};
+    for (int sl = 0; sl < 2 && use_gq; sl++) {
+        gqs[sl].rec = wss[sl] + o_gq;
+        gqs[sl].part = gqs[sl].rec + (gq::REC + 31) / 32 * 32;
+        gqs[sl].gpart = gqs[sl].part + (long long)NBMAX * gq::UP;
+        gqs[sl].qscr = gqs[sl].gpart + (long long)NGMAX * gq::UP;
+        gqs[sl].cnt = c->d_counters + cnt_tree;  // main stream only
     }
+    double* ws = ws0;
+    Info* info = (Info*)(ws0 + base.o_info_d);
+    gq::GQ* g = use_gq ? &gqs[0] : nullptr;
 
-    auto mkplan = [&](long long mcap) {
+    auto mkplan = [&](long long mcap, int sl = 0) {
         Plan pl = base;
         Plan t;
         plan_bond(CT, mcap, KC, &t, pmax);
+        int* ints = (int*)(wss[sl] + base.o_nodes);
         pl.L = t.L;
         pl.P = t.P;
         pl.KL = KLMAX;
         pl.cnt = c->d_counters;
         pl.qn = ints;
         pl.pass = ints + 2 * PMAX;
-        pl.info = info;
+        pl.info = (Info*)(wss[sl] + base.o_info_d);
         pl.stats = c->d_stats;
         pl.work = (c->tkind == PTT_TIME_TSQR) ? c->d_work + PTT_TIME_TSQR : nullptr;
         return pl;
@@ -1345,10 +1358,27 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
                             (const Info*)info));
         PTT_LAUNCHED(c);
     }
-    // right-to-left truncation
+    // right-to-left truncation.  The tail of bond i (V replay, Q V_r into
+    // core i, swap of core i) is not needed by bond i - 1, which only reads
+    // core i - 1 and the new rank r_i: it runs on the side stream from the
+    // bond's slot (bond parity) while the main stream carries on; the main
+    // stream waits for a slot's previous tail before reusing it, and for both
+    // at the end.  Inside a caller's stream capture the sweep stays serial.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    PTT_CUDA(cudaStreamIsCapturing(c->stream, &cap));
+    const bool ovl = cap == cudaStreamCaptureStatusNone && !c->capturing;
+    bool pending[2] = {false, false};
     for (int i = d - 1; i >= 1 && (phases & 2); i--) {
+        const int sl = ovl ? (i & 1) : 0;
+        if (pending[sl]) {
+            PTT_CUDA(cudaStreamWaitEvent(c->stream, c->ev_tail[sl], 0));
+            pending[sl] = false;
+        }
+        ws = wss[sl];
+        info = (Info*)(ws + base.o_info_d);
+        g = use_gq ? &gqs[sl] : nullptr;
         const long long mcap = (long long)x->n[i] * rk[i + 1];
-        Plan pl = mkplan(mcap);
+        Plan pl = mkplan(mcap, sl);
         if ((rc = launch_factor<CT>(c, x, i, RIGHT_T, pl, ws, g, mcap))) return rc;
         const int mr = maxr ? maxr[i] : rk[i];
         ptt_time_begin(c, PTT_TIME_SVD);
@@ -1360,14 +1390,47 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
                                 i, c->d_status));
         ptt_time_end(c, PTT_TIME_SVD);
         PTT_LAUNCHED(c);
-        PTT_CUDA(ptt_launch(c, k_svd_replay, dim3((CT + 7) / 8), dim3(256), replay_smem<CT>(), pl, ws));
-        PTT_LAUNCHED(c);
-        if ((rc = launch_apply<CT>(c, x, i, RIGHT_T, pl, ws, &info->rank, CT))) return rc;
-        if (g) {  // Q V_r for a bond the grid Cholesky QR finished
-            int gx = (int)((mcap + gq::WROWS - 1) / gq::WROWS);
-            gx = gx < 1 ? 1 : (gx > 2 * c->nsm ? 2 * c->nsm : gx);
-            PTT_CUDA(ptt_launch(c, gq::k_gq_write, dim3(gx), dim3(gq::NT), 0, dd, i, pl, *g, ws));
+        // the tail: V_r, then Q V_r (Householder tree or grid Cholesky QR) into alt[i]
+        auto tail = [&]() -> int {
+            PTT_CUDA(ptt_launch(c, k_svd_replay, dim3((CT + 7) / 8), dim3(256), replay_smem<CT>(), pl, ws));
             PTT_LAUNCHED(c);
+            int r2 = launch_apply<CT>(c, x, i, RIGHT_T, pl, ws, &info->rank, CT);
+            if (r2) return r2;
+            if (g) {  // Q V_r for a bond the grid Cholesky QR finished
+                int gx = (int)((mcap + gq::WROWS - 1) / gq::WROWS);
+                gx = gx < 1 ? 1 : (gx > 2 * c->nsm ? 2 * c->nsm : gx);
+                PTT_CUDA(ptt_launch(c, gq::k_gq_write, dim3(gx), dim3(gq::NT), 0, dd, i, pl, *g, ws));
+                PTT_LAUNCHED(c);
+            }
+            return PTT_OK;
+        };
+        if (ovl) {
+            PTT_CUDA(cudaEventRecord(c->ev_svd[sl], c->stream));
+            PTT_CUDA(cudaStreamWaitEvent(c->side, c->ev_svd[sl], 0));
+            // the launch helpers issue on c->stream: point it at the side
+            // stream; plain launches there (full stream order after the
+            // event wait, no programmatic early start)
+            cudaStream_t mainst = c->stream;
+            const int pdl = c->no_pdl;
+            c->stream = c->side;
+            c->no_pdl = 1;
+            rc = tail();
+            if (!rc) {
+                const cudaError_t e = ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i, i, -1,
+                                                 (const int*)&info->rank, (const Info*)info);
+                rc = e == cudaSuccess ? PTT_OK : ptt_set_error(PTT_ERR_CUDA, "CUDA: %s", cudaGetErrorString(e));
+                PTT_LAUNCHED(c);
+            }
+            if (!rc) {
+                const cudaError_t e = cudaEventRecord(c->ev_tail[sl], c->side);
+                rc = e == cudaSuccess ? PTT_OK : ptt_set_error(PTT_ERR_CUDA, "CUDA: %s", cudaGetErrorString(e));
+            }
+            c->stream = mainst;
+            c->no_pdl = pdl;
+            if (rc) return rc;
+            pending[sl] = true;
+        } else if ((rc = tail())) {
+            return rc;
         }
         {
             const long long mcap2 = (long long)rk[i - 1] * x->n[i - 1];
@@ -1376,10 +1439,13 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
             PTT_CUDA(ptt_launch(c, k_gemm_xm, dim3(gx, (CT + GT - 1) / GT), dim3(256), 0, x->dd, i - 1, pl, ws, Fin{}));
             PTT_LAUNCHED(c);
         }
-        PTT_CUDA(ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i, i, i - 1, (const int*)&info->rank,
-                            (const Info*)info));
+        // the new rank r_i and core i - 1 (core i too when the tail ran here)
+        PTT_CUDA(ptt_launch(c, k_bond_finalize, dim3(1), dim3(32), 0, x->dd, i, ovl ? i - 1 : i, ovl ? -1 : i - 1,
+                            (const int*)&info->rank, (const Info*)info));
         PTT_LAUNCHED(c);
     }
+    for (int sl = 0; sl < 2; sl++)
+        if (pending[sl]) PTT_CUDA(cudaStreamWaitEvent(c->stream, c->ev_tail[sl], 0));
     return PTT_OK;
 }
 
