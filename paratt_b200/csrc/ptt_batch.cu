@@ -21,6 +21,7 @@ static int lane_ctx(ptt_ctx* c, int i, ptt_ctx** out) {
         cudaFree(l->d_status);
         l->d_status = c->d_status;
         l->shared_status = 1;
+        l->lane = 1;
         c->lanes[c->nlanes++] = l;
     }
     c->lanes[i]->no_cholqr = c->no_cholqr;

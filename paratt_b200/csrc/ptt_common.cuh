@@ -78,6 +78,9 @@ struct ptt_ctx {
     // fell back, Gram stages of the finished ones]
     int no_cholqr;
     long long* d_qrstat;
+    // a worker context of ptt_round_batch: the batch already overlaps whole
+    // roundings, so a lane runs each rounding's chain on its one stream
+    int lane;
     // programmatic dependent launch of the rounding chain: 0 = used (default)
     int no_pdl;
     int capturing;                // inside ptt_graph_run's own capture
