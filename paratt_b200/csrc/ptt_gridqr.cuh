@@ -112,33 +112,56 @@ __device__ __forceinline__ void tile_solve(double* Xs, int h, const double* R, c
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int li = lane >> 2, lk = lane & 3;
     const int ntile = (h + 7) >> 3, nb = (c + 7) >> 3;
-    for (int t = warp; t < ntile; t += NT / 32) {
-        double* xr = Xs + (t * 8 + li) * XP;  // this lane's row
+    constexpr int NW = NT / 32;
+    // two tiles at a time (t and t + NW), their dependent chains interleaved;
+    // a warp with one tile left solves it twice and stores it once
+    for (int t = warp; t < ntile; t += 2 * NW) {
+        const bool two = t + NW < ntile;
+        double* xa = Xs + (t * 8 + li) * XP;  // this lane's rows
+        double* xb = two ? Xs + ((t + NW) * 8 + li) * XP : xa;
         for (int J = 0; J < nb; J++) {
-            const double2 cv = *(const double2*)(xr + 8 * J + 2 * lk);
-            double c0 = cv.x, c1 = cv.y;  // columns 8J + 2lk, 8J + 2lk + 1
+            const double2 ca = *(const double2*)(xa + 8 * J + 2 * lk);
+            const double2 cb = *(const double2*)(xb + 8 * J + 2 * lk);
+            double a0 = ca.x, a1 = ca.y, b0 = cb.x, b1 = cb.y;  // columns 8J + 2lk, 8J + 2lk + 1
             for (int kk = 0; kk < 2 * J; kk++) {
-                const double av = -xr[4 * kk + lk];
                 const double bv = R[(4 * kk + lk) * RP + 8 * J + li];
+                const double ava = -xa[4 * kk + lk], avb = -xb[4 * kk + lk];
                 asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-                             : "+d"(c0), "+d"(c1)
-                             : "d"(av), "d"(bv));
+                             : "+d"(a0), "+d"(a1)
+                             : "d"(ava), "d"(bv));
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                             : "+d"(b0), "+d"(b1)
+                             : "d"(avb), "d"(bv));
             }
             const double* Rb = R + 8 * J * RP + 8 * J;
 #pragma unroll
             for (int j = 0; j < 8; j++) {
                 const int own = j >> 1;
+                const double ivj = iv[8 * J + j];
                 if (lk == own) {
-                    if (j & 1)
-                        c1 *= iv[8 * J + j];
-                    else
-                        c0 *= iv[8 * J + j];
+                    if (j & 1) {
+                        a1 *= ivj;
+                        b1 *= ivj;
+                    } else {
+                        a0 *= ivj;
+                        b0 *= ivj;
+                    }
                 }
-                const double y = __shfl_sync(0xffffffffu, (j & 1) ? c1 : c0, (lane & ~3) | own);
-                if (2 * lk > j) c0 = fma(-y, Rb[j * RP + 2 * lk], c0);
-                if (2 * lk + 1 > j) c1 = fma(-y, Rb[j * RP + 2 * lk + 1], c1);
+                const double ya = __shfl_sync(0xffffffffu, (j & 1) ? a1 : a0, (lane & ~3) | own);
+                const double yb = __shfl_sync(0xffffffffu, (j & 1) ? b1 : b0, (lane & ~3) | own);
+                if (2 * lk > j) {
+                    const double r = Rb[j * RP + 2 * lk];
+                    a0 = fma(-ya, r, a0);
+                    b0 = fma(-yb, r, b0);
+                }
+                if (2 * lk + 1 > j) {
+                    const double r = Rb[j * RP + 2 * lk + 1];
+                    a1 = fma(-ya, r, a1);
+                    b1 = fma(-yb, r, b1);
+                }
             }
-            *(double2*)(xr + 8 * J + 2 * lk) = make_double2(c0, c1);
+            *(double2*)(xa + 8 * J + 2 * lk) = make_double2(a0, a1);
+            if (two) *(double2*)(xb + 8 * J + 2 * lk) = make_double2(b0, b1);
             __syncwarp();
         }
     }
