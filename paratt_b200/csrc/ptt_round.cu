@@ -972,13 +972,16 @@ __device__ void gemm_tile(GV A, GV B, double* C, long long crs, long long ccs, i
     __shared__ double sA[GK][GT + 1];
     __shared__ double sB[GK][GT + 1];
     const int tid = threadIdx.x;
-    const int tx = tid & 15, ty = tid >> 4;
     const int m0 = tm * GT, n0 = tn * GT;
-    double acc[4][4];
+    // the tile product on the FP64 tensor cores: warp w owns the eight 8 x 8
+    // output tiles of tile row w (mma.m8n8k4, four k a step)
+    const int warp = tid >> 5, lane = tid & 31, li = lane >> 2, lk = lane & 3;
+    double d0[8], d1[8];
 #pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+    for (int t = 0; t < 8; t++) {
+        d0[t] = 0.0;
+        d1[t] = 0.0;
+    }
     for (int k0 = 0; k0 < K; k0 += GK) {
         for (int e = tid; e < GT * GK; e += 256) {
             const int r = e % GT, kk = e / GT;
@@ -992,27 +995,25 @@ __device__ void gemm_tile(GV A, GV B, double* C, long long crs, long long ccs, i
         }
         __syncthreads();
 #pragma unroll
-        for (int kk = 0; kk < GK; kk++) {
-            double a[4], b[4];
+        for (int k4 = 0; k4 < GK; k4 += 4) {
+            const double av = sA[k4 + lk][8 * warp + li];
 #pragma unroll
-            for (int i = 0; i < 4; i++) a[i] = sA[kk][ty + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; j++) b[j] = sB[kk][tx + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+            for (int t = 0; t < 8; t++) {
+                const double bv = sB[k4 + lk][8 * t + li];
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                             : "+d"(d0[t]), "+d"(d1[t])
+                             : "d"(av), "d"(bv));
+            }
         }
         __syncthreads();
     }
+    const int gr = m0 + 8 * warp + li;
+    if (gr < M) {
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int gr = m0 + ty + 16 * i;
-        if (gr >= M) continue;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int gc = n0 + tx + 16 * j;
-            if (gc < N) C[(long long)gr * crs + (long long)gc * ccs] = acc[i][j];
+        for (int t = 0; t < 8; t++) {
+            const int gc = n0 + 8 * t + 2 * lk;
+            if (gc < N) C[(long long)gr * crs + (long long)gc * ccs] = d0[t];
+            if (gc + 1 < N) C[(long long)gr * crs + (long long)(gc + 1) * ccs] = d1[t];
         }
     }
 }
