@@ -340,6 +340,9 @@ def run_ours(args, rank, world, local_rank):
     # the step: the path that the step's low ranks never reach
     c1 = config1_rounding(P, ctx, 3, 1)
     out["round_c1"] = {k: c1[k] for k in ("ms", "ranks_out", "achieved_gbs", "frac", "fp64_tflops", "breakdown")}
+    c1o = config1_rounding(P, ctx, 3, 1, ozaki=True)
+    out["round_c1_ozaki"] = {k: c1o[k] for k in ("ms", "ranks_out", "rel_diff_vs_fp64", "breakdown")}
+    out["round_c1_ozaki"]["gram"] = "7 BF16 digit slices per element, tcgen05.mma FP32 accumulation, FP64 recombination"
     if world == 1 and not args.no_cpu_baseline:
         nthr = cpu_threads()
         os.environ.setdefault("OPENBLAS_NUM_THREADS", str(nthr))
@@ -471,10 +474,12 @@ def run_batch(args, rank, world, local_rank):
 # ---------------------------------------------------------------------------
 # single rounding (--workload round): x + y of two rank-32 trains -> rank 32
 # ---------------------------------------------------------------------------
-def config1_rounding(P, ctx, steps, warmup):
+def config1_rounding(P, ctx, steps, warmup, ozaki=False):
     """d=40, n=256: z = x + y of two seeded random trains of interior rank
     32 (entries N(0, 1/(n r)) -- std 1/sqrt(n r)), rounded to tol 1e-10 x
-    ||z||_RMS with rank cap 32, plain FP64.  Device time by events on the
+    ||z||_RMS with rank cap 32, plain FP64 (ozaki: the Gram matrices of the
+    factorisations by the Ozaki split on the tensor cores, the result's
+    relative difference to the FP64 path reported).  Device time by events on the
     context stream, L2 flushed before each rounding (outside the events);
     roofline against the algorithmic bytes 8 sum_k (3 R_k n R_{k+1} +
     r_k n r_{k+1}); the algorithmic FP64 flops (Householder QR and Q of every
@@ -495,6 +500,7 @@ def config1_rounding(P, ctx, steps, warmup):
     P.axpby(1.0, X, 1.0, Y, Z)
     tol = 1e-10 * Z.norm()
     W = P.TT(ctx, [n] * d, cap)
+    ctx.ozaki(ozaki)
     ts = []
     for i in range(warmup + steps):
         W.copy_from(Z)
@@ -528,10 +534,23 @@ def config1_rounding(P, ctx, steps, warmup):
         ctx.time_kernels(0)
         breakdown[name] = {"ms": kms, "launches": kl}
     sweeps = [int(v) for v in ctx.round_stats(d)[1:, 2]]
+    diff = None
+    if ozaki:  # ||W_ozaki - W_fp64|| / ||W_fp64||, the difference formed as a train
+        ctx.ozaki(False)
+        W2 = P.TT(ctx, [n] * d, cap)
+        W2.copy_from(Z)
+        W2.round(tol, r)
+        D = P.TT(ctx, [n] * d, [1] + [4 * r] * (d - 1) + [1])
+        P.axpby(1.0, W, -1.0, W2, D)
+        D.round(0.0, 4 * r)  # orthogonal gauge first: the norm of the formal difference cancels
+        diff = D.norm() / W2.norm()
+        D.close()
+        W2.close()
+    ctx.ozaki(False)
     for t_ in (X, Y, Z, W):
         t_.close()
     hbm, src = peaks()
-    return {"ms": t, "ms_all": ts, "ranks_out": max(rk_out), "algorithmic_bytes": alg, "algorithmic_flops": flops,
+    return {"ms": t, "rel_diff_vs_fp64": diff, "ms_all": ts, "ranks_out": max(rk_out), "algorithmic_bytes": alg, "algorithmic_flops": flops,
             "achieved_gbs": alg / (t / 1e3) / 1e9, "frac": alg / (t / 1e3) / 1e9 / hbm, "peak": hbm,
             "peak_source": src, "fp64_tflops": flops / (t / 1e3) / 1e12, "breakdown": breakdown,
             "jacobi_sweeps": sweeps}
@@ -546,10 +565,11 @@ def run_round(args, rank, world, local_rank):
     ctx = P.Context(local_rank)
     if not args.no_autotune:
         autotune(ctx)  # Cholesky-QR cluster sizes, timed once per context
-    c1 = config1_rounding(P, ctx, args.steps, args.warmup)
+    c1 = config1_rounding(P, ctx, args.steps, args.warmup, ozaki=args.ozaki)
     t = c1["ms"]
+    gram = "Ozaki split (BF16 slices, tcgen05)" if args.ozaki else "FP64"
     out = {
-        "metric": "TT rounding d=40, n=256, ranks 64 -> 32 (plain FP64), roundings/s", "value": 1e3 / t,
+        "metric": f"TT rounding d=40, n=256, ranks 64 -> 32 (Gram: {gram}), roundings/s", "value": 1e3 / t,
         "unit": "roundings/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "round(x + y), x, y seeded rank-32 trains, N(0, 1/(n r)) entries, tol 1e-10 x "
@@ -560,6 +580,7 @@ def run_round(args, rank, world, local_rank):
         "fp64": {"algorithmic_flops": c1["algorithmic_flops"], "tflops": c1["fp64_tflops"]},
         "breakdown": c1["breakdown"],
         "jacobi_sweeps": c1["jacobi_sweeps"],
+        "rel_diff_vs_fp64": c1["rel_diff_vs_fp64"],
     }
     print(json.dumps(out))
     ctx.close()
@@ -679,6 +700,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ozaki", action="store_true",
+                    help="--workload round: Gram matrices by the Ozaki split on the tensor cores")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the built-in cluster-size and tile rules (short runs under a profiler)")
     ap.add_argument("--formal-d", type=int, default=40, help="cores of the trains of --workload formal")

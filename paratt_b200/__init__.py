@@ -81,6 +81,8 @@ _SIGS = {
     "ptt_ctx_fixed_plans": (_i, [_p, _i]),
     "ptt_ctx_graphs": (_i, [_p, _i]),
     "ptt_ctx_cholqr": (_i, [_p, _i]),
+    "ptt_ctx_ozaki": (_i, [_p, _i]),
+    "ptt_gram": (_i, [_p, _p, C.c_longlong, _i, C.c_longlong, _p, _i]),
     "ptt_ctx_pdl": (_i, [_p, _i]),
     "ptt_ctx_autotune": (_i, [_p]),
     "ptt_checkpoint_begin": (_p, [_p, C.c_char_p]),
@@ -194,6 +196,17 @@ class Context:
         """Cholesky-QR factorisation of unfoldings with <= 32 columns (default
         on; off = Householder TSQR only)."""
         _check(lib().ptt_ctx_cholqr(self.h, 1 if on else 0))
+
+    def ozaki(self, on=True):
+        """Gram matrices of the 33-64-column Cholesky QR by the Ozaki split on
+        the fifth-generation tensor cores (default off = FP64 mma)."""
+        _check(lib().ptt_ctx_ozaki(self.h, 1 if on else 0))
+
+    def gram(self, a_ptr, m, c, lda, g_ptr, method=0):
+        """G = A^T A of device arrays (column-major m x c at a_ptr, c x c at
+        g_ptr); method 0 FP64 mma, 1 Ozaki split; synchronises the context."""
+        _check(lib().ptt_gram(self.h, C.c_void_p(a_ptr), m, c, lda, C.c_void_p(g_ptr), method))
+        _check(lib().ptt_ctx_synchronize(self.h))
 
     def autotune(self):
         """Pick the Cholesky-QR cluster size per (columns, rows) bucket by

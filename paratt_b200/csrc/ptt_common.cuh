@@ -78,6 +78,9 @@ struct ptt_ctx {
     // fell back, Gram stages of the finished ones]
     int no_cholqr;
     long long* d_qrstat;
+    // Gram matrices of the grid Cholesky QR (33-64 columns) by the Ozaki
+    // split on the fifth-generation tensor cores: 0 = FP64 mma (default)
+    int ozaki;
     // a worker context of ptt_round_batch: the batch already overlaps whole
     // roundings, so a lane runs each rounding's chain on its one stream
     int lane;

@@ -36,6 +36,8 @@
 // the bonds finished here (Plan::gqstate).
 #pragma once
 
+#include "ptt_ozaki.cuh"
+
 namespace gq {
 
 constexpr int NT = 256;
@@ -59,6 +61,11 @@ constexpr double U = 1.1102230246251565e-16;
 constexpr int FSZ = CB * RP + CB;      // a factor and its inverse pivots
 constexpr int SCR = CB * GP + 2 * FSZ + 64;  // Gram, two candidate factors, row broadcasts of the deciding CTA
 constexpr size_t SMEM = sizeof(double) * ((size_t)RPB_MAX * XP + (size_t)SCR);
+// the Ozaki Gram (ptt_ozaki.cuh): the digit slices take the scratch region
+// and beyond once the rows are solved; its 64 x 65 sum buffer the rows' region
+constexpr size_t SMEM_OZ = sizeof(double) * (size_t)RPB_MAX * XP + oz::SMEM;
+static_assert(RPB_MAX == oz::KMAX, "one CTA's rows are one exact FP32 accumulation");
+static_assert(SMEM_OZ >= SMEM && RPB_MAX * XP >= 64 * 65, "Ozaki buffers");
 static_assert(CB * GP <= FSZ, "the accumulated R fits a factor buffer");
 static_assert(CB * RP + CB <= SCR, "factor fits the scratch");
 
@@ -287,12 +294,55 @@ __device__ bool warp_chol64(const double* G, int c, double shift, double* R, dou
     return ok;
 }
 
+// Partial Gram matrix (upper 8 x 8 tiles) of the CTA's rows on the FP64
+// tensor cores: warp w accumulates tiles w, w + 8, ... over all rows, four
+// rows per mma.m8n8k4 (A = the tile's row-block columns transposed, B = its
+// column-block columns), and writes them straight to P (tile q at P + 64 q).
+__device__ __forceinline__ void gram_fp64(const double* Xs, int h, double* P) {
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int li = lane >> 2, lk = lane & 3;
+    constexpr int NWP = NT / 32, TPW = (36 + NWP - 1) / NWP;
+    double c0[TPW], c1[TPW];
+    int oa[TPW], ob[TPW];
+#pragma unroll
+    for (int t = 0; t < TPW; t++) {
+        int ti = 0, tj = 0;
+        if (warp + NWP * t < 36) cq::upper_tile(warp + NWP * t, &ti, &tj);
+        oa[t] = ti * TS + li;
+        ob[t] = tj * TS + li;
+        c0[t] = 0.0;
+        c1[t] = 0.0;
+    }
+    for (int r = 0; r < h; r += 4) {
+        const int row = r + lk;
+        const double* xr = Xs + row * XP;
+        const bool ok = row < h;
+#pragma unroll
+        for (int t = 0; t < TPW; t++) {
+            if (warp + NWP * t < 36) {
+                const double av = ok ? xr[oa[t]] : 0.0;
+                const double bv = ok ? xr[ob[t]] : 0.0;
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                             : "+d"(c0[t]), "+d"(c1[t])
+                             : "d"(av), "d"(bv));
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < TPW; t++)
+        if (warp + NWP * t < 36)
+            *(double2*)(P + (warp + NWP * t) * TS * TS + li * TS + 2 * lk) = make_double2(c0[t], c1[t]);
+}
+
 // One stage of the factorisation of core k's unfolding (mode); gridDim.x CTAs
-// of g.rpb rows each.
+// of g.rpb rows each.  OZ: the Gram partials by the Ozaki split on the
+// fifth-generation tensor cores (ptt_ozaki.cuh) instead of FP64 mma.
+template <bool OZ>
 __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int mode, Plan pl, GQ g, double* ws,
                                                     int stage, long long* qstat) {
     PTT_PDL_ENTRY();
-    extern __shared__ double gsm[];
+    extern __shared__ __align__(128) double gsm[];
     double* Xs = gsm;                     // rpb x XP rows
     double* sScr = Xs + RPB_MAX * XP;     // factor; Gram partials; decision arrays
     __shared__ int s_state, s_fin, s_ticket, s_flags, s_cok[2];
@@ -411,46 +461,11 @@ __global__ void __launch_bounds__(NT, 1) k_gq_stage(const DevDesc* D, int k, int
         }
         if (s_state == FINISH) return;  // the last factor is applied: Q is final
     }
-    // partial Gram matrix (upper 8 x 8 tiles) of this CTA's rows on the FP64
-    // tensor cores: warp w accumulates tiles w, w + 8, ... over all rows, four
-    // rows per mma.m8n8k4 (A = the tile's row-block columns transposed, B =
-    // its column-block columns), and writes them straight to its partial
-    {
-        const int warp = tid >> 5, lane = tid & 31;
-        const int li = lane >> 2, lk = lane & 3;
-        constexpr int NWP = NT / 32, TPW = (36 + NWP - 1) / NWP;
-        double c0[TPW], c1[TPW];
-        int oa[TPW], ob[TPW];
-#pragma unroll
-        for (int t = 0; t < TPW; t++) {
-            int ti = 0, tj = 0;
-            if (warp + NWP * t < 36) cq::upper_tile(warp + NWP * t, &ti, &tj);
-            oa[t] = ti * TS + li;
-            ob[t] = tj * TS + li;
-            c0[t] = 0.0;
-            c1[t] = 0.0;
-        }
-        for (int r = 0; r < h; r += 4) {
-            const int row = r + lk;
-            const double* xr = Xs + row * XP;
-            const bool ok = row < h;
-#pragma unroll
-            for (int t = 0; t < TPW; t++) {
-                if (warp + NWP * t < 36) {
-                    const double av = ok ? xr[oa[t]] : 0.0;
-                    const double bv = ok ? xr[ob[t]] : 0.0;
-                    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-                                 : "+d"(c0[t]), "+d"(c1[t])
-                                 : "d"(av), "d"(bv));
-                }
-            }
-        }
-        double* P = g.part + (long long)b * UP;
-#pragma unroll
-        for (int t = 0; t < TPW; t++)
-            if (warp + NWP * t < 36)
-                *(double2*)(P + (warp + NWP * t) * TS * TS + li * TS + 2 * lk) = make_double2(c0[t], c1[t]);
-    }
+    // partial Gram matrix (upper 8 x 8 tiles) of this CTA's rows
+    if constexpr (OZ)
+        oz::gram_partial<NT>(Xs, XP, h, c, (unsigned char*)sScr, Xs, g.part + (long long)b * UP);
+    else
+        gram_fp64(Xs, h, g.part + (long long)b * UP);
     // first level: the last CTA of each group sums the group's partials
     const int ngroups = (nb + GROUP - 1) / GROUP;
     const int grp = b / GROUP;
@@ -750,6 +765,67 @@ __global__ void __launch_bounds__(NT) k_gq_write(const DevDesc* D, int k, Plan p
                 y1 = fma(sQ[row * (CB + 1) + t + 1], sB[(t + 1) * (CB + 1) + col], y1);
             }
             out[(long long)r0 * rank + e] = y0 + y1;
+        }
+    }
+}
+
+// G = A^T A of a column-major m x c matrix (c <= CB, leading dimension lda),
+// the Gram matrix of an unfolding on its own (ptt_gram): CTA b forms the
+// partial of rows [b RPB_MAX, (b + 1) RPB_MAX) -- on the FP64 tensor cores,
+// or by the Ozaki split on tcgen05 when OZ -- the last-arriving CTA of each
+// group of GROUP sums the group's partials in CTA order, the last-arriving
+// group sums the groups in order and writes G (c x c, column-major, both
+// triangles).  Deterministic; no CTA waits for another.
+template <bool OZ>
+__global__ void __launch_bounds__(NT, 1) k_gram(const double* A, long long m, int c, long long lda, double* part,
+                                                double* gpart, int* cnt, double* G) {
+    extern __shared__ __align__(128) double gsm[];
+    double* Xs = gsm;
+    __shared__ int s_ticket;
+    const int tid = threadIdx.x, b = (int)blockIdx.x, nb = (int)gridDim.x;
+    const long long r0 = (long long)b * RPB_MAX;
+    const int h = (m - r0) < RPB_MAX ? (int)(m - r0) : RPB_MAX;
+    for (int e = tid; e < RPB_MAX * XP; e += NT) Xs[e] = 0.0;
+    __syncthreads();
+    for (int e = tid; e < h * c; e += NT) {
+        const int col = e / h, row = e - col * h;
+        Xs[row * XP + col] = A[r0 + row + (long long)col * lda];
+    }
+    __syncthreads();
+    if constexpr (OZ)
+        oz::gram_partial<NT>(Xs, XP, h, c, (unsigned char*)(Xs + RPB_MAX * XP), Xs, part + (long long)b * UP);
+    else
+        gram_fp64(Xs, h, part + (long long)b * UP);
+    const int ngroups = (nb + GROUP - 1) / GROUP, grp = b / GROUP;
+    const int gsize = (nb - grp * GROUP) < GROUP ? (nb - grp * GROUP) : GROUP;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_ticket = atomicAdd(&cnt[grp], 1);
+    __syncthreads();
+    if (s_ticket != gsize - 1) return;
+    if (tid == 0) cnt[grp] = 0;
+    __threadfence();
+    for (int u = tid; u < UP; u += NT) {
+        double a = 0.0;
+        for (int t = 0; t < gsize; t++) a += ldcg(part + (long long)(grp * GROUP + t) * UP + u);
+        gpart[(long long)grp * UP + u] = a;
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_ticket = atomicAdd(&cnt[ngroups], 1);
+    __syncthreads();
+    if (s_ticket != ngroups - 1) return;
+    if (tid == 0) cnt[ngroups] = 0;
+    __threadfence();
+    for (int u = tid; u < UP; u += NT) {
+        double a = 0.0;
+        for (int t = 0; t < ngroups; t++) a += ldcg(gpart + (long long)t * UP + u);
+        int ti = 0, tj = 0;
+        cq::upper_tile(u >> 6, &ti, &tj);
+        const int i = ti * TS + ((u >> 3) & 7), j = tj * TS + (u & 7);
+        if (i < c && j < c && (ti < tj || i <= j)) {  // a diagonal tile's upper half
+            G[i + (long long)j * c] = a;
+            G[j + (long long)i * c] = a;
         }
     }
 }

@@ -1201,7 +1201,9 @@ static int set_attrs() {
                                       (int)ring_smem<CT <= 64 ? CT : 64>()));
     PTT_CUDA(cudaFuncSetAttribute(k_svd_replay, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)replay_smem<128>()));
-    PTT_CUDA(cudaFuncSetAttribute(gq::k_gq_stage, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gq::SMEM));
+    PTT_CUDA(cudaFuncSetAttribute(gq::k_gq_stage<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gq::SMEM));
+    PTT_CUDA(cudaFuncSetAttribute(gq::k_gq_stage<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)gq::SMEM_OZ));
     done.fetch_or(bit);
     return PTT_OK;
 }
@@ -1217,8 +1219,12 @@ static int launch_factor(ptt_ctx* c, ptt_tt* x, int k, int mode, Plan& pl, doubl
         const int nb = gq::ctas(mcap, g->rpb);
         pl.gqstate = (const int*)g->rec;
         for (int s = 0; s < gq::MAXST; s++) {
-            PTT_CUDA(ptt_launch(c, gq::k_gq_stage, dim3(nb), dim3(gq::NT), gq::SMEM, (const DevDesc*)x->dd, k, mode, pl,
-                                *g, ws, s, c->d_qrstat));
+            if (c->ozaki)
+                PTT_CUDA(ptt_launch(c, gq::k_gq_stage<true>, dim3(nb), dim3(gq::NT), gq::SMEM_OZ,
+                                    (const DevDesc*)x->dd, k, mode, pl, *g, ws, s, c->d_qrstat));
+            else
+                PTT_CUDA(ptt_launch(c, gq::k_gq_stage<false>, dim3(nb), dim3(gq::NT), gq::SMEM,
+                                    (const DevDesc*)x->dd, k, mode, pl, *g, ws, s, c->d_qrstat));
             PTT_LAUNCHED(c);
         }
     }
@@ -1804,6 +1810,44 @@ extern "C" int ptt_ctx_fixed_plans(ptt_ctx* c, int on) {
 
 extern "C" int ptt_round(ptt_tt* x, double tol, const int* maxrank) {
     return ptt_round_phases(x, tol, maxrank, 3, 0);
+}
+
+extern "C" int ptt_ctx_ozaki(ptt_ctx* c, int on) {
+    if (!c) return ptt_set_error(PTT_ERR_ARG, "null context");
+    c->ozaki = on ? 1 : 0;
+    for (int l = 0; l < c->nlanes; l++)
+        if (c->lanes[l]) c->lanes[l]->ozaki = c->ozaki;
+    return PTT_OK;
+}
+
+// G = A^T A of a device m x c column-major matrix (c <= 64): method 0 on the
+// FP64 tensor cores, 1 by the Ozaki split on the fifth-generation tensor
+// cores (the two Gram kernels of the grid Cholesky QR, ptt_gridqr.cuh and
+// ptt_ozaki.cuh).
+extern "C" int ptt_gram(ptt_ctx* c, const double* A, long long m, int cols, long long lda, double* G, int method) {
+    if (!c || !A || !G || m < 1 || cols < 1 || cols > gq::CB || lda < m || (method != 0 && method != 1))
+        return ptt_set_error(PTT_ERR_ARG, "ptt_gram: bad arguments");
+    const long long nbl = (m + gq::RPB_MAX - 1) / gq::RPB_MAX;
+    if (nbl > (1ll << 24)) return ptt_set_error(PTT_ERR_CAPACITY, "ptt_gram: %lld rows", m);
+    cudaSetDevice(c->device);
+    int rc;
+    const int nb = (int)nbl, ng = (nb + gq::GROUP - 1) / gq::GROUP;
+    if ((rc = ptt_ws_reserve(c, sizeof(double) * (size_t)(nb + ng) * gq::UP + 256))) return rc;
+    if ((rc = ptt_counters_reserve(c, (size_t)ng + 1))) return rc;
+    double* part = (double*)c->ws;
+    double* gpart = part + (long long)nb * gq::UP;
+    if (method == 1) {
+        PTT_CUDA(cudaFuncSetAttribute(gq::k_gram<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)gq::SMEM_OZ));
+        gq::k_gram<true><<<nb, gq::NT, gq::SMEM_OZ, c->stream>>>(A, m, cols, lda, part, gpart, c->d_counters, G);
+    } else {
+        PTT_CUDA(cudaFuncSetAttribute(gq::k_gram<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(sizeof(double) * gq::RPB_MAX * gq::XP)));
+        gq::k_gram<false><<<nb, gq::NT, sizeof(double) * gq::RPB_MAX * gq::XP, c->stream>>>(A, m, cols, lda, part,
+                                                                                          gpart, c->d_counters, G);
+    }
+    PTT_LAUNCHED(c);
+    return PTT_OK;
 }
 
 // ---------------------------------------------------------------------------
