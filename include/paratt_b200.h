@@ -89,16 +89,17 @@ PTT_API int ptt_ctx_graphs(ptt_ctx* ctx, int on);
  * and its batch workers: [0] factorisations finished by Cholesky QR, [1] fell
  * back, [2] Gram stages of the finished ones (synchronises). */
 PTT_API int ptt_ctx_cholqr(ptt_ctx* ctx, int on);
-/* Precision of the Gram matrices of the Cholesky-QR factorisation of 33- to
- * 64-column unfoldings (no counterpart in the reference): with on != 0 each
- * CTA's Gram partial is an Ozaki split-precision product -- its rows split
- * into seven BF16 digit slices of 8 bits with a power-of-two scale per column,
- * the slice products on the fifth-generation tensor cores (tcgen05.mma, FP32
- * accumulation, exact for the <= 112 rows a CTA holds), recombined in double
- * precision; with on == 0 (the default) FP64 mma.  The digits drop less than
- * 2^-52 max|a_i| max|a_j| per row, so both give the Gram matrix to double
- * precision; the triangular solves, the Q and R the factorisation returns and
- * the SVD stay FP64. */
+/* Precision of the contractions of the rounding's 33- to 64-column bonds
+ * (no counterpart in the reference): with on != 0 the Gram matrices of the
+ * Cholesky-QR stages and the R x core products of the left-to-right sweep are
+ * Ozaki split-precision products -- each operand split into seven BF16 digit
+ * slices of 8 bits with a power-of-two scale per row or column, the slice
+ * products on the fifth-generation tensor cores (tcgen05.mma, FP32
+ * accumulation, exact for the <= 112-term sums each accumulator takes),
+ * recombined in double precision; with on == 0 (the default) FP64 mma.  The
+ * digits drop less than 2^-52 max|a_i| max|b_j| per term, so both give the
+ * products to double precision; the triangular solves, the factors and the
+ * SVD stay FP64. */
 PTT_API int ptt_ctx_ozaki(ptt_ctx* ctx, int on);
 /* G = A^T A of a device m x c column-major matrix A (1 <= c <= 64, leading
  * dimension lda >= m) into the device array G (c x c, column-major), on the

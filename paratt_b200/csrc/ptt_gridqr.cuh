@@ -36,8 +36,6 @@
 // the bonds finished here (Plan::gqstate).
 #pragma once
 
-#include "ptt_ozaki.cuh"
-
 namespace gq {
 
 constexpr int NT = 256;

@@ -1084,6 +1084,37 @@ __global__ void __launch_bounds__(256) k_gemm_xm(DevDesc* D, int im1, Plan pl, d
     fin_last_block(D, fin, pl.info);
 }
 
+#include "ptt_ozaki.cuh"
+
+// k_gemm_rx of the block-level path with the product as an Ozaki
+// split-precision product on the fifth-generation tensor cores
+// (oz::gemm_tiles): R (q x c, row-major, leading dimension CT) times core
+// i1 (c x N, column-major) into alt[i1] (q x N); CTA y takes the 64-column
+// tiles y, y + gridDim.y, ...
+__global__ void __launch_bounds__(256, 1) k_gemm_rx_oz(DevDesc* D, int i1, Plan pl, double* ws) {
+    PTT_PDL_ENTRY();
+    extern __shared__ __align__(128) unsigned char osm[];
+    if (pl.info->status != 0) return;
+    const int q = pl.info->q, c = pl.info->c;
+    const int N = D->n[i1] * D->r[i1 + 1];
+    if (q > oz::KG || c > oz::KG || 64 * (int)blockIdx.y >= N) return;  // uniform
+    oz::gemm_tiles<256>(ws + pl.o_Rn, pl.CT, 1, D->core[i1], 1, c, D->alt[i1], q, q, N, c, osm, false);
+}
+
+// k_gemm_xm of the block-level path as an Ozaki product: core[i-1] (M x c,
+// column-major) times U_r S_r (c x rank, column-major, leading dimension CT)
+// into alt[i-1], formed as its transpose (U_r S_r)^T core^T so that the
+// 64-wide tiles run along the M rows
+__global__ void __launch_bounds__(256, 1) k_gemm_xm_oz(DevDesc* D, int im1, Plan pl, double* ws) {
+    PTT_PDL_ENTRY();
+    extern __shared__ __align__(128) unsigned char osm[];
+    if (pl.info->status != 0) return;
+    const int c = pl.info->c, rank = pl.info->rank;
+    const int M = D->r[im1] * D->n[im1];
+    if (rank > oz::KG || c > oz::KG || 64 * (int)blockIdx.y >= M) return;  // uniform
+    oz::gemm_tiles<256>(ws + pl.o_US, pl.CT, 1, D->core[im1], M, 1, D->alt[im1], M, rank, M, c, osm, true);
+}
+
 // publish a bond's new rank and swap the two rewritten cores
 __global__ void k_bond_finalize(DevDesc* D, int kq, int ka, int kb, const int* val, const Info* info) {
     PTT_PDL_ENTRY();
@@ -1204,6 +1235,8 @@ static int set_attrs() {
     PTT_CUDA(cudaFuncSetAttribute(gq::k_gq_stage<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gq::SMEM));
     PTT_CUDA(cudaFuncSetAttribute(gq::k_gq_stage<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)gq::SMEM_OZ));
+    PTT_CUDA(cudaFuncSetAttribute(k_gemm_rx_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)oz::SMEM_GEMM));
+    PTT_CUDA(cudaFuncSetAttribute(k_gemm_xm_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)oz::SMEM_GEMM));
     done.fetch_or(bit);
     return PTT_OK;
 }
@@ -1355,7 +1388,12 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
             const long long ncap = (long long)x->n[i + 1] * rk[i + 2];
             int gy = (int)((ncap + GT - 1) / GT);
             if (gy > 4096) gy = 4096;
-            PTT_CUDA(ptt_launch(c, k_gemm_rx, dim3((CT + GT - 1) / GT, gy), dim3(256), 0, x->dd, i + 1, pl, ws, Fin{}));
+            if (c->ozaki && CT <= oz::KG)  // one wave, R split once per CTA
+                PTT_CUDA(ptt_launch(c, k_gemm_rx_oz, dim3(1, gy < c->nsm ? gy : c->nsm), dim3(256), oz::SMEM_GEMM,
+                                    x->dd, i + 1, pl, ws));
+            else
+                PTT_CUDA(ptt_launch(c, k_gemm_rx, dim3((CT + GT - 1) / GT, gy), dim3(256), 0, x->dd, i + 1, pl, ws,
+                                    Fin{}));
             PTT_LAUNCHED(c);
         }
         PTT_CUDA(ptt_launch(c, k_set_identity, dim3(32), dim3(256), 0, pl, ws));
@@ -1446,7 +1484,12 @@ static int round_impl(ptt_tt* x, const int* rk, double delta, const int* maxr, i
             const long long mcap2 = (long long)rk[i - 1] * x->n[i - 1];
             int gx = (int)((mcap2 + GT - 1) / GT);
             if (gx > 4096) gx = 4096;
-            PTT_CUDA(ptt_launch(c, k_gemm_xm, dim3(gx, (CT + GT - 1) / GT), dim3(256), 0, x->dd, i - 1, pl, ws, Fin{}));
+            if (c->ozaki && CT <= oz::KG)  // one wave, U_r S_r split once per CTA
+                PTT_CUDA(ptt_launch(c, k_gemm_xm_oz, dim3(1, gx < c->nsm ? gx : c->nsm), dim3(256), oz::SMEM_GEMM,
+                                    x->dd, i - 1, pl, ws));
+            else
+                PTT_CUDA(ptt_launch(c, k_gemm_xm, dim3(gx, (CT + GT - 1) / GT), dim3(256), 0, x->dd, i - 1, pl, ws,
+                                    Fin{}));
             PTT_LAUNCHED(c);
         }
         // the new rank r_i and core i - 1 (core i too when the tail ran here)

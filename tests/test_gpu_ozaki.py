@@ -12,7 +12,11 @@
   the Gram stages of the grid Cholesky QR on the Ozaki path
   (ptt_ctx_ozaki): ranks equal to the reference's paratt_truncate
   (pattac.c:590-675, compiled in oracle/_ref), relative difference <= 1e-12,
-  and the same against the FP64 path of this library."""
+  and the same against the FP64 path of this library.  With ptt_ctx_ozaki the
+  R X products of the left sweep (R x core_{k+1}, K = the bond rank <= 64)
+  are Ozaki products too.
+* Roundings of gapped trains with 33-64-column unfoldings on the Ozaki path
+  against the oracle (ranks equal, <= 1e-12, right-orthonormal cores)."""
 import numpy as np
 import pytest
 
@@ -107,3 +111,37 @@ def test_config1_rounding_ozaki_vs_reference(ctx):
     print(f"config-1 rounding, Ozaki Gram: vs reference {err:.2e}, vs FP64 path {err_fp:.2e}")
     assert err <= 1e-12, err
     assert err_fp <= 1e-12, err_fp
+
+
+OZ_CASES = [
+    # dims, ranks, keep (per bond), maxrank: 33-64-column unfoldings, where the
+    # Gram stages and the R X products take the Ozaki path
+    ([64, 64, 64], [1, 64, 64, 1], [1, 40, 50, 1], 64),
+    ([16, 40, 24, 16], [1, 16, 60, 48, 1], [1, 12, 35, 20, 1], 64),
+    ([48, 48, 48, 48], [1, 48, 64, 48, 1], [1, 33, 45, 30, 1], 40),  # rank cap binds
+]
+
+
+@pytest.mark.parametrize("dims,ranks,keep,maxr", OZ_CASES)
+def test_round_parity_ozaki(ctx, dims, ranks, keep, maxr):
+    """Rounding with the Ozaki Gram matrices and R X products against the
+    oracle on gapped trains: ranks equal, difference <= 1e-12 of ||X||, and
+    cores 1..d-1 right-orthonormal."""
+    from test_gpu_round import gapped_tt
+
+    x = gapped_tt(dims, ranks, 13, keep)
+    tol = 1e-6 * O.norm(x)
+    ref = O.round_tt(x, tol, maxr)
+    ctx.ozaki(True)
+    try:
+        X = P.TT.from_cores(ctx, x)
+        X.round(tol, [maxr] * (len(dims) + 1))
+        got = X.get()
+        X.close()
+    finally:
+        ctx.ozaki(False)
+    assert O.ranks_of(got) == O.ranks_of(ref)
+    assert O.rel_diff_exact(got, ref) <= 1e-12
+    for c in got[1:]:
+        m = O.right_unfold(c)
+        np.testing.assert_allclose(m @ m.T, np.eye(m.shape[0]), atol=1e-12)
