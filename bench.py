@@ -693,6 +693,79 @@ def run_one_step(args, local_rank):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the reference's own driver program (--workload driver)
+# ---------------------------------------------------------------------------
+def run_driver(args, rank, world, local_rank):
+    """The reference's Burgers-Hopf CDF driver program
+    (mpi_pattac_rxn_burgers_rank_max_read_file.c, compiled unmodified from the
+    reference tree by oracle/Makefile) on libparatt_b200.so against the same
+    program on the compiled reference (host cores), from the same seeded
+    initial condition: d = 20 Gaussian modes of n = 256 points, rank cap
+    32, max(steps, 10) time steps of dt 1e-5 (fixed in the driver).  Times are
+    the driver's own (MPI_Wtime around its time loop, from its log): value =
+    the driver's steps/s on the GPU library.  The ranks it prints and the TT
+    folder it writes at t = 0 are compared between the two runs."""
+    import re
+    import subprocess
+    import tempfile
+
+    from oracle import tt_oracle as O  # checker of the two runs' outputs
+
+    if rank != 0:
+        return 0
+    here = os.path.dirname(os.path.abspath(__file__))
+    bins = {k: os.path.join(here, "oracle", "_ref", f"cdf_driver_{k}") for k in ("b200", "ref")}
+    if not all(os.path.exists(b) for b in bins.values()):
+        print(json.dumps({"workload": "driver", "unavailable": "oracle/_ref/cdf_driver_* not built (make -C oracle)"}))
+        return 0
+    d, n, rmax = 20, 256, 32
+    steps = max(args.steps, 10)
+    T, t, count = steps * 1e-5, 0.0, 0
+    while t < T:  # the driver's own loop: time_now += dt until >= t_end
+        t += 1e-5
+        count += 1
+    x = np.linspace(-1.3, 1.3, n)
+    res = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for k, b in bins.items():
+            wd = os.path.join(tmp, k)
+            os.makedirs(os.path.join(wd, "ic"))
+            for m in range(d):
+                v = np.exp(-(x - 0.05 * m) ** 2 / (2 * 0.3 ** 2)) / (0.3 * np.sqrt(2 * np.pi))
+                with open(os.path.join(wd, "ic", f"core_{m + 1}.cr"), "w") as f:
+                    f.write(f"1,{n},1\n")
+                    f.writelines("%+1.16e\n" % a for a in v)
+            env = dict(os.environ, PARATT_DEVICE=str(local_rank))
+            out = subprocess.run([b, "ic", str(d), str(rmax), "1e-5", "0.0", repr(T), "0"], cwd=wd, env=env,
+                                 capture_output=True, text=True, timeout=1800)
+            if out.returncode != 0:
+                raise RuntimeError(f"driver ({k}) failed: {out.stderr[-500:]}")
+            log = open(os.path.join(wd, "kse_cdf_timing_nprocs=1.log")).read().split()
+            folder = os.path.join(wd, "data", f"bg_rxn_d{d}_rk{rmax}_tt", "cdf_t_0.000")
+            cores = []
+            for m in range(d):
+                with open(os.path.join(folder, f"core_{m + 1}.cr")) as f:
+                    rl, nn, rr = (int(v) for v in f.readline().split(","))
+                    cores.append(np.array([float(v) for v in f.read().split()]).reshape((rl, nn, rr), order="F"))
+            res[k] = {"seconds": float(log[-1]), "ranks": re.findall(r"tt rank:\n([\d\t ]+)\n", out.stdout),
+                      "cores": cores}
+    g, r = res["b200"], res["ref"]
+    out = {
+        "metric": "reference CDF driver program, unmodified, on the library: time steps/s", "value": count / g["seconds"],
+        "unit": "steps/s", "n_gpus": 1, "steps": count, "warmup": 0, "ms_per_step": 1e3 * g["seconds"] / count,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "mpi_pattac_rxn_burgers_rank_max_read_file.c (Burgers-Hopf CDF), d=20 Gaussian modes, "
+                               "n=256, rank cap 32, dt 1e-5", "timing": "the driver's MPI_Wtime around its time loop"},
+        "reference": {"value": count / r["seconds"], "unit": "steps/s", "seconds": r["seconds"], "cores": cpu_threads(),
+                      "kind": "reference", "sample": f"the same program linked to the compiled reference, {count} steps"},
+        "speedup_vs_reference": r["seconds"] / g["seconds"],
+        "parity": {"ranks_equal": g["ranks"] == r["ranks"], "rel_tt_t0": O.rel_diff_exact(g["cores"], r["cores"])},
+    }
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -707,9 +780,10 @@ def main():
     ap.add_argument("--formal-d", type=int, default=40, help="cores of the trains of --workload formal")
     ap.add_argument("--one-step", choices=["plain", "learned"], default=None,
                     help="profiling aid: W warm-up steps, then one step; prints the launch index to skip to")
-    ap.add_argument("--workload", default="rk2", choices=["rk2", "batch", "round", "formal"],
+    ap.add_argument("--workload", default="rk2", choices=["rk2", "batch", "round", "formal", "driver"],
                     help="rk2: the headline reaction-Burgers steps; batch: 64 independent roundings; "
-                         "round: one rank-64 -> 32 rounding; formal: the HBM-bound formal kernels at full rank")
+                         "round: one rank-64 -> 32 rounding; formal: the HBM-bound formal kernels at full rank; "
+                         "driver: the reference's own CDF driver program on the library and on the reference")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -724,6 +798,8 @@ def main():
         return run_round(args, rank, world, local_rank)
     if args.workload == "formal":
         return run_formal(args, rank, world, local_rank)
+    if args.workload == "driver":
+        return run_driver(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 
 

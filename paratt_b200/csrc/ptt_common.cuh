@@ -65,6 +65,12 @@ struct ptt_ctx {
     int ones_n;
     void* flush;                  // L2 flush buffer
     size_t flush_bytes;
+    // whole-train transfers of pageable host cores (ptt_tt_set / ptt_tt_get):
+    // page-locked and device staging buffers, grown on demand
+    double* h_stage;
+    size_t h_stage_n;
+    double* d_stage;
+    size_t d_stage_n;
     // worker contexts of batched calls (own stream and workspaces, the
     // parent's status word)
     struct ptt_ctx* lanes[PTT_MAX_LANES];

@@ -199,6 +199,8 @@ extern "C" void ptt_ctx_destroy(ptt_ctx* c) {
     cudaFree(c->d_work);
     cudaFree(c->d_qrstat);
     cudaFreeHost(c->h_scalars);
+    cudaFreeHost(c->h_stage);
+    cudaFree(c->d_stage);
     for (int i = 0; i < 64; i++)
         if (c->marks[i]) cudaEventDestroy(c->marks[i]);
     for (int i = 0; i < 2 * c->tcap; i++) cudaEventDestroy(c->tev[i]);
@@ -540,6 +542,72 @@ extern "C" int ptt_tt_reserve(ptt_tt* t, const int* rank_cap) {
     return PTT_OK;
 }
 
+// Whole-train host transfers.  Cores in pageable host memory (the reference
+// API's malloc'd cores) go through one page-locked staging buffer: the host
+// packs them contiguously, one bulk copy crosses PCIe, and one kernel
+// scatters them to (or gathers them from) the device cores -- instead of a
+// pageable copy per core, each with its own staging and, device to host, its
+// own synchronisation.  Other memory (device, managed, page-locked) is copied
+// core by core.
+struct StageMap {
+    double* core[PTT_MAX_DIM];
+    long long off[PTT_MAX_DIM + 1];
+};
+__global__ void k_stage_scatter(const double* src, StageMap m) {
+    const int k = blockIdx.y;
+    const long long a = m.off[k], n = m.off[k + 1] - a;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        m.core[k][e] = src[a + e];
+}
+__global__ void k_stage_gather(double* dst, StageMap m) {
+    const int k = blockIdx.y;
+    const long long a = m.off[k], n = m.off[k + 1] - a;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        dst[a + e] = m.core[k][e];
+}
+
+static bool all_pageable(const void* const* p, int d) {
+    for (int k = 0; k < d; k++) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, p[k]) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        if (a.type != cudaMemoryTypeUnregistered) return false;
+    }
+    return true;
+}
+
+// staging for n doubles; callers leave no transfer in flight on the buffers
+// (ptt_tt_set and ptt_tt_get end with a stream synchronisation)
+static int stage_reserve(ptt_ctx* c, size_t n) {
+    if (n > c->h_stage_n) {
+        cudaFreeHost(c->h_stage);
+        c->h_stage = nullptr;
+        c->h_stage_n = 0;
+        const size_t m = n < (1u << 16) ? (1u << 16) : n + n / 2;
+        PTT_CUDA(cudaMallocHost(&c->h_stage, m * sizeof(double)));
+        c->h_stage_n = m;
+    }
+    if (n > c->d_stage_n) {
+        PTT_CUDA(cudaStreamSynchronize(c->stream));
+        cudaFree(c->d_stage);
+        c->d_stage = nullptr;
+        c->d_stage_n = 0;
+        const size_t m = n < (1u << 16) ? (1u << 16) : n + n / 2;
+        PTT_CUDA(cudaMalloc(&c->d_stage, m * sizeof(double)));
+        c->d_stage_n = m;
+    }
+    return PTT_OK;
+}
+
+static int stage_grid(const StageMap& m, int d) {
+    long long mx = 0;
+    for (int k = 0; k < d; k++) mx = (m.off[k + 1] - m.off[k]) > mx ? (m.off[k + 1] - m.off[k]) : mx;
+    long long g = (mx + 255) / 256;
+    return (int)(g < 1 ? 1 : (g > 64 ? 64 : g));
+}
+
 extern "C" int ptt_tt_set(ptt_tt* t, const int* ranks, const double* const* cores) {
     if (!t || !ranks || !cores) return ptt_set_error(PTT_ERR_ARG, "ptt_tt_set: bad arguments");
     if (ranks[0] != 1 || ranks[t->d] != 1) return ptt_set_error(PTT_ERR_ARG, "ptt_tt_set: boundary ranks must be 1");
@@ -556,10 +624,27 @@ extern "C" int ptt_tt_set(ptt_tt* t, const int* ranks, const double* const* core
     }
     int rc = ptt_pull_desc(t);
     if (rc) return rc;
+    StageMap m;
+    m.off[0] = 0;
     for (int k = 0; k < t->d; k++) {
-        size_t cnt = (size_t)ranks[k] * t->n[k] * ranks[k + 1];
-        PTT_CUDA(cudaMemcpyAsync(t->hd.core[k], cores[k], cnt * sizeof(double), cudaMemcpyDefault,
-                                 t->ctx->stream));
+        m.core[k] = t->hd.core[k];
+        m.off[k + 1] = m.off[k] + (long long)ranks[k] * t->n[k] * ranks[k + 1];
+    }
+    ptt_ctx* c = t->ctx;
+    if (m.off[t->d] > 0 && all_pageable((const void* const*)cores, t->d)) {
+        if ((rc = stage_reserve(c, (size_t)m.off[t->d]))) return rc;
+        for (int k = 0; k < t->d; k++)
+            memcpy(c->h_stage + m.off[k], cores[k], sizeof(double) * (size_t)(m.off[k + 1] - m.off[k]));
+        PTT_CUDA(cudaMemcpyAsync(c->d_stage, c->h_stage, sizeof(double) * (size_t)m.off[t->d],
+                                 cudaMemcpyHostToDevice, c->stream));
+        k_stage_scatter<<<dim3(stage_grid(m, t->d), t->d), 256, 0, c->stream>>>(c->d_stage, m);
+        PTT_LAUNCHED(c);
+    } else {
+        for (int k = 0; k < t->d; k++) {
+            size_t cnt = (size_t)ranks[k] * t->n[k] * ranks[k + 1];
+            PTT_CUDA(cudaMemcpyAsync(t->hd.core[k], cores[k], cnt * sizeof(double), cudaMemcpyDefault,
+                                     t->ctx->stream));
+        }
     }
     for (int k = 0; k <= t->d; k++) t->hd.r[k] = ranks[k];
     rc = ptt_push_desc(t);
@@ -584,6 +669,24 @@ extern "C" int ptt_tt_get(ptt_tt* t, int* ranks, double* const* cores) {
     if (rc) return rc;
     if (ranks) memcpy(ranks, t->hd.r, sizeof(int) * (t->d + 1));
     if (cores) {
+        StageMap m;
+        m.off[0] = 0;
+        for (int k = 0; k < t->d; k++) {
+            m.core[k] = t->hd.core[k];
+            m.off[k + 1] = m.off[k] + (long long)t->hd.r[k] * t->n[k] * t->hd.r[k + 1];
+        }
+        ptt_ctx* c = t->ctx;
+        if (m.off[t->d] > 0 && all_pageable((const void* const*)cores, t->d)) {
+            if ((rc = stage_reserve(c, (size_t)m.off[t->d]))) return rc;
+            k_stage_gather<<<dim3(stage_grid(m, t->d), t->d), 256, 0, c->stream>>>(c->d_stage, m);
+            PTT_LAUNCHED(c);
+            PTT_CUDA(cudaMemcpyAsync(c->h_stage, c->d_stage, sizeof(double) * (size_t)m.off[t->d],
+                                     cudaMemcpyDeviceToHost, c->stream));
+            rc = ptt_ctx_synchronize(c);
+            for (int k = 0; k < t->d; k++)
+                memcpy(cores[k], c->h_stage + m.off[k], sizeof(double) * (size_t)(m.off[k + 1] - m.off[k]));
+            return rc;
+        }
         for (int k = 0; k < t->d; k++) {
             size_t cnt = (size_t)t->hd.r[k] * t->n[k] * t->hd.r[k + 1];
             PTT_CUDA(cudaMemcpyAsync(cores[k], t->hd.core[k], cnt * sizeof(double), cudaMemcpyDefault,
