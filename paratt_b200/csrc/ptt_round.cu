@@ -982,18 +982,36 @@ __device__ void gemm_tile(GV A, GV B, double* C, long long crs, long long ccs, i
         d0[t] = 0.0;
         d1[t] = 0.0;
     }
-    for (int k0 = 0; k0 < K; k0 += GK) {
-        for (int e = tid; e < GT * GK; e += 256) {
-            const int r = e % GT, kk = e / GT;
-            const int gr = m0 + r, gk = k0 + kk;
-            sA[kk][r] = (gr < M && gk < K) ? A.p[(long long)gr * A.rs + (long long)gk * A.cs] : 0.0;
+    // every element of a K chunk requested before the first is stored, and the
+    // next chunk's loads in flight during this chunk's products
+    constexpr int PT = GT * GK / 256;
+    double va[PT], vb[PT];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int u = 0; u < PT; u++) {
+            const int e = tid + 256 * u;
+            {
+                const int r = e % GT, kk = e / GT;
+                const int gr = m0 + r, gk = k0 + kk;
+                va[u] = (gr < M && gk < K) ? A.p[(long long)gr * A.rs + (long long)gk * A.cs] : 0.0;
+            }
+            {
+                const int kk = e % GK, cn = e / GK;
+                const int gk = k0 + kk, gc = n0 + cn;
+                vb[u] = (gk < K && gc < N) ? B.p[(long long)gk * B.rs + (long long)gc * B.cs] : 0.0;
+            }
         }
-        for (int e = tid; e < GT * GK; e += 256) {
-            const int kk = e % GK, cn = e / GK;
-            const int gk = k0 + kk, gc = n0 + cn;
-            sB[kk][cn] = (gk < K && gc < N) ? B.p[(long long)gk * B.rs + (long long)gc * B.cs] : 0.0;
+    };
+    if (K > 0) load(0);
+    for (int k0 = 0; k0 < K; k0 += GK) {
+#pragma unroll
+        for (int u = 0; u < PT; u++) {
+            const int e = tid + 256 * u;
+            sA[e / GT][e % GT] = va[u];
+            sB[e % GK][e / GK] = vb[u];
         }
         __syncthreads();
+        if (k0 + GK < K) load(k0 + GK);
 #pragma unroll
         for (int k4 = 0; k4 < GK; k4 += 4) {
             const double av = sA[k4 + lk][8 * warp + li];
