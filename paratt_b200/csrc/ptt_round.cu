@@ -318,9 +318,25 @@ __global__ void __launch_bounds__(NTH) k_svd_jacobi(Plan pl, double* ws, double 
     const int c = info->c, q = info->q;
     const int qq = q + (q & 1);
     const double* R = ws + pl.o_Rn;  // root factor, row-major CT x CT; L = R^T
-    for (int e = tid; e < qq * S; e += SVD_NT) {
-        const int j = e / S, t = e - (e / S) * S;
-        Lc[e] = (j < q && t < c) ? R[(long long)j * CT + t] : 0.0;
+    constexpr int LPT = (CT * S + SVD_NT - 1) / SVD_NT;  // qq <= CT
+    if constexpr (LPT <= 16) {  // every element requested before the first is stored
+        double v[LPT];
+#pragma unroll
+        for (int u = 0; u < LPT; u++) {
+            const int e = tid + u * SVD_NT;
+            const int j = e / S, t = e - (e / S) * S;
+            v[u] = (e < qq * S && j < q && t < c) ? R[(long long)j * CT + t] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < LPT; u++) {
+            const int e = tid + u * SVD_NT;
+            if (e < qq * S) Lc[e] = v[u];
+        }
+    } else {
+        for (int e = tid; e < qq * S; e += SVD_NT) {
+            const int j = e / S, t = e - (e / S) * S;
+            Lc[e] = (j < q && t < c) ? R[(long long)j * CT + t] : 0.0;
+        }
     }
     __syncthreads();
     double2* rot = (double2*)(ws + pl.o_rot);
