@@ -1,7 +1,12 @@
-// Ozaki split-precision Gram matrix of a CTA's rows on the fifth-generation
-// tensor cores: tcgen05.mma with BF16 operands from shared memory and FP32
-// accumulators in tensor memory, recombined to double precision.  Included by
-// ptt_gridqr.cuh (inside ptt_round.cu's anonymous namespace).
+// Ozaki split-precision products on the fifth-generation tensor cores:
+// tcgen05.mma with BF16 operands from shared memory and FP32 accumulators in
+// tensor memory, recombined to double precision -- the Gram partial of a
+// CTA's rows (gram_partial, the grid Cholesky QR's Gram stages) and a small
+// factor times 64-column tiles of a core (gemm_tiles, the R X and X U_r S_r
+// contractions of the block-level sweeps).  Included by ptt_round.cu inside
+// its anonymous namespace.  Described below for the Gram; the tile products
+// split both operands the same way (per-row scales for the factor, per-column
+// for the tile) with K = the bond rank <= KG = 64.
 //
 // Splitting (error-free transformation of Ozaki, Ogita, Oishi, Rump, Numer.
 // Algorithms 59 (2012), in the integer-digit form of Ootomo, Ozaki, Yokota,
@@ -29,7 +34,8 @@
 // Shared memory (K-major, no swizzle: 8 x 16-byte core matrices): digit s of
 // element (k, j) at byte
 //     s SL + (j / 8) SBO + (k / 8) 128 + (j % 8) 16 + (k % 8) 2,
-// SBO = KMAX 16, SL = 8 SBO.  Slices are contiguous, so M = 128 rows of an
+// SBO = 16 x the K bound (KMAX; KG for the tile products), SL = 8 SBO.
+// Slices are contiguous, so M = 128 rows of an
 // operand are two consecutive slices and N = 64 nb columns nb consecutive
 // ones; one mma step takes K = 16 (two core matrices 128 bytes apart: LBO).
 // An eighth slice stays zero (the second half of the M = 128 tile of digit 6).
